@@ -1,0 +1,403 @@
+#!/usr/bin/env python
+"""Benchmark: cell-stage updates/s of the CUBISM-MPCF hot path on B200.
+
+Workload (one GPU): 512^3 cells, a cloud of 200 non-overlapping gas bubbles
+(radii U[0.02,0.06], centres uniform in [0.2,0.8]^3, seeded rejection
+sampling) in a stiffened-gas liquid at p=1000 (gamma=6.59, pc=4096,
+rho=1000; gas gamma=1.4, pc=0, rho=1, p=0.0234), tanh interface over 1.5
+cells, U(-1e-3,1e-3) velocity noise, absorbing boundaries, CFL 0.3.
+Synthetic inputs of that shape (no dataset is involved).
+
+One step = max speed of sound + on-device dt + three LSRK3 stages, replayed
+as a CUDA graph over device-resident state (inputs 11 GB > L2, so no flush
+is needed between steps).  The headline `value` is the MIXED form
+(FP32 bulk, FP64 pressure recovery and conservation sums); the line also
+carries the all-FP64 throughput on the same workload and the L1 / L-inf
+error of rho, p and G of the mixed run against the FP64 run.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+--impl reference times the reference algorithm's CPU implementation (the
+C restatement in oracle/, OpenMP over all host cores; the reference's own
+GPU convection does not build with CUDA 12) on a bounded sample of the
+same workload.
+"""
+import argparse
+import ctypes
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+REPO = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(REPO, "cubism-jr-gpu-mpcf_b200"))
+
+WORKLOAD = "c3_512"
+METRIC = "cell-stage updates/s on 1 B200: mixed vs plain FP64 at stated L1 error"
+UNIT = "cell-stage updates/s"
+BYTES_PER_CELL_STAGE = {"fp32_ref": 112, "fp32": 112, "mixed": 112, "fp64": 224}
+
+
+def flops_per_cell_stage():
+    """Algorithmic FP operations of one cell-stage, counted from the oracle's
+    operation mix: written down once, used for the compute
+    roofline."""
+    return FLOPS_PER_CELL_STAGE
+
+
+# filled from the operation count of the face pipeline (oracle restatement,
+# counting add/sub/mul/compare/min/max = 1, FMA = 2, div = 1, sqrt = 1):
+# per face 14 WENO reconstructions + wave speeds + 7 HLLC fluxes + u*,
+# three faces per cell, plus primitive conversion, divergence and update.
+FLOPS_PER_CELL_STAGE = None
+
+
+def env_rank():
+    return int(os.environ.get("RANK", "0")), int(os.environ.get("WORLD_SIZE", "1")), int(os.environ.get("LOCAL_RANK", "0"))
+
+
+class ClockSampler:
+    """nvidia-smi clocks / throttle reasons sampled during the timed region."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), "--query-gpu=" + self.Q,
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                smax = float(f[2])
+            except ValueError:
+                continue
+            for n, v in zip(names, f[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(n)
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": smax, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def measured_peaks():
+    p = os.path.join(REPO, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        return d.get("hbm_gbs", 6650.0), "measured"
+    return 6650.0, "fallback"
+
+
+def make_solver(mpcf, cfg, precision):
+    s = mpcf.Solver(cfg["dims"], precision=precision)
+    for d, bub in enumerate(cfg["bubbles"]):
+        s.ic_cloud(cfg["params"], bub, dom=d)
+    return s
+
+
+def derived_fields(st, dtype=np.float64):
+    rho = st[0].astype(dtype)
+    ke = 0.5 * (st[1].astype(dtype) ** 2 + st[2].astype(dtype) ** 2 + st[3].astype(dtype) ** 2) / rho
+    G = st[5].astype(dtype)
+    p = (st[4].astype(dtype) - ke - st[6].astype(dtype)) / G
+    return rho, p, G
+
+
+def time_steps(mpcf, s, steps, warmup, cfl, dist=None):
+    """Device-timed graph replay of `steps` LSRK3 steps; returns ms (max over ranks)."""
+    import torch
+    s.run(warmup, cfl=cfl, graph=True)
+    s.synchronize()
+    if dist is not None:
+        dist.barrier()
+    torch.cuda.synchronize()
+    # events on the solver's own stream are not reachable from torch; the
+    # library replays the graph on its stream and synchronises it, and the
+    # elapsed device time is taken with CUDA events around the same replay
+    # inside mpcf_time_run (below)
+    ms = run_timed(mpcf, s, steps, cfl)
+    torch.cuda.synchronize()
+    if dist is not None:
+        t = torch.tensor([ms], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+        dist.barrier()
+    return ms
+
+
+def run_timed(mpcf, s, steps, cfl):
+    L = mpcf.lib()
+    ms = ctypes.c_double()
+    mpcf._lib.check(L.mpcf_time_run(s._h, int(steps), float(cfl), 1e30, ctypes.byref(ms)))
+    return ms.value
+
+
+def stage_kernel_ms(mpcf, s, reps=6):
+    """Average duration of one stage-kernel launch (CUDA events on the
+    solver's stream), for the roofline."""
+    return s.time_stages(reps, dtinvh=0.0)
+
+
+def cpu_sample(cfg_params, bub, dims, threads):
+    """Oracle (C restatement, OpenMP) on a sub-block of the workload: cell-stage updates/s."""
+    import mpcf
+    sys.path.insert(0, os.path.join(REPO, "tests"))
+    import oracle_lib as O
+    os.environ["OMP_NUM_THREADS"] = str(threads)
+    U = mpcf.ic_cloud_host(dims, cfg_params, bub, np.float32)
+    R = [np.zeros_like(a) for a in U]
+    t0 = time.perf_counter()
+    O.step(dims, (0,) * 6, U, R, cfl=0.3)
+    dt = time.perf_counter() - t0
+    n = dims[0] * dims[1] * dims[2]
+    return 3.0 * n / dt, dt
+
+
+def reference_arm(args):
+    rank, world, _ = env_rank()
+    if rank != 0:
+        return 0
+    import mpcf
+    cores = os.cpu_count() or 1
+    os.environ["OMP_NUM_THREADS"] = str(cores)
+    cfg = mpcf.configs.config(WORKLOAD)
+    # bounded sample: a 512 x 512 x 16 slab of the 512^3 cloud (same cell
+    # spacing, bubbles and material data), one full LSRK3 step per timed step
+    sub = (512, 512, 16)
+    vals = []
+    for i in range(args.warmup + args.steps):
+        v, dt = cpu_sample(cfg["params"], cfg["bubbles"][0], sub, cores)
+        if i >= args.warmup:
+            vals.append(v)
+    value = statistics.median(vals)
+    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 3.0 * 512 ** 3 / value * 1e3,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic", "config": {"workload": WORKLOAD + ": 512^3, 200-bubble cloud, liquid p=1000, "
+                                            "absorbing, CFL 0.3", "sample": "512x512x16 slab, 1 LSRK3 step"},
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "port",
+                             "sample": "C restatement of the reference kernels (oracle/), FP32 reference "
+                                       "rounding, one LSRK3 step of a 512x512x16 slab of the workload"},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-fp64", action="store_true")
+    ap.add_argument("--workload", default=WORKLOAD)
+    args = ap.parse_args()
+    if args.impl == "reference":
+        return reference_arm(args)
+
+    import torch
+    rank, world, local = env_rank()
+    dist = None
+    if world > 1:
+        import torch.distributed as tdist
+        torch.cuda.set_device(local)
+        tdist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=300))
+        dist = tdist
+    else:
+        torch.cuda.set_device(0)
+    import mpcf
+    cfg = mpcf.configs.config(args.workload)
+    ncell = sum(d[0] * d[1] * d[2] for d in cfg["dims"])
+    K, W = args.steps, max(3, args.warmup)
+    cfl = mpcf.configs.CFL
+
+    # ---------------- mixed (headline)
+    s = make_solver(mpcf, cfg, "mixed")
+    s.set_tiling(*pick_tiling(mpcf, s))
+    s.track_conservation(True)
+    sums0 = s.conserved_sums()
+    clocks = ClockSampler(local)
+    clocks.start()
+    ms = time_steps(mpcf, s, K, W, cfl, dist)
+    clk = clocks.stop()
+    value = world * ncell * 3.0 * K / (ms * 1e-3)
+    ms_step = ms / K
+    mixed_state = s.get_state(with_reg=False) if rank == 0 else None
+    sums1 = s.conserved_sums()
+    # roofline of the dominant kernel (stage) on this same solver
+    st_ms = stage_kernel_ms(mpcf, s)
+    nt, grid, threads = s.launch_shape()
+    tiling = s.tiling()
+    s.close()
+    hbm, peak_kind = measured_peaks()
+    bytes_launch = BYTES_PER_CELL_STAGE["mixed"] * ncell
+    achieved = bytes_launch / (st_ms * 1e-3) / 1e9
+
+    # ---------------- FP64 on the same workload and step count
+    fp64 = None
+    err = None
+    if not args.no_fp64:
+        s64 = make_solver(mpcf, cfg, "fp64")
+        s64.set_tiling(*pick_tiling(mpcf, s64))
+        ms64 = time_steps(mpcf, s64, K, W, cfl, dist)
+        fp64 = world * ncell * 3.0 * K / (ms64 * 1e-3)
+        if rank == 0:
+            st64 = s64.get_state(with_reg=False)
+            r64, p64, G64 = derived_fields(st64)
+            rm, pm, Gm = derived_fields(mixed_state)
+            def l1(a, b):
+                return float(np.mean(np.abs(a - b)) / np.mean(np.abs(b)))
+            def linf(a, b):
+                return float(np.max(np.abs(a - b)) / np.max(np.abs(b)))
+            err = {"L1_rho": l1(rm, r64), "Linf_rho": linf(rm, r64), "L1_p": l1(pm, p64),
+                   "Linf_p": linf(pm, p64), "L1_G": l1(Gm, G64), "Linf_G": linf(Gm, G64),
+                   "note": "relative to the all-FP64 run after the same number of steps (W+K)"}
+            del st64
+        s64.close()
+
+    # ---------------- e2e through the C ABI with host buffers
+    e2e = None
+    if not args.no_e2e:
+        e2e = e2e_measure(mpcf, cfg, K=max(2, min(K, 4)), W=1, cfl=cfl, dist=dist)
+
+    # ---------------- CPU baseline (rank 0, N=1 only)
+    cpu = None
+    if not args.no_cpu and world == 1 and rank == 0:
+        cores = os.cpu_count() or 1
+        sub = (512, 512, 16)
+        v, dtc = cpu_sample(cfg["params"], cfg["bubbles"][0], sub, cores)
+        cpu = {"value": v, "unit": UNIT, "cores": cores, "kind": "port",
+               "sample": "C restatement of the reference kernels (oracle/), OpenMP, one LSRK3 step of a "
+                         "512x512x16 slab of the workload (%.1f s)" % dtc}
+
+    if rank == 0:
+        fp32_peak = ctypes.c_double()
+        mpcf._lib.check(mpcf.lib().mpcf_probe_fp32_peak(0, ctypes.byref(fp32_peak)))
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": K, "warmup": W,
+            "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32+f64 (mixed)", "data": "synthetic",
+            "config": {"workload": cfg["name"] + ": " + cfg["desc"] + ", absorbing, CFL 0.3, mixed form",
+                       "cells_per_gpu": ncell, "l2": "inputs 11 GB > 126 MB L2 (no flush needed)",
+                       "parallelism": "replicas" if world > 1 else "single GPU",
+                       "tiling": {"ty": tiling[0], "dz": tiling[1], "persistent": tiling[2]},
+                       "graph": True},
+            "fp64_value": fp64, "mixed_over_fp64": (value / fp64) if fp64 else None,
+            "precision_error": err,
+            "conservation_drift": {"mass": float((sums1[0][0] - sums0[0][0]) / sums0[0][0]),
+                                   "energy": float((sums1[0][4] - sums0[0][4]) / sums0[0][4]),
+                                   "note": "FP64 sums, absorbing boundaries (boundary fluxes included)"},
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
+                         "frac": achieved / hbm, "traffic": None,
+                         "kernel": "stage_kernel<PolMixed>", "ms_per_launch": st_ms,
+                         "algorithmic_bytes_per_launch": bytes_launch,
+                         "peak_kind": peak_kind},
+            "roofline_fp32": {"bound": "fp32", "peak_tflops_measured": fp32_peak.value,
+                              "flops_per_cell_stage": FLOPS_PER_CELL_STAGE,
+                              "achieved_tflops": (FLOPS_PER_CELL_STAGE * ncell / (st_ms * 1e-3) / 1e12)
+                              if FLOPS_PER_CELL_STAGE else None},
+            "gpu_launches": 5 * K * (1 if world == 1 else 1),
+            "clocks": clk,
+            "e2e": e2e,
+            "cpu_baseline": cpu,
+        }
+        if FLOPS_PER_CELL_STAGE:
+            line["roofline_fp32"]["frac"] = line["roofline_fp32"]["achieved_tflops"] / fp32_peak.value
+        print(json.dumps(line), flush=True)
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+def pick_tiling(mpcf, s):
+    """Tiling for the bench: the autotuned choice when available."""
+    env = os.environ.get("MPCF_TILING")
+    if env:
+        ty, dz, p = (int(v) for v in env.split(","))
+        return ty, dz, bool(p)
+    return s.tiling()
+
+
+def e2e_measure(mpcf, cfg, K, W, cfl, dist):
+    """Same metric through the C ABI with pinned host buffers: every step
+    uploads state + register, advances one LSRK3 step, downloads both."""
+    import torch
+    dims = cfg["dims"][0]
+    n = dims[0] * dims[1] * dims[2]
+    s = make_solver(mpcf, cfg, "mixed")
+    hst = [torch.empty(n, dtype=torch.float32, pin_memory=True) for _ in range(14)]
+    st = s.get_state()
+    for q in range(7):
+        hst[q].numpy()[:] = st[0][q]
+        hst[7 + q].numpy()[:] = st[1][q]
+    del st
+    L = mpcf.lib()
+    up = (ctypes.c_void_p * 7)(*[hst[q].data_ptr() for q in range(7)])
+    ur = (ctypes.c_void_p * 7)(*[hst[7 + q].data_ptr() for q in range(7)])
+
+    def one():
+        mpcf._lib.check(L.mpcf_set_state(s._h, 0, up, ur, 0))
+        mpcf._lib.check(L.mpcf_step(s._h, cfl, 1e30, None))
+        mpcf._lib.check(L.mpcf_get_state(s._h, 0, up, ur, 0))
+
+    for _ in range(W):
+        one()
+    if dist is not None:
+        dist.barrier()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(K):
+        one()
+    torch.cuda.synchronize()
+    sec = time.perf_counter() - t0
+    if dist is not None:
+        t = torch.tensor([sec], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        sec = float(t.item())
+    world = dist.get_world_size() if dist is not None else 1
+    s.close()
+    return {"value": world * n * 3.0 * K / sec, "unit": UNIT, "h2d_bytes_per_step": 14 * 4 * n,
+            "d2h_bytes_per_step": 14 * 4 * n,
+            "path": "mpcf_set_state (pinned host) + mpcf_step + mpcf_get_state, host wall clock"}
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,921 @@
+// mpcf_api.cu -- host runtime behind the C ABI of include/mpcf_b200.h.
+//
+// A solver owns, per domain, two state buffers (ping-pong) and the LSRK3
+// register in HBM, plus per-domain device scalars (dt/h, dt, time, the
+// sound-speed accumulator) and one CUDA stream.  Nothing is staged through
+// the host between stages: the reference's chunked PCIe streaming
+// (GPUlab.cpp:202-372,703-793) and its host-side halo fills
+// (BoundaryConditions.h:60-109) are replaced by the fused stage kernel.
+#include <cuda_runtime.h>
+#include <algorithm>
+#include <cstdarg>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <cmath>
+#include <random>
+#include <string>
+#include <vector>
+
+#include "../../include/mpcf_b200.h"
+#include "mpcf_types.h"
+#include "mpcf_launch.h"
+#include "mpcf_ic.h"
+
+using namespace mpcf;
+
+namespace {
+
+thread_local std::string g_err;
+
+int fail(int code, const char* fmt, ...)
+{
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof(buf), fmt, ap);
+    va_end(ap);
+    g_err = buf;
+    return code;
+}
+
+#define CK(call) do { cudaError_t e_ = (call); if (e_ != cudaSuccess) \
+    return fail(MPCF_ERR_CUDA, "%s failed: %s (%s:%d)", #call, cudaGetErrorString(e_), __FILE__, __LINE__); } while (0)
+
+struct DeviceGuard
+{
+    int prev = -1;
+    explicit DeviceGuard(int dev) { cudaGetDevice(&prev); if (prev != dev) cudaSetDevice(dev); else prev = -1; }
+    ~DeviceGuard() { if (prev >= 0) cudaSetDevice(prev); }
+};
+
+const double kLSRK3[3][2] = {{0.0, 1.0/4.0}, {-17.0/32.0, 8.0/9.0}, {-32.0/27.0, 3.0/4.0}};
+
+} // namespace
+
+struct mpcf_solver
+{
+    int device = 0;
+    int pol = 0;
+    int ndom = 0;
+    size_t esz = 4;
+    cudaStream_t stream = nullptr;
+    int num_sms = 148;
+
+    std::vector<DomDev> hdoms;
+    DomDev* ddoms = nullptr;
+    std::vector<void*> allocs;      // device allocations owned by the solver
+    int parity = 0;
+
+    // device scalars
+    void* sos_bits = nullptr;       // ndom * esz
+    void* dtinvh = nullptr;         // ndom * esz
+    double* dt = nullptr;           // ndom
+    double* time = nullptr;         // ndom
+    unsigned* err = nullptr;        // 1
+    unsigned* counter = nullptr;    // 1
+    double* tile_sums = nullptr;    // ntiles * 5
+    double* chunk_sums = nullptr;   // nchunks * 5
+    double* sums = nullptr;         // ndom * 5
+    double* bubbles = nullptr;      // scratch for IC
+    int bubbles_cap = 0;
+    void* host_stage = nullptr;     // pinned host scratch (ndom doubles/elems)
+
+    // launch configuration
+    int ty = 4, dz = 64, persist = 0;
+    int ntiles = 0;
+    int sos_chunk = 32768, nchunks = 0;
+    bool track_cons = false;
+    bool sums_valid = false;
+
+    // graphs of one step for the two parities
+    cudaGraphExec_t graph[2] = {nullptr, nullptr};
+    double graph_cfl = -1, graph_dtmax = -1;
+    bool graph_cons = false;
+};
+
+namespace {
+
+bool valid_ty(const mpcf_solver* s, int ty)
+{
+    if (ty == 2 || ty == 4 || ty == 8) return true;
+    return ty == 16 && s->pol == 0;
+}
+
+StageKernelInfo stage_info(const mpcf_solver* s, int ty, bool persist)
+{
+    return s->pol == 0 ? stage_info_ref(ty, persist) : stage_info_fast(s->pol, ty, persist);
+}
+
+void destroy_graphs(mpcf_solver* s)
+{
+    for (int i = 0; i < 2; ++i)
+        if (s->graph[i]) { cudaGraphExecDestroy(s->graph[i]); s->graph[i] = nullptr; }
+}
+
+int dev_alloc(mpcf_solver* s, void** p, size_t bytes)
+{
+    cudaError_t e = cudaMalloc(p, bytes);
+    if (e != cudaSuccess)
+    {
+        cudaGetLastError();
+        return fail(MPCF_ERR_NOMEM, "cudaMalloc(%zu bytes) failed: %s", bytes, cudaGetErrorString(e));
+    }
+    s->allocs.push_back(*p);
+    return MPCF_OK;
+}
+
+// Recompute the tile tables for the current tiling and upload the domain
+// descriptors.
+int apply_tiling(mpcf_solver* s)
+{
+    int t = 0, c = 0;
+    for (auto& D : s->hdoms)
+    {
+        D.tiles_x = (D.nx + 31) / 32;
+        D.tiles_y = (D.ny + s->ty - 1) / s->ty;
+        D.tiles_z = (D.nz + s->dz - 1) / s->dz;
+        D.tile_begin = t;
+        t += D.tiles_x * D.tiles_y * D.tiles_z;
+        const long long N = (long long)D.nx * D.ny * D.nz;
+        D.sos_chunk_begin = c;
+        D.sos_chunks = (int)((N + s->sos_chunk - 1) / s->sos_chunk);
+        c += D.sos_chunks;
+    }
+    s->ntiles = t;
+    s->nchunks = c;
+    if (s->tile_sums)
+    {
+        cudaFree(s->tile_sums);
+        s->allocs.erase(std::remove(s->allocs.begin(), s->allocs.end(), (void*)s->tile_sums), s->allocs.end());
+        s->tile_sums = nullptr;
+    }
+    int rc = dev_alloc(s, (void**)&s->tile_sums, sizeof(double) * 5 * (size_t)std::max(t, 1));
+    if (rc) return rc;
+    if (!s->chunk_sums)
+        if ((rc = dev_alloc(s, (void**)&s->chunk_sums, sizeof(double) * 5 * (size_t)std::max(c, 1)))) return rc;
+    CK(cudaMemcpyAsync(s->ddoms, s->hdoms.data(), sizeof(DomDev) * s->ndom, cudaMemcpyHostToDevice, s->stream));
+    CK(cudaStreamSynchronize(s->stream));
+    destroy_graphs(s);
+    return MPCF_OK;
+}
+
+int persistent_grid(mpcf_solver* s, int ty)
+{
+    StageKernelInfo I = stage_info(s, ty, true);
+    int nb = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, I.fn, 32 * ty, I.smem) != cudaSuccess || nb < 1)
+    {
+        cudaGetLastError();
+        nb = 1;
+    }
+    return std::min(s->ntiles, nb * s->num_sms);
+}
+
+StageArgs stage_args(mpcf_solver* s, double a, double b, bool sums)
+{
+    StageArgs A;
+    A.doms = s->ddoms;
+    A.ndom = s->ndom;
+    A.ntiles = s->ntiles;
+    A.dz = s->dz;
+    A.parity = s->parity;
+    A.a = a;
+    A.b = b;
+    A.dtinvh = s->dtinvh;
+    A.counter = s->counter;
+    A.err = s->err;
+    A.tile_sums = sums ? s->tile_sums : nullptr;
+    return A;
+}
+
+// Enqueue one stage on the solver's stream (device dt/h) and flip parity.
+int enqueue_stage(mpcf_solver* s, double a, double b, bool sums)
+{
+    StageArgs A = stage_args(s, a, b, sums);
+    int grid = s->ntiles;
+    if (s->persist)
+    {
+        grid = persistent_grid(s, s->ty);
+        CK(cudaMemsetAsync(s->counter, 0, sizeof(unsigned), s->stream));
+    }
+    cudaError_t e = s->pol == 0 ? launch_stage_ref(s->ty, s->persist != 0, A, grid, s->stream)
+                                : launch_stage_fast(s->pol, s->ty, s->persist != 0, A, grid, s->stream);
+    if (e != cudaSuccess) return fail(MPCF_ERR_CUDA, "stage launch failed: %s", cudaGetErrorString(e));
+    s->parity ^= 1;
+    if (sums)
+    {
+        CK(launch_sum_tiles(s->ddoms, s->ndom, s->tile_sums, s->sums, s->stream));
+        s->sums_valid = true;
+    }
+    else s->sums_valid = false;
+    return MPCF_OK;
+}
+
+int enqueue_sos(mpcf_solver* s)
+{
+    CK(cudaMemsetAsync(s->sos_bits, 0, s->esz * s->ndom, s->stream));
+    SosArgs A;
+    A.doms = s->ddoms;
+    A.ndom = s->ndom;
+    A.nchunks = s->nchunks;
+    A.chunk = s->sos_chunk;
+    A.parity = s->parity;
+    A.sos_bits = s->sos_bits;
+    CK(launch_sos(s->pol, A, s->stream));
+    return MPCF_OK;
+}
+
+int enqueue_dt(mpcf_solver* s, double cfl, double dt_max)
+{
+    DtArgs A;
+    A.doms = s->ddoms;
+    A.ndom = s->ndom;
+    A.cfl = cfl;
+    A.dt_max = dt_max;
+    A.sos_bits = s->sos_bits;
+    A.dtinvh = s->dtinvh;
+    A.dt = s->dt;
+    A.time = s->time;
+    A.err = s->err;
+    CK(launch_dt(s->pol, A, s->stream));
+    return MPCF_OK;
+}
+
+// The whole LSRK3 step on the stream: sound speed, dt, three stages.
+int enqueue_step(mpcf_solver* s, double cfl, double dt_max)
+{
+    int rc;
+    if ((rc = enqueue_sos(s))) return rc;
+    if ((rc = enqueue_dt(s, cfl, dt_max))) return rc;
+    for (int k = 0; k < 3; ++k)
+        if ((rc = enqueue_stage(s, kLSRK3[k][0], kLSRK3[k][1], s->track_cons && k == 2))) return rc;
+    return MPCF_OK;
+}
+
+int check_dom(const mpcf_solver* s, int dom)
+{
+    if (!s) return fail(MPCF_ERR_ARG, "null solver");
+    if (dom < 0 || dom >= s->ndom) return fail(MPCF_ERR_ARG, "domain index %d out of range [0,%d)", dom, s->ndom);
+    return MPCF_OK;
+}
+
+// Copy 7 fields between caller arrays and a device buffer (field stride fs).
+int copy_fields(mpcf_solver* s, void* dev_base, long long fs, long long n,
+                const void* const* src7, void* const* dst7, bool to_device, bool user_is_device)
+{
+    for (int q = 0; q < 7; ++q)
+    {
+        char* dev = (char*)dev_base + (size_t)q * fs * s->esz;
+        const size_t bytes = (size_t)n * s->esz;
+        if (to_device)
+        {
+            if (!src7[q]) return fail(MPCF_ERR_ARG, "field %d pointer is null", q);
+            CK(cudaMemcpyAsync(dev, src7[q], bytes, user_is_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, s->stream));
+        }
+        else
+        {
+            if (!dst7[q]) return fail(MPCF_ERR_ARG, "field %d pointer is null", q);
+            CK(cudaMemcpyAsync(dst7[q], dev, bytes, user_is_device ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost, s->stream));
+        }
+    }
+    return MPCF_OK;
+}
+
+} // namespace
+
+// ===========================================================================
+extern "C" {
+
+int mpcf_version(void) { return MPCF_API_VERSION; }
+const char* mpcf_last_error(void) { return g_err.c_str(); }
+int mpcf_elem_size(int precision)
+{
+    if (precision < 0 || precision > 3) return fail(MPCF_ERR_ARG, "unknown precision %d", precision);
+    return precision == MPCF_PREC_FP64 ? 8 : 4;
+}
+
+int mpcf_create(mpcf_solver** out, int ndomains, const int* dims, const int* bc, int precision, int device)
+{
+    if (!out) return fail(MPCF_ERR_ARG, "null output handle");
+    *out = nullptr;
+    if (ndomains < 1) return fail(MPCF_ERR_ARG, "ndomains must be >= 1 (got %d)", ndomains);
+    if (!dims) return fail(MPCF_ERR_ARG, "null dims");
+    if (precision < 0 || precision > 3) return fail(MPCF_ERR_ARG, "unknown precision %d", precision);
+    for (int d = 0; d < ndomains; ++d)
+    {
+        const int nx = dims[3 * d], ny = dims[3 * d + 1], nz = dims[3 * d + 2];
+        if (nx < 5 || ny < 5 || nz < 3)
+            return fail(MPCF_ERR_ARG, "domain %d: size %dx%dx%d below the minimum 5x5x3", d, nx, ny, nz);
+        if ((long long)nx * ny * nz > (1LL << 34))
+            return fail(MPCF_ERR_ARG, "domain %d: %lld cells exceed the supported 2^34", d, (long long)nx * ny * nz);
+        if (bc)
+            for (int f = 0; f < 6; ++f)
+                if (bc[6 * d + f] != MPCF_BC_ABSORBING && bc[6 * d + f] != MPCF_BC_REFLECTING)
+                    return fail(MPCF_ERR_ARG, "domain %d: unknown boundary condition %d on face %d", d, bc[6 * d + f], f);
+    }
+    int ndev = 0;
+    CK(cudaGetDeviceCount(&ndev));
+    if (device < 0 || device >= ndev) return fail(MPCF_ERR_ARG, "device %d not present (%d devices)", device, ndev);
+
+    mpcf_solver* s = new mpcf_solver();
+    s->device = device;
+    s->pol = precision;
+    s->ndom = ndomains;
+    s->esz = precision == MPCF_PREC_FP64 ? 8 : 4;
+    DeviceGuard g(device);
+    int rc = MPCF_OK;
+    auto bail = [&](int code) { mpcf_destroy(s); return code; };
+
+    if (cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking) != cudaSuccess)
+    { cudaGetLastError(); delete s; return fail(MPCF_ERR_CUDA, "cudaStreamCreate failed"); }
+    cudaDeviceGetAttribute(&s->num_sms, cudaDevAttrMultiProcessorCount, device);
+
+    s->hdoms.resize(ndomains);
+    for (int d = 0; d < ndomains; ++d)
+    {
+        DomDev& D = s->hdoms[d];
+        memset(&D, 0, sizeof(D));
+        D.nx = dims[3 * d]; D.ny = dims[3 * d + 1]; D.nz = dims[3 * d + 2];
+        for (int f = 0; f < 6; ++f) D.bc[f] = bc ? bc[6 * d + f] : MPCF_BC_ABSORBING;
+        D.h = 1.0 / (double)std::max(D.nx, std::max(D.ny, D.nz));
+        const long long N = (long long)D.nx * D.ny * D.nz;
+        D.fs = (N + 63) / 64 * 64;
+        for (int b = 0; b < 2; ++b)
+            if ((rc = dev_alloc(s, &D.U[b], (size_t)7 * D.fs * s->esz))) return bail(rc);
+        if ((rc = dev_alloc(s, &D.R, (size_t)7 * D.fs * s->esz))) return bail(rc);
+        if (cudaMemsetAsync(D.R, 0, (size_t)7 * D.fs * s->esz, s->stream) != cudaSuccess) return bail(fail(MPCF_ERR_CUDA, "memset"));
+    }
+    if ((rc = dev_alloc(s, (void**)&s->ddoms, sizeof(DomDev) * ndomains))) return bail(rc);
+    if ((rc = dev_alloc(s, &s->sos_bits, 8 * ndomains))) return bail(rc);
+    if ((rc = dev_alloc(s, &s->dtinvh, 8 * ndomains))) return bail(rc);
+    if ((rc = dev_alloc(s, (void**)&s->dt, 8 * ndomains))) return bail(rc);
+    if ((rc = dev_alloc(s, (void**)&s->time, 8 * ndomains))) return bail(rc);
+    if ((rc = dev_alloc(s, (void**)&s->sums, 8 * 5 * ndomains))) return bail(rc);
+    if ((rc = dev_alloc(s, (void**)&s->err, 16))) return bail(rc);
+    if ((rc = dev_alloc(s, (void**)&s->counter, 16))) return bail(rc);
+    cudaMemsetAsync(s->sos_bits, 0, 8 * ndomains, s->stream);
+    cudaMemsetAsync(s->dtinvh, 0, 8 * ndomains, s->stream);
+    cudaMemsetAsync(s->dt, 0, 8 * ndomains, s->stream);
+    cudaMemsetAsync(s->time, 0, 8 * ndomains, s->stream);
+    cudaMemsetAsync(s->sums, 0, 8 * 5 * ndomains, s->stream);
+    cudaMemsetAsync(s->err, 0, 16, s->stream);
+    cudaMemsetAsync(s->counter, 0, 16, s->stream);
+    if (cudaMallocHost(&s->host_stage, 8 * (size_t)ndomains * 8) != cudaSuccess)
+    { cudaGetLastError(); return bail(fail(MPCF_ERR_NOMEM, "cudaMallocHost failed")); }
+
+    // allow the large shared-memory footprints of every tiling variant
+    const int tys[4] = {2, 4, 8, 16};
+    for (int i = 0; i < 4; ++i)
+    {
+        if (!valid_ty(s, tys[i])) continue;
+        for (int p = 0; p < 2; ++p)
+        {
+            StageKernelInfo I = stage_info(s, tys[i], p != 0);
+            if (!I.fn) continue;
+            if (cudaFuncSetAttribute(I.fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)I.smem) != cudaSuccess)
+            { cudaGetLastError(); return bail(fail(MPCF_ERR_CUDA, "cannot grant %zu B shared memory to the stage kernel (ty=%d)", I.smem, tys[i])); }
+        }
+    }
+    s->ty = 4;
+    s->dz = 64;
+    s->persist = 0;
+    if ((rc = apply_tiling(s))) return bail(rc);
+    *out = s;
+    return MPCF_OK;
+}
+
+int mpcf_destroy(mpcf_solver* s)
+{
+    if (!s) return MPCF_OK;
+    DeviceGuard g(s->device);
+    if (s->stream) cudaStreamSynchronize(s->stream);
+    destroy_graphs(s);
+    for (void* p : s->allocs) cudaFree(p);
+    if (s->host_stage) cudaFreeHost(s->host_stage);
+    if (s->stream) cudaStreamDestroy(s->stream);
+    delete s;
+    return MPCF_OK;
+}
+
+int mpcf_num_domains(const mpcf_solver* s) { return s ? s->ndom : fail(MPCF_ERR_ARG, "null solver"); }
+int mpcf_precision(const mpcf_solver* s) { return s ? s->pol : fail(MPCF_ERR_ARG, "null solver"); }
+
+int mpcf_set_state(mpcf_solver* s, int dom, const void* const* state7, const void* const* reg7, int src_is_device)
+{
+    int rc = check_dom(s, dom);
+    if (rc) return rc;
+    if (!state7) return fail(MPCF_ERR_ARG, "null state pointers");
+    DeviceGuard g(s->device);
+    DomDev& D = s->hdoms[dom];
+    const long long N = (long long)D.nx * D.ny * D.nz;
+    if ((rc = copy_fields(s, D.U[s->parity], D.fs, N, state7, nullptr, true, src_is_device != 0))) return rc;
+    if (reg7) { if ((rc = copy_fields(s, D.R, D.fs, N, reg7, nullptr, true, src_is_device != 0))) return rc; }
+    else CK(cudaMemsetAsync(D.R, 0, (size_t)7 * D.fs * s->esz, s->stream));
+    s->sums_valid = false;
+    CK(cudaStreamSynchronize(s->stream));
+    return MPCF_OK;
+}
+
+int mpcf_get_state(mpcf_solver* s, int dom, void* const* state7, void* const* reg7, int dst_is_device)
+{
+    int rc = check_dom(s, dom);
+    if (rc) return rc;
+    DeviceGuard g(s->device);
+    DomDev& D = s->hdoms[dom];
+    const long long N = (long long)D.nx * D.ny * D.nz;
+    if (state7) { if ((rc = copy_fields(s, D.U[s->parity], D.fs, N, nullptr, state7, false, dst_is_device != 0))) return rc; }
+    if (reg7)   { if ((rc = copy_fields(s, D.R, D.fs, N, nullptr, reg7, false, dst_is_device != 0))) return rc; }
+    CK(cudaStreamSynchronize(s->stream));
+    return MPCF_OK;
+}
+
+int mpcf_device_pointers(mpcf_solver* s, int dom, void** state7, void** reg7)
+{
+    int rc = check_dom(s, dom);
+    if (rc) return rc;
+    DomDev& D = s->hdoms[dom];
+    for (int q = 0; q < 7; ++q)
+    {
+        if (state7) state7[q] = (char*)D.U[s->parity] + (size_t)q * D.fs * s->esz;
+        if (reg7)   reg7[q]   = (char*)D.R + (size_t)q * D.fs * s->esz;
+    }
+    return MPCF_OK;
+}
+
+int mpcf_max_sos(mpcf_solver* s, double* sos)
+{
+    if (!s) return fail(MPCF_ERR_ARG, "null solver");
+    DeviceGuard g(s->device);
+    int rc = enqueue_sos(s);
+    if (rc) return rc;
+    std::vector<char> buf(s->esz * s->ndom);
+    CK(cudaMemcpyAsync(buf.data(), s->sos_bits, buf.size(), cudaMemcpyDeviceToHost, s->stream));
+    CK(cudaMemsetAsync(s->sos_bits, 0, s->esz * s->ndom, s->stream));
+    CK(cudaStreamSynchronize(s->stream));
+    if (sos)
+        for (int d = 0; d < s->ndom; ++d)
+            sos[d] = s->esz == 8 ? ((double*)buf.data())[d] : (double)((float*)buf.data())[d];
+    return MPCF_OK;
+}
+
+int mpcf_stage(mpcf_solver* s, double a, double b, const double* dtinvh)
+{
+    if (!s) return fail(MPCF_ERR_ARG, "null solver");
+    DeviceGuard g(s->device);
+    if (dtinvh)
+    {
+        CK(cudaStreamSynchronize(s->stream));   // host staging buffer reuse
+        for (int d = 0; d < s->ndom; ++d)
+        {
+            if (s->esz == 8) ((double*)s->host_stage)[d] = dtinvh[d];
+            else ((float*)s->host_stage)[d] = (float)dtinvh[d];
+        }
+        CK(cudaMemcpyAsync(s->dtinvh, s->host_stage, s->esz * s->ndom, cudaMemcpyHostToDevice, s->stream));
+    }
+    int rc = enqueue_stage(s, a, b, false);
+    if (rc) return rc;
+    CK(cudaStreamSynchronize(s->stream));
+    return MPCF_OK;
+}
+
+int mpcf_compute_dt(mpcf_solver* s, double cfl, double dt_max, double* dt_out)
+{
+    if (!s) return fail(MPCF_ERR_ARG, "null solver");
+    if (!(cfl > 0) || !(dt_max > 0)) return fail(MPCF_ERR_ARG, "cfl and dt_max must be positive");
+    DeviceGuard g(s->device);
+    int rc;
+    if ((rc = enqueue_sos(s))) return rc;
+    if ((rc = enqueue_dt(s, cfl, dt_max))) return rc;
+    if (dt_out) CK(cudaMemcpyAsync(dt_out, s->dt, sizeof(double) * s->ndom, cudaMemcpyDeviceToHost, s->stream));
+    CK(cudaStreamSynchronize(s->stream));
+    return MPCF_OK;
+}
+
+int mpcf_step(mpcf_solver* s, double cfl, double dt_max, double* dt_out)
+{
+    if (!s) return fail(MPCF_ERR_ARG, "null solver");
+    if (!(cfl > 0) || !(dt_max > 0)) return fail(MPCF_ERR_ARG, "cfl and dt_max must be positive");
+    DeviceGuard g(s->device);
+    int rc = enqueue_step(s, cfl, dt_max);
+    if (rc) return rc;
+    if (dt_out)
+    {
+        CK(cudaMemcpyAsync(dt_out, s->dt, sizeof(double) * s->ndom, cudaMemcpyDeviceToHost, s->stream));
+        CK(cudaStreamSynchronize(s->stream));
+    }
+    return MPCF_OK;
+}
+
+int mpcf_run(mpcf_solver* s, int nsteps, double cfl, double dt_max, int use_graph, double* time_out)
+{
+    if (!s) return fail(MPCF_ERR_ARG, "null solver");
+    if (nsteps < 0) return fail(MPCF_ERR_ARG, "nsteps < 0");
+    if (!(cfl > 0) || !(dt_max > 0)) return fail(MPCF_ERR_ARG, "cfl and dt_max must be positive");
+    DeviceGuard g(s->device);
+    int rc;
+    if (use_graph)
+    {
+        if (s->graph_cfl != cfl || s->graph_dtmax != dt_max || s->graph_cons != s->track_cons) destroy_graphs(s);
+        for (int p = 0; p < 2; ++p)
+        {
+            if (s->graph[p]) continue;
+            const int saved = s->parity;
+            s->parity = p;
+            cudaGraph_t gr = nullptr;
+            CK(cudaStreamBeginCapture(s->stream, cudaStreamCaptureModeThreadLocal));
+            rc = enqueue_step(s, cfl, dt_max);
+            cudaError_t ec = cudaStreamEndCapture(s->stream, &gr);
+            s->parity = saved;
+            if (rc) { if (gr) cudaGraphDestroy(gr); return rc; }
+            if (ec != cudaSuccess) return fail(MPCF_ERR_CUDA, "graph capture failed: %s", cudaGetErrorString(ec));
+            ec = cudaGraphInstantiate(&s->graph[p], gr, 0);
+            cudaGraphDestroy(gr);
+            if (ec != cudaSuccess) { s->graph[p] = nullptr; return fail(MPCF_ERR_CUDA, "graph instantiate failed: %s", cudaGetErrorString(ec)); }
+        }
+        s->graph_cfl = cfl;
+        s->graph_dtmax = dt_max;
+        s->graph_cons = s->track_cons;
+        for (int n = 0; n < nsteps; ++n)
+        {
+            CK(cudaGraphLaunch(s->graph[s->parity], s->stream));
+            s->parity ^= 1;   // three stages: odd number of buffer swaps
+        }
+        if (nsteps > 0) s->sums_valid = s->track_cons;
+    }
+    else
+    {
+        for (int n = 0; n < nsteps; ++n)
+            if ((rc = enqueue_step(s, cfl, dt_max))) return rc;
+    }
+    if (time_out) CK(cudaMemcpyAsync(time_out, s->time, sizeof(double) * s->ndom, cudaMemcpyDeviceToHost, s->stream));
+    CK(cudaStreamSynchronize(s->stream));
+    return MPCF_OK;
+}
+
+int mpcf_synchronize(mpcf_solver* s)
+{
+    if (!s) return fail(MPCF_ERR_ARG, "null solver");
+    DeviceGuard g(s->device);
+    CK(cudaStreamSynchronize(s->stream));
+    return MPCF_OK;
+}
+
+int mpcf_set_track_conservation(mpcf_solver* s, int on)
+{
+    if (!s) return fail(MPCF_ERR_ARG, "null solver");
+    s->track_cons = on != 0;
+    return MPCF_OK;
+}
+
+int mpcf_conserved_sums(mpcf_solver* s, double* out)
+{
+    if (!s || !out) return fail(MPCF_ERR_ARG, "null argument");
+    DeviceGuard g(s->device);
+    if (!s->sums_valid)
+    {
+        // deterministic two-pass reduction of the current state
+        CK(launch_sum_state(s->ddoms, s->ndom, s->parity, s->nchunks, s->sos_chunk, s->esz == 8,
+                            s->chunk_sums, s->sums, s->stream));
+        s->sums_valid = true;
+    }
+    CK(cudaMemcpyAsync(out, s->sums, sizeof(double) * 5 * s->ndom, cudaMemcpyDeviceToHost, s->stream));
+    CK(cudaStreamSynchronize(s->stream));
+    return MPCF_OK;
+}
+
+int mpcf_error_word(mpcf_solver* s, unsigned* word, int clear)
+{
+    if (!s || !word) return fail(MPCF_ERR_ARG, "null argument");
+    DeviceGuard g(s->device);
+    CK(cudaMemcpyAsync(s->host_stage, s->err, sizeof(unsigned), cudaMemcpyDeviceToHost, s->stream));
+    if (clear) CK(cudaMemsetAsync(s->err, 0, sizeof(unsigned), s->stream));
+    CK(cudaStreamSynchronize(s->stream));
+    *word = *(unsigned*)s->host_stage;
+    return MPCF_OK;
+}
+
+int mpcf_set_bc(mpcf_solver* s, int dom, const int* bc6)
+{
+    int rc = check_dom(s, dom);
+    if (rc) return rc;
+    if (!bc6) return fail(MPCF_ERR_ARG, "null bc");
+    for (int f = 0; f < 6; ++f)
+        if (bc6[f] != MPCF_BC_ABSORBING && bc6[f] != MPCF_BC_REFLECTING)
+            return fail(MPCF_ERR_ARG, "unknown boundary condition %d on face %d", bc6[f], f);
+    DeviceGuard g(s->device);
+    for (int f = 0; f < 6; ++f) s->hdoms[dom].bc[f] = bc6[f];
+    CK(cudaMemcpyAsync(s->ddoms, s->hdoms.data(), sizeof(DomDev) * s->ndom, cudaMemcpyHostToDevice, s->stream));
+    CK(cudaStreamSynchronize(s->stream));
+    return MPCF_OK;
+}
+
+int mpcf_fill_ghosts(mpcf_solver* s, int dom, void* gx, void* gy, void* gz, int dst_is_device)
+{
+    int rc = check_dom(s, dom);
+    if (rc) return rc;
+    if (!gx || !gy || !gz) return fail(MPCF_ERR_ARG, "null ghost buffer");
+    DeviceGuard g(s->device);
+    DomDev& D = s->hdoms[dom];
+    const size_t sx = 2 * 7 * 3 * (size_t)D.ny * D.nz * s->esz;
+    const size_t sy = 2 * 7 * 3 * (size_t)D.nx * D.nz * s->esz;
+    const size_t sz = 2 * 7 * 3 * (size_t)D.nx * D.ny * s->esz;
+    void *dx = gx, *dy = gy, *dzp = gz;
+    void* tmp = nullptr;
+    if (!dst_is_device)
+    {
+        if (cudaMalloc(&tmp, sx + sy + sz) != cudaSuccess) { cudaGetLastError(); return fail(MPCF_ERR_NOMEM, "ghost scratch"); }
+        dx = tmp; dy = (char*)tmp + sx; dzp = (char*)tmp + sx + sy;
+    }
+    cudaError_t e = launch_fill_ghosts(s->esz == 8, s->ddoms + dom, s->parity, dx, dy, dzp, s->stream);
+    if (e == cudaSuccess && !dst_is_device)
+    {
+        e = cudaMemcpyAsync(gx, dx, sx, cudaMemcpyDeviceToHost, s->stream);
+        if (e == cudaSuccess) e = cudaMemcpyAsync(gy, dy, sy, cudaMemcpyDeviceToHost, s->stream);
+        if (e == cudaSuccess) e = cudaMemcpyAsync(gz, dzp, sz, cudaMemcpyDeviceToHost, s->stream);
+    }
+    cudaError_t e2 = cudaStreamSynchronize(s->stream);
+    if (tmp) cudaFree(tmp);
+    if (e != cudaSuccess) return fail(MPCF_ERR_CUDA, "ghost fill: %s", cudaGetErrorString(e));
+    if (e2 != cudaSuccess) return fail(MPCF_ERR_CUDA, "ghost fill: %s", cudaGetErrorString(e2));
+    return MPCF_OK;
+}
+
+int mpcf_ic_cloud(mpcf_solver* s, int dom, const mpcf_ic_params* p, int nbubbles, const double* bubbles4)
+{
+    int rc = check_dom(s, dom);
+    if (rc) return rc;
+    if (!p || nbubbles < 0 || (nbubbles > 0 && !bubbles4)) return fail(MPCF_ERR_ARG, "bad IC arguments");
+    DeviceGuard g(s->device);
+    if (nbubbles > s->bubbles_cap)
+    {
+        if (s->bubbles)
+        {
+            CK(cudaStreamSynchronize(s->stream));
+            cudaFree(s->bubbles);
+            s->allocs.erase(std::remove(s->allocs.begin(), s->allocs.end(), (void*)s->bubbles), s->allocs.end());
+            s->bubbles = nullptr;
+        }
+        if ((rc = dev_alloc(s, (void**)&s->bubbles, sizeof(double) * 4 * (size_t)nbubbles))) return rc;
+        s->bubbles_cap = nbubbles;
+    }
+    if (nbubbles > 0) CK(cudaMemcpyAsync(s->bubbles, bubbles4, sizeof(double) * 4 * nbubbles, cudaMemcpyHostToDevice, s->stream));
+    IcParams P;
+    memcpy(&P, p, sizeof(P));
+    CK(launch_ic_cloud(s->esz == 8, s->ddoms + dom, s->parity, P, s->bubbles, nbubbles, s->stream));
+    s->sums_valid = false;
+    CK(cudaStreamSynchronize(s->stream));
+    return MPCF_OK;
+}
+
+int mpcf_ic_cloud_host(int nx, int ny, int nz, const mpcf_ic_params* p, int nbubbles,
+                       const double* bubbles4, int elem_size, void* const* out7)
+{
+    if (nx < 1 || ny < 1 || nz < 1 || !p || !out7 || nbubbles < 0 || (nbubbles > 0 && !bubbles4))
+        return fail(MPCF_ERR_ARG, "bad IC arguments");
+    if (elem_size != 4 && elem_size != 8) return fail(MPCF_ERR_ARG, "elem_size must be 4 or 8");
+    for (int q = 0; q < 7; ++q) if (!out7[q]) return fail(MPCF_ERR_ARG, "null output field %d", q);
+    IcParams P;
+    memcpy(&P, p, sizeof(P));
+    const double h = 1.0 / (double)std::max(nx, std::max(ny, nz));
+    const long long N = (long long)nx * ny * nz;
+    for (long long i = 0; i < N; ++i)
+    {
+        const int ix = (int)(i % nx), iy = (int)((i / nx) % ny), iz = (int)(i / ((long long)nx * ny));
+        double c[7];
+        ic_cell(P, bubbles4, nbubbles, h, ix, iy, iz, (unsigned long long)i, c);
+        for (int q = 0; q < 7; ++q)
+        {
+            if (elem_size == 8) ((double*)out7[q])[i] = c[q];
+            else ((float*)out7[q])[i] = (float)c[q];
+        }
+    }
+    return MPCF_OK;
+}
+
+int mpcf_bubbles(unsigned long long seed, int n, double rmin, double rmax,
+                 const double* lo3, const double* hi3, double gap, int max_tries, double* out4)
+{
+    if (n < 0 || !lo3 || !hi3 || (n > 0 && !out4) || !(rmin > 0) || rmax < rmin)
+        return fail(MPCF_ERR_ARG, "bad bubble arguments");
+    std::mt19937_64 rng(seed);
+    // explicit 53-bit uniforms: independent of the standard library's
+    // distribution implementations
+    auto uni = [&](double a, double b) { return a + (b - a) * ((double)(rng() >> 11) * (1.0 / 9007199254740992.0)); };
+    int placed = 0;
+    const int tries = max_tries > 0 ? max_tries : 100000;
+    for (int t = 0; t < tries && placed < n; ++t)
+    {
+        const double x = uni(lo3[0], hi3[0]), y = uni(lo3[1], hi3[1]), z = uni(lo3[2], hi3[2]);
+        const double r = uni(rmin, rmax);
+        bool ok = true;
+        for (int k = 0; k < placed && ok; ++k)
+        {
+            const double dx = x - out4[4 * k], dy = y - out4[4 * k + 1], dz = z - out4[4 * k + 2];
+            ok = std::sqrt(dx * dx + dy * dy + dz * dz) >= r + out4[4 * k + 3] + gap;
+        }
+        if (!ok) continue;
+        out4[4 * placed] = x; out4[4 * placed + 1] = y; out4[4 * placed + 2] = z; out4[4 * placed + 3] = r;
+        ++placed;
+    }
+    return placed;
+}
+
+int mpcf_set_tiling(mpcf_solver* s, int ty, int dz, int persistent)
+{
+    if (!s) return fail(MPCF_ERR_ARG, "null solver");
+    if (!valid_ty(s, ty)) return fail(MPCF_ERR_ARG, "unsupported tile height ty=%d for this precision", ty);
+    if (dz < 1) return fail(MPCF_ERR_ARG, "dz must be >= 1");
+    DeviceGuard g(s->device);
+    s->ty = ty;
+    s->dz = dz;
+    s->persist = persistent != 0;
+    return apply_tiling(s);
+}
+
+int mpcf_get_tiling(const mpcf_solver* s, int* ty, int* dz, int* persistent)
+{
+    if (!s) return fail(MPCF_ERR_ARG, "null solver");
+    if (ty) *ty = s->ty;
+    if (dz) *dz = s->dz;
+    if (persistent) *persistent = s->persist;
+    return MPCF_OK;
+}
+
+int mpcf_launch_shape(const mpcf_solver* s, long long* ntiles, long long* grid, int* threads)
+{
+    if (!s) return fail(MPCF_ERR_ARG, "null solver");
+    if (ntiles) *ntiles = s->ntiles;
+    if (grid) *grid = s->persist ? persistent_grid(const_cast<mpcf_solver*>(s), s->ty) : s->ntiles;
+    if (threads) *threads = 32 * s->ty;
+    return MPCF_OK;
+}
+
+int mpcf_time_stages(mpcf_solver* s, int reps, double dtinvh, double* ms_per_stage)
+{
+    if (!s || reps < 1) return fail(MPCF_ERR_ARG, "bad arguments");
+    DeviceGuard g(s->device);
+    std::vector<double> dv(s->ndom, dtinvh);
+    CK(cudaStreamSynchronize(s->stream));
+    for (int d = 0; d < s->ndom; ++d)
+    {
+        if (s->esz == 8) ((double*)s->host_stage)[d] = dtinvh;
+        else ((float*)s->host_stage)[d] = (float)dtinvh;
+    }
+    CK(cudaMemcpyAsync(s->dtinvh, s->host_stage, s->esz * s->ndom, cudaMemcpyHostToDevice, s->stream));
+    cudaEvent_t e0, e1;
+    CK(cudaEventCreate(&e0));
+    CK(cudaEventCreate(&e1));
+    int rc = MPCF_OK;
+    CK(cudaEventRecord(e0, s->stream));
+    for (int r = 0; r < reps && !rc; ++r) rc = enqueue_stage(s, kLSRK3[r % 3][0], kLSRK3[r % 3][1], false);
+    CK(cudaEventRecord(e1, s->stream));
+    CK(cudaEventSynchronize(e1));
+    float ms = 0;
+    cudaEventElapsedTime(&ms, e0, e1);
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (rc) return rc;
+    if (ms_per_stage) *ms_per_stage = ms / reps;
+    return MPCF_OK;
+}
+
+int mpcf_autotune(mpcf_solver* s, int reps, int* best3, double* best_ms)
+{
+    if (!s) return fail(MPCF_ERR_ARG, "null solver");
+    if (reps < 1) reps = 3;
+    DeviceGuard g(s->device);
+    CK(cudaStreamSynchronize(s->stream));
+    // Trials read the current state and write the other state buffer; the
+    // register is redirected to a scratch copy so the solver's state is
+    // unchanged afterwards.
+    std::vector<void*> saved_R(s->ndom);
+    std::vector<void*> scratch(s->ndom, nullptr);
+    int rc = MPCF_OK;
+    for (int d = 0; d < s->ndom && !rc; ++d)
+    {
+        DomDev& D = s->hdoms[d];
+        const size_t bytes = (size_t)7 * D.fs * s->esz;
+        if (cudaMalloc(&scratch[d], bytes) != cudaSuccess) { cudaGetLastError(); rc = fail(MPCF_ERR_NOMEM, "autotune scratch"); break; }
+        saved_R[d] = D.R;
+    }
+    const int saved_ty = s->ty, saved_dz = s->dz, saved_p = s->persist, saved_parity = s->parity;
+    std::vector<char> saved_dtinvh(s->esz * s->ndom);
+    CK(cudaMemcpy(saved_dtinvh.data(), s->dtinvh, saved_dtinvh.size(), cudaMemcpyDeviceToHost));
+    int bty = saved_ty, bdz = saved_dz, bp = saved_p;
+    double bms = 1e300;
+    if (!rc)
+    {
+        int maxn = 0;
+        for (auto& D : s->hdoms) maxn = std::max(maxn, D.nz);
+        std::vector<int> dzs = {16, 32, 64, 128};
+        dzs.push_back(maxn);
+        const int tys[4] = {2, 4, 8, 16};
+        for (int i = 0; i < 4 && !rc; ++i)
+        {
+            if (!valid_ty(s, tys[i])) continue;
+            for (int dz : dzs)
+            {
+                if (dz > maxn && dz != maxn) continue;
+                for (int p = 0; p < 2 && !rc; ++p)
+                {
+                    s->ty = tys[i]; s->dz = dz; s->persist = p;
+                    for (int d = 0; d < s->ndom; ++d)
+                    {
+                        s->hdoms[d].R = scratch[d];
+                        cudaMemcpyAsync(scratch[d], saved_R[d], (size_t)7 * s->hdoms[d].fs * s->esz, cudaMemcpyDeviceToDevice, s->stream);
+                    }
+                    if ((rc = apply_tiling(s))) break;
+                    double ms = 0;
+                    // one warm-up launch, then the timed ones; parity is reset
+                    // so every trial reads the same state
+                    s->parity = saved_parity;
+                    if ((rc = mpcf_time_stages(s, 1, 0.0, &ms))) break;
+                    s->parity = saved_parity;
+                    double tot = 0;
+                    for (int r = 0; r < reps && !rc; ++r)
+                    {
+                        rc = mpcf_time_stages(s, 1, 0.0, &ms);
+                        s->parity = saved_parity;
+                        tot += ms;
+                    }
+                    if (!rc && tot / reps < bms) { bms = tot / reps; bty = tys[i]; bdz = dz; bp = p; }
+                }
+            }
+        }
+    }
+    for (int d = 0; d < s->ndom; ++d) if (saved_R[d]) s->hdoms[d].R = saved_R[d];
+    s->parity = saved_parity;
+    s->ty = rc ? saved_ty : bty;
+    s->dz = rc ? saved_dz : bdz;
+    s->persist = rc ? saved_p : bp;
+    int rc2 = apply_tiling(s);
+    for (void* p : scratch) if (p) cudaFree(p);
+    if (cudaMemcpy(s->dtinvh, saved_dtinvh.data(), saved_dtinvh.size(), cudaMemcpyHostToDevice) != cudaSuccess && !rc2)
+        rc2 = fail(MPCF_ERR_CUDA, "restoring dt/h after autotune failed");
+    if (rc) return rc;
+    if (rc2) return rc2;
+    if (best3) { best3[0] = s->ty; best3[1] = s->dz; best3[2] = s->persist; }
+    if (best_ms) *best_ms = bms;
+    return MPCF_OK;
+}
+
+int mpcf_probe_fp32_peak(int device, double* tflops)
+{
+    if (!tflops) return fail(MPCF_ERR_ARG, "null output");
+    DeviceGuard g(device);
+    int sms = 0;
+    CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device));
+    float* out = nullptr;
+    CK(cudaMalloc(&out, 16));
+    cudaEvent_t e0, e1;
+    CK(cudaEventCreate(&e0));
+    CK(cudaEventCreate(&e1));
+    const int blocks = sms * 8, iters = 4096;
+    double best = 0;
+    for (int r = 0; r < 4; ++r)
+    {
+        CK(cudaEventRecord(e0, 0));
+        CK(launch_fma_probe(blocks, iters, out, 0));
+        CK(cudaEventRecord(e1, 0));
+        CK(cudaEventSynchronize(e1));
+        float ms = 0;
+        cudaEventElapsedTime(&ms, e0, e1);
+        // 8 chains x 16 FMA x iters per thread, 2 flops per FMA
+        const double flops = 2.0 * 8 * 16 * (double)iters * 256.0 * blocks;
+        if (r > 0) best = std::max(best, flops / (ms * 1e-3) / 1e12);
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    cudaFree(out);
+    *tflops = best;
+    return MPCF_OK;
+}
+
+int mpcf_time_run(mpcf_solver* s, int nsteps, double cfl, double dt_max, double* ms)
+{
+    if (!s || nsteps < 1 || !ms) return fail(MPCF_ERR_ARG, "bad arguments");
+    DeviceGuard g(s->device);
+    int rc = mpcf_run(s, 0, cfl, dt_max, 1, nullptr);   // builds the graphs
+    if (rc) return rc;
+    cudaEvent_t e0, e1;
+    CK(cudaEventCreate(&e0));
+    CK(cudaEventCreate(&e1));
+    CK(cudaEventRecord(e0, s->stream));
+    for (int n = 0; n < nsteps; ++n)
+    {
+        CK(cudaGraphLaunch(s->graph[s->parity], s->stream));
+        s->parity ^= 1;
+    }
+    CK(cudaEventRecord(e1, s->stream));
+    CK(cudaEventSynchronize(e1));
+    float t = 0;
+    cudaEventElapsedTime(&t, e0, e1);
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    s->sums_valid = s->track_cons;
+    *ms = t;
+    return MPCF_OK;
+}
+
+} // extern "C"

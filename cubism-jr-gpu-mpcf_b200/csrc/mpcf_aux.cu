@@ -1,0 +1,338 @@
+// mpcf_aux.cu -- the small kernels around the stage: maximum speed of sound
+// (CFL reduction), on-device dt, deterministic FP64 conservation sums, the
+// bubble-cloud initial condition and an explicit ghost-buffer fill.
+#include <cuda_runtime.h>
+#include <math.h>
+#include "mpcf_math.cuh"
+#include "mpcf_stage.cuh"
+#include "mpcf_launch.h"
+#include "mpcf_ic.h"
+
+namespace mpcf {
+
+// ---------------------------------------------------------------------------
+// Maximum speed of sound.  Per cell (reference formula, GPUkernels.cu:1207-1209):
+//   p = (E - (U*U + V*V + W*W)*(0.5f/rho) - P) / G        (U,V,W momenta)
+//   c = sqrt(((p + P)/G + p)/rho)
+//   s = c + max(|U|,|V|,|W|)/rho
+// The mixed policy evaluates p in FP64.  Reduction: warp shuffle, block max
+// through shared memory, one atomicMax per block on the bit pattern (all
+// values are >= 0, so the unsigned order of the bits is the float order; a
+// NaN compares above every finite value and surfaces as the result).
+// ---------------------------------------------------------------------------
+template <class Pol>
+__device__ __forceinline__ typename Pol::T cell_sos(const typename Pol::T r, const typename Pol::T u,
+        const typename Pol::T v, const typename Pol::T w, const typename Pol::T e,
+        const typename Pol::T G, const typename Pol::T P)
+{
+    typedef typename Pol::T T;
+    T p;
+    if (Pol::kP64)
+        p = (T)(((double)e - ((double)u*(double)u + (double)v*(double)v + (double)w*(double)w)*(0.5/(double)r) - (double)P) / (double)G);
+    else
+        p = (e - (u*u + v*v + w*w)*((T)0.5f/r) - P) / G;
+    const T c = dsqrt(((p + P) / G + p) / r);
+    return c + dmax(dmax(fabs(u), fabs(v)), fabs(w)) / r;
+}
+
+__device__ __forceinline__ void atomic_max_bits(void* p, float v)
+{
+    atomicMax((unsigned*)p, __float_as_uint(v));
+}
+__device__ __forceinline__ void atomic_max_bits(void* p, double v)
+{
+    atomicMax((unsigned long long*)p, (unsigned long long)__double_as_longlong(v));
+}
+__device__ __forceinline__ float  shfl_max(float v)  { for (int o = 16; o > 0; o >>= 1) v = fmaxf(v, __shfl_xor_sync(0xffffffffu, v, o)); return v; }
+__device__ __forceinline__ double shfl_max(double v) { for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o)); return v; }
+
+template <class Pol>
+__global__ void __launch_bounds__(256) sos_kernel(const SosArgs A)
+{
+    typedef typename Pol::T T;
+    __shared__ T wmax[8];
+    const int c = blockIdx.x;
+    int d = 0;
+    while (d + 1 < A.ndom && A.doms[d + 1].sos_chunk_begin <= c) ++d;
+    const DomDev& D = A.doms[d];
+    const long long N = (long long)D.nx * D.ny * D.nz;
+    const long long beg = (long long)(c - D.sos_chunk_begin) * A.chunk;
+    const long long end = min(beg + (long long)A.chunk, N);
+    const T* __restrict__ U = (const T*)D.U[A.parity];
+    const long long fs = D.fs;
+
+    T s = (T)0;
+    bool bad = false;
+    for (long long i = beg + threadIdx.x; i < end; i += blockDim.x)
+    {
+        const T v = cell_sos<Pol>(__ldg(U + i), __ldg(U + fs + i), __ldg(U + 2 * fs + i), __ldg(U + 3 * fs + i),
+                                  __ldg(U + 4 * fs + i), __ldg(U + 5 * fs + i), __ldg(U + 6 * fs + i));
+        bad = bad || !(v >= (T)0);   // NaN (fmax would drop it) or negative
+        s = dmax(s, v);
+    }
+    bad = __syncthreads_or(bad);
+    s = shfl_max(s);
+    if ((threadIdx.x & 31) == 0) wmax[threadIdx.x >> 5] = s;
+    __syncthreads();
+    if (threadIdx.x < 32)
+    {
+        T m = threadIdx.x < (blockDim.x >> 5) ? wmax[threadIdx.x] : (T)0;
+        m = shfl_max(m);
+        // a NaN's bit pattern orders above every finite non-negative value,
+        // so it wins the atomic maximum and reaches the dt kernel
+        if (threadIdx.x == 0) atomic_max_bits((char*)A.sos_bits + d * sizeof(T), bad ? (T)NAN : m);
+    }
+}
+
+// dt = min(CFL*h/sos, dt_max), dt/h rounded to the stage type
+// (LSRK3_IntegratorMPI.cpp:37-38, process_all(.., dt/h) converts to Real).
+// The sound-speed accumulator is cleared for the next reduction.
+template <class Pol>
+__global__ void dt_kernel(const DtArgs A)
+{
+    typedef typename Pol::T T;
+    const int d = blockIdx.x * blockDim.x + threadIdx.x;
+    if (d >= A.ndom) return;
+    T* bits = (T*)A.sos_bits;
+    const T sos = bits[d];
+    const double h = A.doms[d].h;
+    double dt = A.cfl*h/sos;
+    dt = A.dt_max < dt ? A.dt_max : dt;
+    if (!(sos > (T)0) || !(dt == dt) || isinf(dt))
+    {
+        atomicOr(A.err, (unsigned)ERRBIT_SOS_NONFINITE);
+        dt = 0.0;   // freeze the domain rather than advance it with garbage
+    }
+    ((T*)A.dtinvh)[d] = (T)(dt/h);
+    A.dt[d] = dt;
+    A.time[d] += dt;
+    bits[d] = (T)0;
+}
+
+cudaError_t launch_sos(int pol, const SosArgs& A, cudaStream_t st)
+{
+    switch (pol)
+    {
+        case 0: sos_kernel<PolRef32><<<A.nchunks, 256, 0, st>>>(A); break;
+        case 1: sos_kernel<PolFast32><<<A.nchunks, 256, 0, st>>>(A); break;
+        case 2: sos_kernel<PolMixed><<<A.nchunks, 256, 0, st>>>(A); break;
+        case 3: sos_kernel<PolFP64><<<A.nchunks, 256, 0, st>>>(A); break;
+        default: return cudaErrorInvalidValue;
+    }
+    return cudaGetLastError();
+}
+
+cudaError_t launch_dt(int pol, const DtArgs& A, cudaStream_t st)
+{
+    const int g = (A.ndom + 63) / 64;
+    switch (pol)
+    {
+        case 0: dt_kernel<PolRef32><<<g, 64, 0, st>>>(A); break;
+        case 1: dt_kernel<PolFast32><<<g, 64, 0, st>>>(A); break;
+        case 2: dt_kernel<PolMixed><<<g, 64, 0, st>>>(A); break;
+        case 3: dt_kernel<PolFP64><<<g, 64, 0, st>>>(A); break;
+        default: return cudaErrorInvalidValue;
+    }
+    return cudaGetLastError();
+}
+
+// Per-domain totals of the per-tile FP64 partial sums, in tile order
+// (deterministic, independent of scheduling).
+__global__ void sum_tiles_kernel(const DomDev* doms, const double* tile_sums, double* out)
+{
+    const int d = blockIdx.x;
+    const int m = threadIdx.x;
+    if (m >= 5) return;
+    const int b = doms[d].tile_begin;
+    const int n = doms[d].tiles_x * doms[d].tiles_y * doms[d].tiles_z;
+    double s = 0;
+    for (int t = 0; t < n; ++t) s += tile_sums[(long long)(b + t) * 5 + m];
+    out[d * 5 + m] = s;
+}
+
+cudaError_t launch_sum_tiles(const DomDev* doms, int ndom, const double* tile_sums, double* out, cudaStream_t st)
+{
+    sum_tiles_kernel<<<ndom, 32, 0, st>>>(doms, tile_sums, out);
+    return cudaGetLastError();
+}
+
+// ---------------------------------------------------------------------------
+// Bubble-cloud initial condition (formula in mpcf_ic.h), one thread per cell,
+// grid-stride; the register is cleared.
+// ---------------------------------------------------------------------------
+template <class T>
+__global__ void ic_cloud_kernel(const DomDev* dom, int parity, const IcParams P,
+                                const double* __restrict__ bub, int nb)
+{
+    const DomDev& D = *dom;
+    const long long N = (long long)D.nx * D.ny * D.nz;
+    T* U = (T*)D.U[parity];
+    T* R = (T*)D.R;
+    const long long fs = D.fs;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < N; i += (long long)gridDim.x * blockDim.x)
+    {
+        const int ix = (int)(i % D.nx);
+        const int iy = (int)((i / D.nx) % D.ny);
+        const int iz = (int)(i / ((long long)D.nx * D.ny));
+        double c[7];
+        ic_cell(P, bub, nb, D.h, ix, iy, iz, (unsigned long long)i, c);
+        for (int m = 0; m < 7; ++m) { U[m * fs + i] = (T)c[m]; R[m * fs + i] = (T)0; }
+    }
+}
+
+cudaError_t launch_ic_cloud(int is_double, const DomDev* dom, int parity, const IcParams& P,
+                            const double* bubbles, int nbubbles, cudaStream_t st)
+{
+    if (is_double) ic_cloud_kernel<double><<<148 * 16, 256, 0, st>>>(dom, parity, P, bubbles, nbubbles);
+    else           ic_cloud_kernel<float><<<148 * 16, 256, 0, st>>>(dom, parity, P, bubbles, nbubbles);
+    return cudaGetLastError();
+}
+
+// ---------------------------------------------------------------------------
+// Explicit ghost buffers in the reference layouts, from the same boundary
+// map the stage kernel applies on the fly:
+//   gx[side][q][GHOSTMAPX(ix,iy,iz)]  = ix + 3*(iy + NY*iz),     ix 0..2
+//   gy[side][q][GHOSTMAPY(ix,iy,iz)]  = ix + NX*(iy + 3*iz),     iy 0..2
+//   gz[side][q][ID3(ix,iy,iz,NX,NY)],                             iz 0..2
+// left side: layer 0 = outermost cell (-3); right side: layer 0 = cell N
+// (Types.h:42-43, BoundaryConditions.h:60-109, GPUlab.h:69-91).
+// ---------------------------------------------------------------------------
+template <class T>
+__global__ void fill_ghosts_kernel(const DomDev* dom, int parity, T* gx, T* gy, T* gz)
+{
+    const DomDev& DD = *dom;
+    DomRegs D;
+    D.nx = DD.nx; D.ny = DD.ny; D.nz = DD.nz;
+    D.bc0 = DD.bc[0]; D.bc1 = DD.bc[1]; D.bc2 = DD.bc[2];
+    D.bc3 = DD.bc[3]; D.bc4 = DD.bc[4]; D.bc5 = DD.bc[5];
+    D.fs = DD.fs;
+    const T* U = (const T*)DD.U[parity];
+    const long long sx = 3LL * D.ny * D.nz, sy = 3LL * D.nx * D.nz, sz = 3LL * D.nx * D.ny;
+    const long long total = 2 * (sx + sy + sz);
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < total; i += (long long)gridDim.x * blockDim.x)
+    {
+        int ix, iy, iz, dir, side;
+        long long o = i, li;
+        if (o < 2 * sx)          { dir = 0; side = (int)(o / sx); li = o % sx; ix = (int)(li % 3); iy = (int)((li / 3) % D.ny); iz = (int)(li / (3LL * D.ny)); }
+        else if ((o -= 2 * sx) < 2 * sy) { dir = 1; side = (int)(o / sy); li = o % sy; ix = (int)(li % D.nx); iy = (int)((li / D.nx) % 3); iz = (int)(li / (3LL * D.nx)); }
+        else { o -= 2 * sy; dir = 2; side = (int)(o / sz); li = o % sz; ix = (int)(li % D.nx); iy = (int)((li / D.nx) % D.ny); iz = (int)(li / ((long long)D.nx * D.ny)); }
+        // ghost layer -> cell coordinate outside the domain
+        int cx = ix, cy = iy, cz = iz;
+        if (dir == 0) cx = side == 0 ? ix - 3 : D.nx + ix;
+        if (dir == 1) cy = side == 0 ? iy - 3 : D.ny + iy;
+        if (dir == 2) cz = side == 0 ? iz - 3 : D.nz + iz;
+        bool fx, fy, fz;
+        const int mx = bc_map(cx, D.nx, D.bc0, D.bc1, fx);
+        const int my = bc_map(cy, D.ny, D.bc2, D.bc3, fy);
+        const int mz = bc_map(cz, D.nz, D.bc4, D.bc5, fz);
+        const long long idx = (long long)mx + (long long)D.nx * ((long long)my + (long long)D.ny * mz);
+        T* dst = dir == 0 ? gx : (dir == 1 ? gy : gz);
+        const long long s = dir == 0 ? sx : (dir == 1 ? sy : sz);
+        for (int q = 0; q < 7; ++q)
+        {
+            T v = U[q * D.fs + idx];
+            if ((q == 1 && fx) || (q == 2 && fy) || (q == 3 && fz)) v = -v;
+            dst[(side * 7 + q) * s + li] = v;
+        }
+    }
+}
+
+cudaError_t launch_fill_ghosts(int is_double, const DomDev* dom, int parity,
+                               void* gx, void* gy, void* gz, cudaStream_t st)
+{
+    if (is_double) fill_ghosts_kernel<double><<<148 * 4, 256, 0, st>>>(dom, parity, (double*)gx, (double*)gy, (double*)gz);
+    else           fill_ghosts_kernel<float><<<148 * 4, 256, 0, st>>>(dom, parity, (float*)gx, (float*)gy, (float*)gz);
+    return cudaGetLastError();
+}
+
+__global__ void zero_kernel(unsigned* p, size_t n)
+{
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) p[i] = 0u;
+}
+
+cudaError_t launch_zero(void* p, size_t bytes, cudaStream_t st)
+{
+    const size_t n = bytes / 4;
+    const int g = (int)((n + 255) / 256 < 1024 ? (n + 255) / 256 : 1024);
+    zero_kernel<<<g > 0 ? g : 1, 256, 0, st>>>((unsigned*)p, n);
+    return cudaGetLastError();
+}
+
+// FP64 sums of (rho, rho u, rho v, rho w, E) of the current state: one block
+// per chunk (same chunking as the sound-speed reduction) writes its partials,
+// then the per-domain totals are summed in chunk order.  Fixed block size and
+// fixed reduction trees make the result independent of scheduling.
+template <class T>
+__global__ void __launch_bounds__(256) sum_state_kernel(const DomDev* doms, int ndom, int parity, int chunk, double* partial)
+{
+    __shared__ double red[5][256];
+    const int c = blockIdx.x;
+    int d = 0;
+    while (d + 1 < ndom && doms[d + 1].sos_chunk_begin <= c) ++d;
+    const DomDev& D = doms[d];
+    const long long N = (long long)D.nx * D.ny * D.nz;
+    const long long beg = (long long)(c - D.sos_chunk_begin) * chunk;
+    const long long end = min(beg + (long long)chunk, N);
+    const T* U = (const T*)D.U[parity];
+    double acc[5] = {0, 0, 0, 0, 0};
+    for (long long i = beg + threadIdx.x; i < end; i += 256)
+        for (int m = 0; m < 5; ++m) acc[m] += (double)U[m * D.fs + i];
+    for (int m = 0; m < 5; ++m) red[m][threadIdx.x] = acc[m];
+    __syncthreads();
+    for (int w = 128; w > 0; w >>= 1)
+    {
+        if ((int)threadIdx.x < w)
+            for (int m = 0; m < 5; ++m) red[m][threadIdx.x] += red[m][threadIdx.x + w];
+        __syncthreads();
+    }
+    if (threadIdx.x < 5) partial[(long long)c * 5 + threadIdx.x] = red[threadIdx.x][0];
+}
+
+__global__ void sum_chunks_kernel(const DomDev* doms, const double* partial, double* out)
+{
+    const int d = blockIdx.x;
+    const int m = threadIdx.x;
+    if (m >= 5) return;
+    double s = 0;
+    for (int c = 0; c < doms[d].sos_chunks; ++c) s += partial[(long long)(doms[d].sos_chunk_begin + c) * 5 + m];
+    out[d * 5 + m] = s;
+}
+
+cudaError_t launch_sum_state(const DomDev* doms, int ndom, int parity, int nchunks, int chunk, int is_double,
+                             double* chunk_sums, double* out, cudaStream_t st)
+{
+    if (is_double) sum_state_kernel<double><<<nchunks, 256, 0, st>>>(doms, ndom, parity, chunk, chunk_sums);
+    else           sum_state_kernel<float><<<nchunks, 256, 0, st>>>(doms, ndom, parity, chunk, chunk_sums);
+    sum_chunks_kernel<<<ndom, 32, 0, st>>>(doms, chunk_sums, out);
+    return cudaGetLastError();
+}
+
+// ---------------------------------------------------------------------------
+// FP32 pipe probe: independent FMA chains, 8 per thread, enough warps to
+// saturate every SM.  Used to measure the CUDA-core FP32 peak that bounds
+// the stage kernel (no such figure is provided by the platform).
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(256) fma_probe_kernel(float* out, int iters, float seed)
+{
+    float a0 = seed + threadIdx.x, a1 = a0 + 1, a2 = a0 + 2, a3 = a0 + 3, a4 = a0 + 4, a5 = a0 + 5, a6 = a0 + 6, a7 = a0 + 7;
+    const float m = 0.999999f, c = 1e-7f;
+    for (int i = 0; i < iters; ++i)
+    {
+#pragma unroll
+        for (int k = 0; k < 16; ++k)
+        {
+            a0 = fmaf(a0, m, c); a1 = fmaf(a1, m, c); a2 = fmaf(a2, m, c); a3 = fmaf(a3, m, c);
+            a4 = fmaf(a4, m, c); a5 = fmaf(a5, m, c); a6 = fmaf(a6, m, c); a7 = fmaf(a7, m, c);
+        }
+    }
+    const float r = a0 + a1 + a2 + a3 + a4 + a5 + a6 + a7;
+    if (r == 12345.678f) out[0] = r;   // keeps the chains alive
+}
+
+cudaError_t launch_fma_probe(int blocks, int iters, float* out, cudaStream_t st)
+{
+    fma_probe_kernel<<<blocks, 256, 0, st>>>(out, iters, 1.0f);
+    return cudaGetLastError();
+}
+
+} // namespace mpcf

@@ -1,0 +1,35 @@
+// mpcf_launch.h -- internal launch interface between the host runtime and
+// the kernel translation units (not part of the public C ABI).
+#pragma once
+
+#include <cuda_runtime.h>
+#include "mpcf_types.h"
+
+namespace mpcf {
+
+struct StageKernelInfo
+{
+    const void* fn;     // kernel entry (for occupancy queries / attributes)
+    size_t smem;        // dynamic shared memory per CTA
+};
+
+// precision policy ids: 0 FP32 reference rounding, 1 fast FP32, 2 mixed, 3 FP64
+cudaError_t launch_stage_ref(int ty, bool persist, const StageArgs& A, int grid, cudaStream_t st);
+cudaError_t launch_stage_fast(int pol, int ty, bool persist, const StageArgs& A, int grid, cudaStream_t st);
+StageKernelInfo stage_info_ref(int ty, bool persist);
+StageKernelInfo stage_info_fast(int pol, int ty, bool persist);
+
+// mpcf_aux.cu
+cudaError_t launch_sos(int pol, const SosArgs& A, cudaStream_t st);
+cudaError_t launch_dt(int pol, const DtArgs& A, cudaStream_t st);
+cudaError_t launch_sum_tiles(const DomDev* doms, int ndom, const double* tile_sums, double* out, cudaStream_t st);
+cudaError_t launch_ic_cloud(int is_double, const DomDev* dom, int parity, const IcParams& P,
+                            const double* bubbles, int nbubbles, cudaStream_t st);
+cudaError_t launch_fill_ghosts(int is_double, const DomDev* dom, int parity,
+                               void* gx, void* gy, void* gz, cudaStream_t st);
+cudaError_t launch_zero(void* p, size_t bytes, cudaStream_t st);
+cudaError_t launch_fma_probe(int blocks, int iters, float* out, cudaStream_t st);
+cudaError_t launch_sum_state(const DomDev* doms, int ndom, int parity, int nchunks, int chunk, int is_double,
+                             double* chunk_sums, double* out, cudaStream_t st);
+
+} // namespace mpcf

@@ -1,0 +1,353 @@
+// mpcf_stage.cuh -- the fused LSRK3 stage kernel.
+//
+// One launch advances every cell of every domain through one low-storage
+// RK stage: ghost synthesis from the boundary conditions, WENO5/HLLC face
+// fluxes in x, y and z, the non-conservative G/P extra terms, the flux
+// divergence with the register update, and the state update.  It replaces
+// the reference chain
+//   _apply_bc (host) -> _xflux/_xextraterm_hllc -> _yflux/_yextraterm_hllc
+//   -> _zflux/_zextraterm_hllc -> _divergence -> _update
+// (BoundaryConditions.h:60-109, GPUkernels.cu:35-1179) and its per-stage
+// PCIe streaming (GPUlab.cpp:202-372,703-793); all state stays in HBM.
+//
+// Work decomposition.  A tile is 32 x TY columns in x-y and a z-chunk of
+// depth dz.  A CTA has 32*TY threads, one per column; warp w owns row w.
+// The CTA marches up the chunk one slab at a time:
+//   * a 6-slab ring of primitives (rho,u,v,w,p,G,P) of the tile's own
+//     columns lives in shared memory (z-stencil of the z faces);
+//   * slab k with its 3-cell x/y halo is staged in `cur` (x/y stencils);
+//   * every thread evaluates the x face at its left, the y face below it
+//     and the z face below it; warp 0 adds the y faces of the row above the
+//     tile, warp 1 the x faces right of the tile (32 + TY extra faces);
+//   * x/y face results go through shared memory, the z face result stays
+//     in registers for the next slab, and the cell below is finalised:
+//     rhs = a*R - dtinvh*div(F) (with the G/P extra terms), R <- rhs,
+//     U_next <- b*rhs + U.
+// Each cell is converted to primitives once per stage (the reference
+// converts the six stencil cells again at every face).  The state is
+// ping-ponged (read U[parity], write U[parity^1]) so neighbouring tiles
+// always see the old state.
+//
+// DRAM traffic per cell-stage: read U (7 T) + read R (7 T) + write R and
+// U_next (14 T) = 112 B in FP32.  Halo and ring re-reads hit L2.
+#pragma once
+
+#include "mpcf_math.cuh"
+#include "mpcf_types.h"
+
+namespace mpcf {
+
+constexpr int kTX = 32;
+
+template <class T, int TY>
+struct StageSmem
+{
+    T zwin[6][7][TY][kTX];          // ring of the tile's own columns
+    T cur[7][TY + 6][kTX + 6];      // slab k with 3-cell x/y halos
+    T fx[12][TY][kTX + 1];          // x faces of slab k
+    T fy[12][TY + 1][kTX];          // y faces of slab k
+    double red[TY][5];              // block reduction of conservation sums
+    int tile;
+};
+
+// Boundary-condition map of one coordinate: absorbing clamps to the edge
+// cell, reflecting mirrors (-1-i on the left, 2n-1-i on the right) and
+// flips the sign of the normal momentum (BoundaryConditions.h:60-109).
+__device__ __forceinline__ int bc_map(int i, const int n, const int lo, const int hi, bool& flip)
+{
+    if (i < 0)       { flip = (lo == BC_REFLECTING); i = flip ? -1 - i : 0; }
+    else if (i >= n) { flip = (hi == BC_REFLECTING); i = flip ? 2 * n - 1 - i : n - 1; }
+    else             { flip = false; }
+    return min(max(i, 0), n - 1);
+}
+
+struct DomRegs
+{
+    int nx, ny, nz;
+    int bc0, bc1, bc2, bc3, bc4, bc5;
+    long long fs;
+};
+
+// Load the conserved state of (ix,iy,iz) (any integers: out-of-domain cells
+// are synthesised from the boundary conditions) and convert to primitives.
+template <class Pol>
+__device__ __forceinline__ void load_prim(const DomRegs& D, const typename Pol::T* __restrict__ U,
+                                          int ix, int iy, int iz, typename Pol::T q[7])
+{
+    typedef typename Pol::T T;
+    bool fx, fy, fz;
+    ix = bc_map(ix, D.nx, D.bc0, D.bc1, fx);
+    iy = bc_map(iy, D.ny, D.bc2, D.bc3, fy);
+    iz = bc_map(iz, D.nz, D.bc4, D.bc5, fz);
+    const long long idx = (long long)ix + (long long)D.nx * ((long long)iy + (long long)D.ny * iz);
+    T c[7];
+#pragma unroll
+    for (int k = 0; k < 7; ++k) c[k] = __ldg(U + k * D.fs + idx);
+    if (fx) c[1] = -c[1];
+    if (fy) c[2] = -c[2];
+    if (fz) c[3] = -c[3];
+    to_primitive<Pol>(c, q);
+}
+
+template <class T>
+__device__ __forceinline__ bool physical(const T r, const T e, const T G, const T P)
+{
+    // also false for NaN
+    return (r > (T)0) && (e > (T)0) && (G > (T)0) && (P >= (T)0) && (e < (T)INFINITY) && (r < (T)INFINITY);
+}
+
+// Register budget: at least kMinWarpsPerSM resident warps per SM.  The
+// face pipeline has 14 independent reconstructions, so the compiler would
+// otherwise trade occupancy for unbounded instruction-level parallelism.
+#ifndef MPCF_MIN_WARPS_PER_SM
+#define MPCF_MIN_WARPS_PER_SM 16
+#endif
+template <int TY> struct MinBlocks
+{
+    static constexpr int v = (MPCF_MIN_WARPS_PER_SM / TY) > 0 ? (MPCF_MIN_WARPS_PER_SM / TY) : 1;
+};
+
+template <class Pol, int TY, bool PERSIST>
+__global__ void __launch_bounds__(kTX * TY, MinBlocks<TY>::v)
+stage_kernel(const StageArgs A)
+{
+    typedef typename Pol::T T;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    StageSmem<T, TY>& S = *reinterpret_cast<StageSmem<T, TY>*>(smem_raw);
+
+    const int tx = threadIdx.x & (kTX - 1);
+    const int ty = threadIdx.x >> 5;
+    const T a = (T)A.a;
+    const T b = (T)A.b;
+    const T factor6 = (T)1.0f / (T)6.0f;   // GPUkernels.cu:1103
+    bool ok = true;
+
+    int t;
+    if (PERSIST)
+    {
+        if (threadIdx.x == 0) S.tile = (int)atomicAdd(A.counter, 1u);
+        __syncthreads();
+        t = S.tile;
+    }
+    else t = blockIdx.x;
+
+    while (t < A.ntiles)
+    {
+        // ---- decode tile -> domain, tile coordinates
+        int d = 0;
+        while (d + 1 < A.ndom && A.doms[d + 1].tile_begin <= t) ++d;
+        const DomDev& DD = A.doms[d];
+        DomRegs D;
+        D.nx = DD.nx; D.ny = DD.ny; D.nz = DD.nz;
+        D.bc0 = DD.bc[0]; D.bc1 = DD.bc[1]; D.bc2 = DD.bc[2];
+        D.bc3 = DD.bc[3]; D.bc4 = DD.bc[4]; D.bc5 = DD.bc[5];
+        D.fs = DD.fs;
+        const T* __restrict__ U    = (const T*)DD.U[A.parity];
+        T* __restrict__       Un   = (T*)DD.U[A.parity ^ 1];
+        T* __restrict__       R    = (T*)DD.R;
+        const T dtinvh = ((const T*)A.dtinvh)[d];
+
+        const int lt = t - DD.tile_begin;
+        const int bx = lt % DD.tiles_x;
+        const int by = (lt / DD.tiles_x) % DD.tiles_y;
+        const int bz = lt / (DD.tiles_x * DD.tiles_y);
+        const int x0 = bx * kTX, y0 = by * TY;
+        const int z0 = bz * A.dz;
+        const int z1 = min(z0 + A.dz, D.nz);
+        const int gx = x0 + tx, gy = y0 + ty;
+        const bool valid = (gx < D.nx) && (gy < D.ny);
+
+        // ---- prologue: slabs z0-3 .. z0+1 of the own column into the ring
+        for (int s = z0 - 3; s <= z0 + 1; ++s)
+        {
+            T q[7];
+            load_prim<Pol>(D, U, gx, gy, s, q);
+            const int sl = (s + 6) % 6;
+#pragma unroll
+            for (int k = 0; k < 7; ++k) S.zwin[sl][k][ty][tx] = q[k];
+        }
+
+        T Sp[7];                 // x/y part of the flux bracket of cell k-1
+        T sG = 0, sP = 0, dU = 0;
+        T zfp[12];               // z face (k-1)-1/2
+#pragma unroll
+        for (int k = 0; k < 7; ++k) Sp[k] = 0;
+#pragma unroll
+        for (int k = 0; k < 12; ++k) zfp[k] = 0;
+        double cs[5] = {0, 0, 0, 0, 0};
+
+        for (int k = z0; k <= z1; ++k)
+        {
+            // (A) leading slab k+2 of the own column
+            {
+                T q[7];
+                load_prim<Pol>(D, U, gx, gy, k + 2, q);
+                const int sl = (k + 2 + 6) % 6;
+#pragma unroll
+                for (int m = 0; m < 7; ++m) S.zwin[sl][m][ty][tx] = q[m];
+            }
+            // (B) slab k with halos into cur
+            if (k < z1)
+            {
+                const int sl = (k + 6) % 6;
+#pragma unroll
+                for (int m = 0; m < 7; ++m) S.cur[m][ty + 3][tx + 3] = S.zwin[sl][m][ty][tx];
+                for (int i = threadIdx.x; i < 6 * kTX + 6 * TY; i += kTX * TY)
+                {
+                    int lx, ly;
+                    if (i < 6 * kTX)
+                    {
+                        const int r = i >> 5;
+                        lx = i & (kTX - 1);
+                        ly = r < 3 ? r - 3 : TY + r - 3;
+                    }
+                    else
+                    {
+                        const int j = i - 6 * kTX;
+                        const int c = j % 6;
+                        ly = j / 6;
+                        lx = c < 3 ? c - 3 : kTX + c - 3;
+                    }
+                    T q[7];
+                    load_prim<Pol>(D, U, x0 + lx, y0 + ly, k, q);
+#pragma unroll
+                    for (int m = 0; m < 7; ++m) S.cur[m][ly + 3][lx + 3] = q[m];
+                }
+            }
+            __syncthreads();
+
+            // (C) x/y faces of slab k
+            if (k < z1)
+            {
+                FaceOut<T> o;
+                {
+                    auto fx_fetch = [&](int q, int j) -> T { return S.cur[q][ty + 3][tx + j]; };
+                    face_flux<Pol, 0>(fx_fetch, o);
+#pragma unroll
+                    for (int m = 0; m < 7; ++m) S.fx[m][ty][tx] = o.f[m];
+                    S.fx[7][ty][tx] = o.Gm; S.fx[8][ty][tx] = o.Gp;
+                    S.fx[9][ty][tx] = o.Pm; S.fx[10][ty][tx] = o.Pp; S.fx[11][ty][tx] = o.vel;
+                }
+                {
+                    auto fy_fetch = [&](int q, int j) -> T { return S.cur[q][ty + j][tx + 3]; };
+                    face_flux<Pol, 1>(fy_fetch, o);
+#pragma unroll
+                    for (int m = 0; m < 7; ++m) S.fy[m][ty][tx] = o.f[m];
+                    S.fy[7][ty][tx] = o.Gm; S.fy[8][ty][tx] = o.Gp;
+                    S.fy[9][ty][tx] = o.Pm; S.fy[10][ty][tx] = o.Pp; S.fy[11][ty][tx] = o.vel;
+                }
+                if (ty == 0)
+                {
+                    // y faces above the tile (row TY)
+                    auto fy_fetch = [&](int q, int j) -> T { return S.cur[q][TY + j][tx + 3]; };
+                    face_flux<Pol, 1>(fy_fetch, o);
+#pragma unroll
+                    for (int m = 0; m < 7; ++m) S.fy[m][TY][tx] = o.f[m];
+                    S.fy[7][TY][tx] = o.Gm; S.fy[8][TY][tx] = o.Gp;
+                    S.fy[9][TY][tx] = o.Pm; S.fy[10][TY][tx] = o.Pp; S.fy[11][TY][tx] = o.vel;
+                }
+                else if (ty == 1 && tx < TY)
+                {
+                    // x faces right of the tile (column 32), one per row
+                    const int row = tx;
+                    auto fx_fetch = [&](int q, int j) -> T { return S.cur[q][row + 3][kTX + j]; };
+                    face_flux<Pol, 0>(fx_fetch, o);
+#pragma unroll
+                    for (int m = 0; m < 7; ++m) S.fx[m][row][kTX] = o.f[m];
+                    S.fx[7][row][kTX] = o.Gm; S.fx[8][row][kTX] = o.Gp;
+                    S.fx[9][row][kTX] = o.Pm; S.fx[10][row][kTX] = o.Pp; S.fx[11][row][kTX] = o.vel;
+                }
+            }
+
+            // (D) z face k-1/2 of the own column
+            FaceOut<T> zf;
+            {
+                const int s0 = (k - 3 + 6) % 6;
+                auto fz_fetch = [&](int q, int j) -> T {
+                    int sl = s0 + j; sl = sl >= 6 ? sl - 6 : sl;
+                    return S.zwin[sl][q][ty][tx];
+                };
+                face_flux<Pol, 2>(fz_fetch, zf);
+            }
+            __syncthreads();
+
+            // (E) finalise cell k-1 of the own column
+            if (k > z0 && valid)
+            {
+                const long long idx = (long long)gx + (long long)D.nx * ((long long)gy + (long long)D.ny * (k - 1));
+                const T sumG = sG + (zfp[8] + zf.Gm);
+                const T sumP = sP + (zfp[10] + zf.Pm);
+                const T divU = dU + (zf.vel - zfp[11]);
+                T un[7];
+#pragma unroll
+                for (int m = 0; m < 7; ++m)
+                {
+                    T br = (Sp[m] + zf.f[m]) - zfp[m];
+                    if (m == 5) br = br - divU * sumG * factor6;
+                    if (m == 6) br = br - divU * sumP * factor6;
+                    const T rhs_m = dtinvh * br;
+                    const T rhs = a * R[m * D.fs + idx] - rhs_m;
+                    R[m * D.fs + idx] = rhs;
+                    un[m] = b * rhs + __ldg(U + m * D.fs + idx);
+                    Un[m * D.fs + idx] = un[m];
+                }
+                ok = ok && physical<T>(un[0], un[4], un[5], un[6]);
+                if (A.tile_sums)
+                {
+#pragma unroll
+                    for (int m = 0; m < 5; ++m) cs[m] += (double)un[m];
+                }
+            }
+
+            // (F) x/y part of cell k, carried to the next slab
+            if (k < z1)
+            {
+#pragma unroll
+                for (int m = 0; m < 7; ++m)
+                    Sp[m] = ((S.fx[m][ty][tx + 1] - S.fx[m][ty][tx]) + S.fy[m][ty + 1][tx]) - S.fy[m][ty][tx];
+                sG = S.fx[8][ty][tx] + S.fx[7][ty][tx + 1];
+                sP = S.fx[10][ty][tx] + S.fx[9][ty][tx + 1];
+                dU = S.fx[11][ty][tx + 1] - S.fx[11][ty][tx];
+                sG = sG + (S.fy[8][ty][tx] + S.fy[7][ty + 1][tx]);
+                sP = sP + (S.fy[10][ty][tx] + S.fy[9][ty + 1][tx]);
+                dU = dU + (S.fy[11][ty + 1][tx] - S.fy[11][ty][tx]);
+            }
+            zfp[0] = zf.f[0]; zfp[1] = zf.f[1]; zfp[2] = zf.f[2]; zfp[3] = zf.f[3];
+            zfp[4] = zf.f[4]; zfp[5] = zf.f[5]; zfp[6] = zf.f[6];
+            zfp[7] = zf.Gm; zfp[8] = zf.Gp; zfp[9] = zf.Pm; zfp[10] = zf.Pp; zfp[11] = zf.vel;
+        }
+
+        // ---- per-tile FP64 conservation sums (deterministic: fixed order)
+        if (A.tile_sums)
+        {
+#pragma unroll
+            for (int m = 0; m < 5; ++m)
+            {
+                double v = cs[m];
+#pragma unroll
+                for (int off = 16; off > 0; off >>= 1) v += __shfl_xor_sync(0xffffffffu, v, off);
+                if (tx == 0) S.red[ty][m] = v;
+            }
+            __syncthreads();
+            if (threadIdx.x < 5)
+            {
+                double v = 0;
+                for (int w = 0; w < TY; ++w) v += S.red[w][threadIdx.x];
+                A.tile_sums[(long long)t * 5 + threadIdx.x] = v;
+            }
+        }
+
+        if (!PERSIST) break;
+        __syncthreads();
+        if (threadIdx.x == 0) S.tile = (int)atomicAdd(A.counter, 1u);
+        __syncthreads();
+        t = S.tile;
+    }
+
+    if (!__all_sync(0xffffffffu, ok) && tx == 0) atomicOr(A.err, (unsigned)ERRBIT_NONPHYSICAL);
+}
+
+template <class T, int TY>
+constexpr size_t stage_smem_bytes() { return sizeof(StageSmem<T, TY>); }
+
+} // namespace mpcf

@@ -1,0 +1,87 @@
+// mpcf_types.h -- plain structures shared by the host runtime and the
+// kernels of libmpcf_b200 (no CUDA types in here beyond what a .cu sees).
+#pragma once
+
+#include <stddef.h>
+#include <stdint.h>
+
+namespace mpcf {
+
+// Boundary condition codes per face (x-left, x-right, y-left, y-right,
+// z-left, z-right).  Absorbing = zeroth-order extrapolation, reflecting =
+// mirror with the normal momentum negated (BoundaryConditions.h:60-109).
+enum { BC_ABSORBING = 0, BC_REFLECTING = 1 };
+
+// Bits of the device error word.
+enum {
+    ERRBIT_NONPHYSICAL = 1u << 0,   // rho <= 0, E <= 0, G <= 0, P < 0 or non-finite after an update
+    ERRBIT_SOS_NONFINITE = 1u << 1, // max sound speed not finite or not positive
+};
+
+// One domain as the kernels see it.  All 7 fields of a buffer live in one
+// allocation with a field stride `fs` (elements, a multiple of 64), cell
+// (ix,iy,iz) at ix + nx*(iy + ny*iz) inside a field (Types.h:31).
+struct DomDev
+{
+    void*  U[2];        // ping-pong state buffers (T*), 7 fields each
+    void*  R;           // low-storage RK register (T*), 7 fields
+    long long fs;       // field stride in elements
+    int    nx, ny, nz;
+    int    bc[6];
+    int    tiles_x, tiles_y, tiles_z;
+    int    tile_begin;  // first global tile id of this domain
+    int    sos_chunk_begin;   // first global sound-speed chunk of this domain
+    int    sos_chunks;
+    double h;
+};
+
+// Arguments of one stage launch (all domains of a solver).
+struct StageArgs
+{
+    const DomDev* doms;
+    int    ndom;
+    int    ntiles;      // total tiles over all domains
+    int    dz;          // z-chunk depth of a tile
+    int    parity;      // read U[parity], write U[parity^1]
+    double a, b;        // LSRK3 stage coefficients
+    const void* dtinvh; // T[ndom], dt/h per domain
+    unsigned* counter;  // persistent-launch work counter (zeroed before launch)
+    unsigned* err;      // device error word
+    double* tile_sums;  // [ntiles][5] FP64 partial conservation sums, or null
+};
+
+struct SosArgs
+{
+    const DomDev* doms;
+    int    ndom;
+    int    nchunks;     // total chunks over all domains
+    int    chunk;       // cells per chunk
+    int    parity;
+    void*  sos_bits;    // per domain: unsigned (float bits) or unsigned long long (double bits)
+};
+
+struct DtArgs
+{
+    const DomDev* doms;
+    int    ndom;
+    double cfl, dt_max;
+    void*  sos_bits;
+    void*  dtinvh;      // T[ndom]
+    double* dt;         // [ndom]
+    double* time;       // [ndom], accumulated
+    unsigned* err;
+};
+
+// Bubble-cloud initial condition (liquid with gas bubbles, tanh-smoothed
+// indicator).  Material parameters gamma and pc give G = 1/(gamma-1) and
+// P = gamma*pc/(gamma-1).
+struct IcParams
+{
+    double rho_l, p_l, gamma_l, pc_l;
+    double rho_g, p_g, gamma_g, pc_g;
+    double noise;       // velocity noise amplitude (uniform in [-noise, noise])
+    double width;       // interface width in cells (tanh smoothing over width*h)
+    unsigned long long seed;
+};
+
+} // namespace mpcf

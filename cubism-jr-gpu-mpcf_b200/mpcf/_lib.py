@@ -1,0 +1,107 @@
+"""ctypes binding of libmpcf_b200 (include/mpcf_b200.h).
+
+The shared library is built in-tree (``make -C cubism-jr-gpu-mpcf_b200``) and
+loaded from ``cubism-jr-gpu-mpcf_b200/lib/libmpcf_b200.so``.  There is no
+fallback: if the library is missing, loading raises, and every compute call
+goes through the CUDA kernels.
+"""
+import ctypes
+import os
+
+PKG_DIR = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+LIB_PATH = os.environ.get("MPCF_B200_LIB", os.path.join(PKG_DIR, "lib", "libmpcf_b200.so"))
+
+PREC_FP32_REF = 0
+PREC_FP32 = 1
+PREC_MIXED = 2
+PREC_FP64 = 3
+PRECISIONS = {"fp32_ref": PREC_FP32_REF, "fp32": PREC_FP32, "mixed": PREC_MIXED, "fp64": PREC_FP64}
+
+BC_ABSORBING = 0
+BC_REFLECTING = 1
+
+ERR_ARG, ERR_CUDA, ERR_NOMEM, ERR_STATE, ERR_NUMERIC = -1, -2, -3, -4, -5
+ERRBIT_NONPHYSICAL = 1
+ERRBIT_SOS = 2
+
+# every symbol the header declares, with (restype, argtypes)
+_c = ctypes
+_P = _c.c_void_p
+_PP = _c.POINTER(_c.c_void_p)
+_I = _c.c_int
+_D = _c.c_double
+_PD = _c.POINTER(_c.c_double)
+_PI = _c.POINTER(_c.c_int)
+
+
+class IcParams(ctypes.Structure):
+    """mirror of mpcf_ic_params"""
+    _fields_ = [("rho_l", _D), ("p_l", _D), ("gamma_l", _D), ("pc_l", _D),
+                ("rho_g", _D), ("p_g", _D), ("gamma_g", _D), ("pc_g", _D),
+                ("noise", _D), ("width", _D), ("seed", _c.c_ulonglong)]
+
+
+SIGNATURES = {
+    "mpcf_version": (_I, []),
+    "mpcf_last_error": (_c.c_char_p, []),
+    "mpcf_elem_size": (_I, [_I]),
+    "mpcf_create": (_I, [_PP, _I, _PI, _PI, _I, _I]),
+    "mpcf_destroy": (_I, [_P]),
+    "mpcf_num_domains": (_I, [_P]),
+    "mpcf_precision": (_I, [_P]),
+    "mpcf_set_state": (_I, [_P, _I, _PP, _PP, _I]),
+    "mpcf_get_state": (_I, [_P, _I, _PP, _PP, _I]),
+    "mpcf_device_pointers": (_I, [_P, _I, _PP, _PP]),
+    "mpcf_max_sos": (_I, [_P, _PD]),
+    "mpcf_stage": (_I, [_P, _D, _D, _PD]),
+    "mpcf_compute_dt": (_I, [_P, _D, _D, _PD]),
+    "mpcf_step": (_I, [_P, _D, _D, _PD]),
+    "mpcf_run": (_I, [_P, _I, _D, _D, _I, _PD]),
+    "mpcf_synchronize": (_I, [_P]),
+    "mpcf_conserved_sums": (_I, [_P, _PD]),
+    "mpcf_set_track_conservation": (_I, [_P, _I]),
+    "mpcf_error_word": (_I, [_P, _c.POINTER(_c.c_uint), _I]),
+    "mpcf_set_bc": (_I, [_P, _I, _PI]),
+    "mpcf_fill_ghosts": (_I, [_P, _I, _P, _P, _P, _I]),
+    "mpcf_ic_cloud": (_I, [_P, _I, _c.POINTER(IcParams), _I, _PD]),
+    "mpcf_ic_cloud_host": (_I, [_I, _I, _I, _c.POINTER(IcParams), _I, _PD, _I, _PP]),
+    "mpcf_bubbles": (_I, [_c.c_ulonglong, _I, _D, _D, _PD, _PD, _D, _I, _PD]),
+    "mpcf_set_tiling": (_I, [_P, _I, _I, _I]),
+    "mpcf_get_tiling": (_I, [_P, _PI, _PI, _PI]),
+    "mpcf_autotune": (_I, [_P, _I, _PI, _PD]),
+    "mpcf_launch_shape": (_I, [_P, _c.POINTER(_c.c_longlong), _c.POINTER(_c.c_longlong), _PI]),
+    "mpcf_time_stages": (_I, [_P, _I, _D, _PD]),
+    "mpcf_probe_fp32_peak": (_I, [_I, _PD]),
+    "mpcf_time_run": (_I, [_P, _I, _D, _D, _PD]),
+}
+
+_lib = None
+
+
+class MpcfError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__(f"mpcf error {code}: {msg}")
+        self.code = code
+
+
+def lib():
+    """Load (once) and return the shared library with typed entry points."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise OSError(f"libmpcf_b200 not built: {LIB_PATH} is missing "
+                          "(run `make -C cubism-jr-gpu-mpcf_b200`)")
+        L = ctypes.CDLL(LIB_PATH)
+        for name, (res, args) in SIGNATURES.items():
+            f = getattr(L, name)
+            f.restype = res
+            f.argtypes = args
+        _lib = L
+    return _lib
+
+
+def check(rc):
+    """Raise MpcfError for a negative status; return non-negative values."""
+    if rc < 0:
+        raise MpcfError(rc, lib().mpcf_last_error().decode(errors="replace"))
+    return rc

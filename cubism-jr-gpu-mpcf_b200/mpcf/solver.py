@@ -1,0 +1,266 @@
+"""Python host layer over the C ABI.
+
+``Solver`` owns one or more independent domains on one GPU.  ``GPUlab``
+mirrors the reference's lab interface (source/GPUlab.h:250-258) so a
+Python driver reads like the reference's LSRK3_IntegratorMPI
+(source/LSRK3_IntegratorMPI.cpp:27-62):
+
+    lab.max_sos() -> (seconds, sos); lab.load_ghosts(); lab.process_all(a, b, dtinvh)
+"""
+import ctypes
+import time
+
+import numpy as np
+
+from . import _lib
+from ._lib import check, lib, IcParams
+
+FIELDS = ("rho", "rhou", "rhov", "rhow", "E", "G", "P")
+
+
+def _ptr_array(arrays):
+    return (ctypes.c_void_p * 7)(*[a.ctypes.data for a in arrays])
+
+
+def dtype_of(precision):
+    return np.float64 if precision == _lib.PREC_FP64 else np.float32
+
+
+class Solver:
+    """Domains advanced by the fused sm_100a stage kernel.
+
+    dims: list of (nx, ny, nz); bc: list of 6-tuples (x-, x+, y-, y+, z-, z+)
+    or None (absorbing); precision: one of _lib.PREC_* or a name in
+    _lib.PRECISIONS.
+    """
+
+    def __init__(self, dims, bc=None, precision="fp32_ref", device=0):
+        if isinstance(precision, str):
+            precision = _lib.PRECISIONS[precision]
+        if isinstance(dims[0], int):
+            dims = [tuple(dims)]
+        self.dims = [tuple(int(v) for v in d) for d in dims]
+        self.ndom = len(self.dims)
+        self.precision = precision
+        self.dtype = dtype_of(precision)
+        flat = (ctypes.c_int * (3 * self.ndom))(*[v for d in self.dims for v in d])
+        bcarr = None
+        if bc is not None:
+            if isinstance(bc[0], int):
+                bc = [bc] * self.ndom
+            bcarr = (ctypes.c_int * (6 * self.ndom))(*[int(v) for b in bc for v in b])
+        h = ctypes.c_void_p()
+        check(lib().mpcf_create(ctypes.byref(h), self.ndom, flat, bcarr, precision, device))
+        self._h = h
+
+    # -- lifetime ---------------------------------------------------------
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().mpcf_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    # -- state ------------------------------------------------------------
+    def ncells(self, dom=0):
+        nx, ny, nz = self.dims[dom]
+        return nx * ny * nz
+
+    def set_state(self, state, reg=None, dom=0):
+        """state/reg: sequences of 7 host arrays (flattened x-fastest)."""
+        st = [np.ascontiguousarray(a, dtype=self.dtype).ravel() for a in state]
+        rg = None if reg is None else [np.ascontiguousarray(a, dtype=self.dtype).ravel() for a in reg]
+        for a in st + (rg or []):
+            if a.size != self.ncells(dom):
+                raise ValueError("field size does not match the domain")
+        check(lib().mpcf_set_state(self._h, dom, _ptr_array(st), None if rg is None else _ptr_array(rg), 0))
+
+    def get_state(self, dom=0, with_reg=True):
+        n = self.ncells(dom)
+        st = [np.empty(n, self.dtype) for _ in range(7)]
+        rg = [np.empty(n, self.dtype) for _ in range(7)] if with_reg else None
+        check(lib().mpcf_get_state(self._h, dom, _ptr_array(st), None if rg is None else _ptr_array(rg), 0))
+        return (st, rg) if with_reg else st
+
+    def device_pointers(self, dom=0):
+        st = (ctypes.c_void_p * 7)()
+        rg = (ctypes.c_void_p * 7)()
+        check(lib().mpcf_device_pointers(self._h, dom, st, rg))
+        return list(st), list(rg)
+
+    # -- hot path ---------------------------------------------------------
+    def max_sos(self):
+        out = (ctypes.c_double * self.ndom)()
+        check(lib().mpcf_max_sos(self._h, out))
+        return list(out)
+
+    def stage(self, a, b, dtinvh=None):
+        arr = None
+        if dtinvh is not None:
+            if np.isscalar(dtinvh):
+                dtinvh = [dtinvh] * self.ndom
+            arr = (ctypes.c_double * self.ndom)(*dtinvh)
+        check(lib().mpcf_stage(self._h, float(a), float(b), arr))
+
+    def compute_dt(self, cfl, dt_max=1e30):
+        out = (ctypes.c_double * self.ndom)()
+        check(lib().mpcf_compute_dt(self._h, float(cfl), float(dt_max), out))
+        return list(out)
+
+    def step(self, cfl=0.3, dt_max=1e30, want_dt=True):
+        out = (ctypes.c_double * self.ndom)() if want_dt else None
+        check(lib().mpcf_step(self._h, float(cfl), float(dt_max), out))
+        return list(out) if want_dt else None
+
+    def run(self, nsteps, cfl=0.3, dt_max=1e30, graph=True):
+        out = (ctypes.c_double * self.ndom)()
+        check(lib().mpcf_run(self._h, int(nsteps), float(cfl), float(dt_max), 1 if graph else 0, out))
+        return list(out)
+
+    def synchronize(self):
+        check(lib().mpcf_synchronize(self._h))
+
+    def conserved_sums(self):
+        out = (ctypes.c_double * (5 * self.ndom))()
+        check(lib().mpcf_conserved_sums(self._h, out))
+        return np.array(out).reshape(self.ndom, 5)
+
+    def track_conservation(self, on=True):
+        check(lib().mpcf_set_track_conservation(self._h, 1 if on else 0))
+
+    def error_word(self, clear=False):
+        w = ctypes.c_uint()
+        check(lib().mpcf_error_word(self._h, ctypes.byref(w), 1 if clear else 0))
+        return w.value
+
+    # -- boundaries -------------------------------------------------------
+    def set_bc(self, bc6, dom=0):
+        check(lib().mpcf_set_bc(self._h, dom, (ctypes.c_int * 6)(*bc6)))
+
+    def fill_ghosts(self, dom=0):
+        nx, ny, nz = self.dims[dom]
+        gx = np.empty(2 * 7 * 3 * ny * nz, self.dtype)
+        gy = np.empty(2 * 7 * nx * 3 * nz, self.dtype)
+        gz = np.empty(2 * 7 * nx * ny * 3, self.dtype)
+        check(lib().mpcf_fill_ghosts(self._h, dom, gx.ctypes.data, gy.ctypes.data, gz.ctypes.data, 0))
+        return gx, gy, gz
+
+    # -- initial conditions -----------------------------------------------
+    def ic_cloud(self, params, bubbles, dom=0):
+        b = np.ascontiguousarray(bubbles, dtype=np.float64).ravel()
+        nb = b.size // 4
+        check(lib().mpcf_ic_cloud(self._h, dom, ctypes.byref(params), nb,
+                                  b.ctypes.data_as(ctypes.POINTER(ctypes.c_double)) if nb else None))
+
+    # -- launch configuration ----------------------------------------------
+    def set_tiling(self, ty, dz, persistent=False):
+        check(lib().mpcf_set_tiling(self._h, int(ty), int(dz), 1 if persistent else 0))
+
+    def tiling(self):
+        ty, dz, p = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
+        check(lib().mpcf_get_tiling(self._h, ctypes.byref(ty), ctypes.byref(dz), ctypes.byref(p)))
+        return ty.value, dz.value, bool(p.value)
+
+    def autotune(self, reps=3):
+        best = (ctypes.c_int * 3)()
+        ms = ctypes.c_double()
+        check(lib().mpcf_autotune(self._h, int(reps), best, ctypes.byref(ms)))
+        return (best[0], best[1], bool(best[2])), ms.value
+
+    def launch_shape(self):
+        nt, g, th = ctypes.c_longlong(), ctypes.c_longlong(), ctypes.c_int()
+        check(lib().mpcf_launch_shape(self._h, ctypes.byref(nt), ctypes.byref(g), ctypes.byref(th)))
+        return nt.value, g.value, th.value
+
+    def time_stages(self, reps, dtinvh=0.0):
+        ms = ctypes.c_double()
+        check(lib().mpcf_time_stages(self._h, int(reps), float(dtinvh), ctypes.byref(ms)))
+        return ms.value
+
+
+def ic_cloud_host(dims, params, bubbles, dtype=np.float32):
+    """Host generator of the bubble-cloud IC (same formula as the device one)."""
+    nx, ny, nz = dims
+    n = nx * ny * nz
+    out = [np.empty(n, dtype) for _ in range(7)]
+    b = np.ascontiguousarray(bubbles, dtype=np.float64).ravel()
+    nb = b.size // 4
+    check(lib().mpcf_ic_cloud_host(nx, ny, nz, ctypes.byref(params), nb,
+                                   b.ctypes.data_as(ctypes.POINTER(ctypes.c_double)) if nb else None,
+                                   np.dtype(dtype).itemsize, _ptr_array(out)))
+    return out
+
+
+def bubbles(seed, n, rmin, rmax, lo=(0.2, 0.2, 0.2), hi=(0.8, 0.8, 0.8), gap=0.0, max_tries=200000):
+    """Seeded non-overlapping spheres (x, y, z, r), shape (placed, 4)."""
+    out = np.zeros((max(n, 1), 4), np.float64)
+    lo3 = (ctypes.c_double * 3)(*lo)
+    hi3 = (ctypes.c_double * 3)(*hi)
+    k = check(lib().mpcf_bubbles(ctypes.c_ulonglong(seed), int(n), float(rmin), float(rmax), lo3, hi3,
+                                 float(gap), int(max_tries), out.ctypes.data_as(ctypes.POINTER(ctypes.c_double))))
+    return out[:k]
+
+
+# LSRK3 coefficients (LSRK3_IntegratorMPI.cpp:46,51,56)
+LSRK3 = ((0.0, 1.0 / 4), (-17.0 / 32, 8.0 / 9), (-32.0 / 27, 3.0 / 4))
+
+
+class GPUlab:
+    """Reference-shaped lab over a single-domain Solver (GPUlab.h:250-258).
+
+    ``nslices`` is accepted for signature compatibility; the state is device
+    resident, so there is no chunking.  ``process_all`` keeps the reference
+    postcondition when ``sync_host`` is set: the host arrays hold the new
+    state and register after each call (GPUlab.cpp:772-788).
+    """
+
+    def __init__(self, solver, nslices=None, host_state=None, host_reg=None, sync_host=False):
+        self.solver = solver
+        self.nslices = nslices
+        self.host_state = host_state
+        self.host_reg = host_reg
+        self.sync_host = sync_host
+
+    def load_ghosts(self, t=0.0):
+        # ghosts are synthesised inside the stage kernel from the boundary
+        # conditions; nothing to stage
+        return None
+
+    def max_sos(self):
+        t0 = time.perf_counter()
+        sos = self.solver.max_sos()[0]
+        return time.perf_counter() - t0, sos
+
+    def process_all(self, a, b, dtinvh):
+        t0 = time.perf_counter()
+        self.solver.stage(a, b, dtinvh)
+        if self.sync_host and self.host_state is not None:
+            st, rg = self.solver.get_state()
+            for q in range(7):
+                self.host_state[q][...] = st[q].reshape(self.host_state[q].shape)
+                if self.host_reg is not None:
+                    self.host_reg[q][...] = rg[q].reshape(self.host_reg[q].shape)
+        return time.perf_counter() - t0
+
+
+def lsrk3_step(lab, h, cfl, dt_max=1e30, real=np.float32):
+    """LSRK3_IntegratorMPI::operator() on one rank, driving a GPUlab."""
+    _, sos = lab.max_sos()
+    dt = cfl * h / sos
+    dt = dt_max if dt_max < dt else dt
+    for a, b in LSRK3:
+        lab.load_ghosts()
+        # process_all takes Real arguments: the coefficients and dt/h are
+        # rounded to the stage precision
+        lab.process_all(float(real(a)), float(real(b)), float(real(dt / h)))
+    return dt

@@ -1,0 +1,188 @@
+/*
+ * mpcf_b200.h -- C ABI of libmpcf_b200, the B200 (sm_100a) implementation of
+ * the CUBISM-MPCF per-step hot path: WENO5/HLLC convection in x/y/z, the
+ * low-storage LSRK3 stage update and the maximum-speed-of-sound CFL
+ * reduction, for the 7-field stiffened-gas two-phase system.
+ *
+ * Plain C: opaque handle, raw pointers and sizes, int status returns (0 on
+ * success, a negative MPCF_ERR_* code otherwise; mpcf_last_error() gives
+ * the message of the calling thread's last failure).  No allocation or CUDA
+ * type appears in a signature.
+ *
+ * Data layout (reference: source/NodeBlock.h:26-36,110-117, Types.h:31):
+ *   a state or register is 7 arrays (rho, rho*u, rho*v, rho*w, E,
+ *   G = 1/(gamma-1), P = gamma*pc/(gamma-1)) of nx*ny*nz elements, cell
+ *   (ix,iy,iz) at ix + nx*(iy + ny*iz).  Element type: float for the
+ *   MPCF_PREC_FP32_REF, MPCF_PREC_FP32 and MPCF_PREC_MIXED precisions,
+ *   double for MPCF_PREC_FP64.
+ * Boundary conditions, per domain, 6 ints in the order
+ *   x-left, x-right, y-left, y-right, z-left, z-right
+ *   (MPCF_BC_ABSORBING / MPCF_BC_REFLECTING, BoundaryConditions.h:60-109).
+ *
+ * Threading: one host thread per solver at a time.  All work of a solver is
+ * ordered on its own CUDA stream; calls that return host data synchronise it.
+ */
+#ifndef MPCF_B200_H
+#define MPCF_B200_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define MPCF_API_VERSION 1
+
+typedef struct mpcf_solver mpcf_solver;
+
+/* precisions */
+#define MPCF_PREC_FP32_REF 0  /* FP32, rounding of the reference source (bit-exact to the CPU restatement) */
+#define MPCF_PREC_FP32     1  /* FP32, fast weights / division, fused multiply-add */
+#define MPCF_PREC_MIXED    2  /* fast FP32 + FP64 pressure recovery + FP64 conservation sums */
+#define MPCF_PREC_FP64     3  /* all FP64 */
+
+/* boundary conditions */
+#define MPCF_BC_ABSORBING  0
+#define MPCF_BC_REFLECTING 1
+
+/* status codes */
+#define MPCF_OK            0
+#define MPCF_ERR_ARG      -1   /* invalid argument */
+#define MPCF_ERR_CUDA     -2   /* CUDA runtime error (message has the CUDA error string) */
+#define MPCF_ERR_NOMEM    -3   /* device or host allocation failed */
+#define MPCF_ERR_STATE    -4   /* call not valid in the solver's state */
+#define MPCF_ERR_NUMERIC  -5   /* the device error word reports a non-physical state */
+
+/* bits of the device error word */
+#define MPCF_ERRBIT_NONPHYSICAL  1u  /* rho<=0, E<=0, G<=0, P<0 or non-finite after an update */
+#define MPCF_ERRBIT_SOS          2u  /* maximum speed of sound not finite or not positive */
+
+/* Bubble-cloud initial condition (liquid with gas bubbles; indicator
+ * alpha = 0.5*(1 - tanh(phi/(width*h))), phi = distance to the nearest
+ * bubble surface; velocity noise uniform in [-noise, noise] from a
+ * counter-based hash of (seed, cell, component)). */
+typedef struct mpcf_ic_params
+{
+    double rho_l, p_l, gamma_l, pc_l;   /* liquid */
+    double rho_g, p_g, gamma_g, pc_g;   /* gas */
+    double noise;                       /* velocity noise amplitude */
+    double width;                       /* interface width in cells */
+    unsigned long long seed;
+} mpcf_ic_params;
+
+/* ---- version / errors --------------------------------------------------- */
+int         mpcf_version(void);
+const char* mpcf_last_error(void);
+int         mpcf_elem_size(int precision);   /* 4 or 8, or MPCF_ERR_ARG */
+
+/* ---- lifetime ----------------------------------------------------------- *
+ * Replaces GPU::alloc / GPU::dealloc (source/GPU/GPU.h:48-49,
+ * GPUhousehold.cu:81-254) and the GPUlab constructor's device set-up
+ * (GPUlab.cpp:25-71).  ndomains >= 1 independent domains of sizes
+ * dims[3*d..3*d+2] (each >= 5 in x and y, >= 3 in z, as the reference's
+ * GPUkernels.cu:18-24 and BoundaryConditions.h mirrors require); bc may be
+ * NULL (all absorbing).  h[d] = 1/max(nx,ny,nz) (NodeBlock.h:71).  The
+ * solver owns all device memory: two state buffers (ping-pong), the
+ * register and the per-domain scalars. */
+int mpcf_create(mpcf_solver** out, int ndomains, const int* dims, const int* bc,
+                int precision, int device);
+int mpcf_destroy(mpcf_solver* s);
+int mpcf_num_domains(const mpcf_solver* s);
+int mpcf_precision(const mpcf_solver* s);
+
+/* ---- state transfer ----------------------------------------------------- *
+ * Replaces the per-stage PCIe staging of GPUlab (h2d_3DArray, h2d_tmp,
+ * d2h_rhs, d2h_tmp: GPU.h:52-56, GPUhousehold.cu:260-334).  state7/reg7 are
+ * 7 pointers each, host memory unless *_is_device is set; reg7 may be NULL
+ * (set: register cleared; get: register not copied). */
+int mpcf_set_state(mpcf_solver* s, int dom, const void* const* state7, const void* const* reg7, int src_is_device);
+int mpcf_get_state(mpcf_solver* s, int dom, void* const* state7, void* const* reg7, int dst_is_device);
+/* current device addresses of the state and register fields (valid until the
+ * next stage, which swaps the state buffers) */
+int mpcf_device_pointers(mpcf_solver* s, int dom, void** state7, void** reg7);
+
+/* ---- the hot path --------------------------------------------------------- *
+ * mpcf_max_sos: GPUlab::max_sos (GPUlab.cpp:647-700) + _maxSOS
+ *   (GPUkernels.cu:1182-1222) / MaxSpeedOfSound_CUDA::compute
+ *   (MaxSpeedOfSound_CUDA.cpp:13-18).  sos[d] per domain.
+ * mpcf_stage: GPUlab::process_all(a, b, dtinvh) (GPUlab.cpp:703-793), i.e.
+ *   ghosts/BCs + Convection_CUDA(a, dtinvh).compute + Update_CUDA(b).compute
+ *   (Convection_CUDA.cpp:15-23, Update_CUDA.cpp:12-17): R <- a*R - dtinvh*L(U),
+ *   U <- U + b*R.  dtinvh[d] per domain (NULL: use the device dt/h of the
+ *   last mpcf_step / mpcf_compute_dt).
+ * mpcf_compute_dt: max speed of sound and dt = min(cfl*h/sos, dt_max) on the
+ *   device (LSRK3_IntegratorMPI.cpp:31-38), no host round trip.
+ * mpcf_step: one LSRK3 step (LSRK3_IntegratorMPI.cpp:27-62): device dt, then
+ *   the three stages (a,b) = (0,1/4), (-17/32,8/9), (-32/27,3/4).  dt_out[d]
+ *   (optional) receives dt (synchronises).
+ * mpcf_run: nsteps steps; use_graph replays a captured CUDA graph of the
+ *   whole step.  time_out[d] (optional) receives the accumulated time. */
+int mpcf_max_sos(mpcf_solver* s, double* sos);
+int mpcf_stage(mpcf_solver* s, double a, double b, const double* dtinvh);
+int mpcf_compute_dt(mpcf_solver* s, double cfl, double dt_max, double* dt_out);
+int mpcf_step(mpcf_solver* s, double cfl, double dt_max, double* dt_out);
+int mpcf_run(mpcf_solver* s, int nsteps, double cfl, double dt_max, int use_graph, double* time_out);
+int mpcf_synchronize(mpcf_solver* s);
+
+/* FP64 sums of (rho, rho u, rho v, rho w, E) over each domain's current
+ * state, out[5*d..5*d+4]; deterministic order. */
+int mpcf_conserved_sums(mpcf_solver* s, double* out);
+/* When on, stage 3 of every step accumulates the FP64 sums of the new
+ * state inside the stage kernel (no extra pass); mpcf_conserved_sums then
+ * returns them without another reduction. */
+int mpcf_set_track_conservation(mpcf_solver* s, int on);
+
+/* device error word (MPCF_ERRBIT_*); clear != 0 resets it */
+int mpcf_error_word(mpcf_solver* s, unsigned* word, int clear);
+
+/* ---- boundary conditions / ghosts ---------------------------------------- *
+ * mpcf_set_bc: change the 6 face conditions of a domain (the per-case
+ *   GPUlab::_apply_bc overrides, e.g. Sim_SICCloudMPI.h:312-321).
+ * mpcf_fill_ghosts: materialise the ghost layers the stage kernel
+ *   synthesises, in the reference's halo layouts (GHOSTMAPX/GHOSTMAPY/ID3,
+ *   Types.h:42-52): gx 2*7*3*ny*nz, gy 2*7*nx*3*nz, gz 2*7*nx*ny*3 elements,
+ *   ordered [side][field][...]; side 0 = left (layer 0 outermost), side 1 =
+ *   right (layer 0 innermost). */
+int mpcf_set_bc(mpcf_solver* s, int dom, const int* bc6);
+int mpcf_fill_ghosts(mpcf_solver* s, int dom, void* gx, void* gy, void* gz, int dst_is_device);
+
+/* ---- initial conditions --------------------------------------------------- */
+/* device generator: state of domain dom from the cloud IC, register cleared */
+int mpcf_ic_cloud(mpcf_solver* s, int dom, const mpcf_ic_params* p, int nbubbles, const double* bubbles4);
+/* host generator of the same IC (elem_size 4 or 8): 7 host arrays */
+int mpcf_ic_cloud_host(int nx, int ny, int nz, const mpcf_ic_params* p, int nbubbles,
+                       const double* bubbles4, int elem_size, void* const* out7);
+/* Seeded rejection sampling of non-overlapping spheres (std::mt19937_64):
+ * centres uniform in [lo[i], hi[i]], radii uniform in [rmin, rmax], at least
+ * `gap` apart surface to surface.  Writes up to n (x,y,z,r) quadruples and
+ * returns how many were placed (>= 0) or an error code. */
+int mpcf_bubbles(unsigned long long seed, int n, double rmin, double rmax,
+                 const double* lo3, const double* hi3, double gap, int max_tries, double* out4);
+
+/* ---- launch configuration ------------------------------------------------- *
+ * tile = 32 x ty columns x dz slabs; persistent = one CTA per resident slot
+ * pulling tiles from a work counter.  mpcf_autotune times the candidates on
+ * the solver's own state (which it leaves unchanged) and keeps the fastest;
+ * best[3] (optional) = {ty, dz, persistent}, best_ms (optional) = stage time. */
+int mpcf_set_tiling(mpcf_solver* s, int ty, int dz, int persistent);
+int mpcf_get_tiling(const mpcf_solver* s, int* ty, int* dz, int* persistent);
+int mpcf_autotune(mpcf_solver* s, int reps, int* best3, double* best_ms);
+
+/* number of tiles one stage launch processes, and of stage-kernel CTAs */
+int mpcf_launch_shape(const mpcf_solver* s, long long* ntiles, long long* grid, int* threads);
+
+/* Time `reps` stage launches of the current configuration with CUDA events on
+ * the solver's stream (state advances; use on throw-away data). */
+int mpcf_time_stages(mpcf_solver* s, int reps, double dtinvh, double* ms_per_stage);
+
+/* Replay nsteps captured step graphs back to back and return their device
+ * time (CUDA events on the solver's stream), ms. */
+int mpcf_time_run(mpcf_solver* s, int nsteps, double cfl, double dt_max, double* ms);
+
+/* Measured FP32 CUDA-core throughput of the device (FMA chains), TFLOP/s:
+ * the denominator of the stage kernel's compute roofline. */
+int mpcf_probe_fp32_peak(int device, double* tflops);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* MPCF_B200_H */

@@ -1,0 +1,211 @@
+"""GPU parity: the sm_100a kernels through the C ABI against the CPU oracle.
+
+MPCF_PREC_FP32_REF is compared bit for bit (rounding of the reference
+source, FP32 with its double-promoted sub-expressions); the fast FP32 and
+mixed forms within the stated tolerances; FP64 against the FP64 oracle.
+Metric for the tolerance tests (the reference's parity metric): per stored
+field and register, max|x_gpu - x_oracle| / max|x_oracle|.
+"""
+import numpy as np
+import pytest
+
+import oracle_lib as O
+from conftest import cloud_state
+
+pytestmark = pytest.mark.gpu
+
+ABS, REF = 0, 1
+
+
+def rel_linf(a, b):
+    den = max(np.abs(b).max(), 1e-300)
+    return float(np.abs(a.astype(np.float64) - b.astype(np.float64)).max() / den)
+
+
+def assert_bitwise(got, want, what):
+    for q in range(7):
+        g, w = got[q], want[q]
+        bad = ~((g == w) | (np.isnan(g) & np.isnan(w)))
+        if bad.any():
+            i = int(np.flatnonzero(bad)[0])
+            raise AssertionError(f"{what} field {q}: {int(bad.sum())} cells differ; first at {i}: "
+                                 f"gpu={g[i]!r} oracle={w[i]!r} (rel linf {rel_linf(g, w):.3e})")
+
+
+def run_pair(mpcf, dims, bc, prec, U0, R0=None, stages=((0.0, 0.25, 0.05),), tiling=None):
+    """Run stages on GPU and oracle from the same inputs; return (gpu, oracle)."""
+    dtype = mpcf.dtype_of(mpcf.PRECISIONS[prec])
+    U = [np.array(a, dtype=dtype) for a in U0]
+    R = [np.zeros_like(a) for a in U] if R0 is None else [np.array(a, dtype=dtype) for a in R0]
+    with mpcf.Solver([dims], bc=[bc], precision=prec) as s:
+        if tiling:
+            s.set_tiling(*tiling)
+        s.set_state(U, R)
+        for a, b, dtinvh in stages:
+            s.stage(a, b, dtinvh)
+        Ug, Rg = s.get_state()
+        assert s.error_word() == 0
+    for a, b, dtinvh in stages:
+        O.stage(dims, bc, U, R, a, b, dtinvh)
+    return (Ug, Rg), (U, R)
+
+
+# ---------------------------------------------------------------------------
+# bit-exact reference-rounding path
+# ---------------------------------------------------------------------------
+@pytest.mark.parametrize("dims,bc", [
+    ((8, 7, 6), (ABS,) * 6),
+    ((8, 7, 6), (REF,) * 6),
+    ((37, 13, 11), (ABS, REF, REF, ABS, ABS, REF)),
+    ((5, 5, 3), (REF, ABS, ABS, REF, REF, ABS)),
+    ((64, 9, 20), (ABS,) * 6),
+])
+def test_ref32_stage_bitexact(mpcf, dims, bc):
+    U0 = cloud_state(dims, nb=2)
+    R0 = [np.asarray(a) * np.float32(1e-3) for a in cloud_state(dims, nb=1, seed=5)]
+    stages = [(0.0, 0.25, 0.057), (-17.0 / 32, 8.0 / 9, 0.057), (-32.0 / 27, 0.75, 0.057)]
+    (Ug, Rg), (Uo, Ro) = run_pair(mpcf, dims, bc, "fp32_ref", U0, R0, stages)
+    assert_bitwise(Ug, Uo, "state")
+    assert_bitwise(Rg, Ro, "register")
+
+
+@pytest.mark.parametrize("tiling", [(2, 3, False), (4, 64, False), (8, 5, True), (16, 7, False), (4, 1, True)])
+def test_ref32_tiling_invariant(mpcf, tiling):
+    dims, bc = (45, 19, 14), (ABS, REF, ABS, ABS, REF, ABS)
+    U0 = cloud_state(dims, nb=3)
+    (Ug, Rg), (Uo, Ro) = run_pair(mpcf, dims, bc, "fp32_ref", U0, tiling=tiling)
+    assert_bitwise(Ug, Uo, f"state tiling={tiling}")
+    assert_bitwise(Rg, Ro, f"register tiling={tiling}")
+
+
+def test_ref32_lsrk3_step_64cube(mpcf):
+    """Configuration 1: 64^3, one bubble, one LSRK3 step at CFL 0.3, absorbing."""
+    cfg = mpcf.configs.config("c1_64")
+    dims = cfg["dims"][0]
+    bc = (ABS,) * 6
+    U = mpcf.ic_cloud_host(dims, cfg["params"], cfg["bubbles"][0], np.float32)
+    R = [np.zeros_like(a) for a in U]
+    with mpcf.Solver([dims], precision="fp32_ref") as s:
+        s.set_state(U, R)
+        dt_gpu = s.step(cfl=0.3)[0]
+        Ug, Rg = s.get_state()
+        assert s.error_word() == 0
+    dt_o, sos_o = O.step(dims, bc, U, R, cfl=0.3)
+    assert dt_gpu == dt_o
+    assert_bitwise(Ug, U, "state")
+    assert_bitwise(Rg, R, "register")
+    for q in range(7):   # the stated parity metric, trivially met when bit-exact
+        assert rel_linf(Ug[q], U[q]) <= 1e-5
+
+
+def test_ref32_drop_in_lab_driver(mpcf):
+    """LSRK3_IntegratorMPI::operator() shape driving the GPUlab mirror."""
+    dims = (24, 20, 16)
+    U = cloud_state(dims, nb=2)
+    R = [np.zeros_like(a) for a in U]
+    host_U = [a.copy() for a in U]
+    host_R = [a.copy() for a in R]
+    with mpcf.Solver([dims], precision="fp32_ref") as s:
+        s.set_state(U, R)
+        lab = mpcf.GPUlab(s, nslices=dims[2], host_state=host_U, host_reg=host_R, sync_host=True)
+        dt = mpcf.lsrk3_step(lab, 1.0 / max(dims), 0.3)
+    dt_o, _ = O.step(dims, (ABS,) * 6, U, R, cfl=0.3)
+    assert dt == dt_o
+    assert_bitwise(host_U, U, "state")
+    assert_bitwise(host_R, R, "register")
+
+
+def test_sos_matches_oracle(mpcf):
+    dims = (33, 17, 9)
+    U = cloud_state(dims, nb=2)
+    with mpcf.Solver([dims], precision="fp32_ref") as s:
+        s.set_state(U)
+        sos = s.max_sos()[0]
+    assert np.float32(sos) == np.float32(O.max_sos([np.asarray(a) for a in U]))
+
+
+def test_ghost_fill_matches_oracle(mpcf):
+    dims = (11, 9, 7)
+    U = cloud_state(dims, nb=1)
+    for bc in [(ABS,) * 6, (REF,) * 6, (ABS, REF, REF, ABS, REF, ABS)]:
+        with mpcf.Solver([dims], bc=[bc], precision="fp32_ref") as s:
+            s.set_state(U)
+            gx, gy, gz = s.fill_ghosts()
+        ox, oy, oz = O.fill_ghosts(dims, bc, [np.asarray(a) for a in U])
+        assert np.array_equal(gx, ox) and np.array_equal(gy, oy) and np.array_equal(gz, oz)
+
+
+def test_graph_and_plain_steps_agree(mpcf):
+    dims = (40, 24, 18)
+    U = cloud_state(dims, nb=2)
+    outs = []
+    for graph in (False, True):
+        with mpcf.Solver([dims], precision="fp32_ref") as s:
+            s.set_state(U)
+            t = s.run(4, cfl=0.3, graph=graph)
+            outs.append((t, s.get_state()))
+    assert outs[0][0] == outs[1][0]
+    assert_bitwise(outs[0][1][0], outs[1][1][0], "graph vs plain state")
+
+
+def test_ensemble_matches_single_domains(mpcf):
+    dims = [(32, 16, 8), (21, 30, 12), (48, 8, 10)]
+    bcs = [(ABS,) * 6, (REF,) * 6, (ABS, REF, ABS, REF, ABS, REF)]
+    states = [cloud_state(d, nb=2, seed=3 + i) for i, d in enumerate(dims)]
+    with mpcf.Solver(dims, bc=bcs, precision="fp32_ref") as s:
+        s.set_tiling(4, 8, True)
+        for i, U in enumerate(states):
+            s.set_state(U, dom=i)
+        dts = s.step(cfl=0.3)
+        got = [s.get_state(dom=i) for i in range(len(dims))]
+    for i, d in enumerate(dims):
+        U = [np.array(a) for a in states[i]]
+        R = [np.zeros_like(a) for a in U]
+        dt_o, _ = O.step(d, bcs[i], U, R, cfl=0.3)
+        assert dts[i] == dt_o
+        assert_bitwise(got[i][0], U, f"domain {i} state")
+        assert_bitwise(got[i][1], R, f"domain {i} register")
+
+
+# ---------------------------------------------------------------------------
+# fast FP32, mixed and FP64
+# ---------------------------------------------------------------------------
+def test_fp64_matches_fp64_oracle(mpcf):
+    dims = (30, 22, 14)
+    bc = (ABS, REF, ABS, ABS, REF, ABS)
+    U0 = cloud_state(dims, nb=2, dtype=np.float64)
+    U = [np.array(a) for a in U0]
+    R = [np.zeros_like(a) for a in U]
+    with mpcf.Solver([dims], bc=[bc], precision="fp64") as s:
+        s.set_state(U, R)
+        dt = s.step(cfl=0.3)[0]
+        Ug, Rg = s.get_state()
+    dt_o, _ = O.step(dims, bc, U, R, cfl=0.3)
+    assert abs(dt - dt_o) <= 1e-14 * dt_o
+    for q in range(7):   # FP64 tolerance: FMA contraction and division order only
+        assert rel_linf(Ug[q], U[q]) <= 1e-12, q
+        assert rel_linf(Rg[q], R[q]) <= 1e-10, q
+
+
+@pytest.mark.parametrize("prec", ["fp32", "mixed"])
+def test_fast_forms_one_stage_close(mpcf, prec):
+    """One stage from identical inputs: rounding differences only (tol 1e-5)."""
+    dims = (40, 26, 18)
+    U0 = cloud_state(dims, nb=2)
+    (Ug, Rg), (Uo, Ro) = run_pair(mpcf, dims, (ABS,) * 6, prec, U0, stages=[(0.0, 0.25, 0.057)])
+    for q in range(7):
+        assert rel_linf(Ug[q], Uo[q]) <= 1e-5, (q, rel_linf(Ug[q], Uo[q]))
+        assert rel_linf(Rg[q], Ro[q]) <= 1e-4, (q, rel_linf(Rg[q], Ro[q]))
+
+
+def test_error_word_flags_nonphysical(mpcf):
+    """A state with negative density raises the device error bit, no fault."""
+    dims = (16, 8, 6)
+    U = cloud_state(dims, nb=1)
+    U[0][5] = -1.0
+    with mpcf.Solver([dims], precision="fp32_ref") as s:
+        s.set_state(U)
+        s.stage(0.0, 0.25, 0.05)
+        w = s.error_word(clear=True)
+        assert w & mpcf._lib.ERRBIT_NONPHYSICAL
+        assert s.error_word() == 0
