@@ -43,18 +43,13 @@ UNIT = "cell-stage updates/s"
 BYTES_PER_CELL_STAGE = {"fp32_ref": 112, "fp32": 112, "mixed": 112, "fp64": 224}
 
 
-def flops_per_cell_stage():
-    """Algorithmic FP operations of one cell-stage, counted from the oracle's
-    operation mix: written down once, used for the compute
-    roofline."""
-    return FLOPS_PER_CELL_STAGE
-
-
-# filled from the operation count of the face pipeline (oracle restatement,
-# counting add/sub/mul/compare/min/max = 1, FMA = 2, div = 1, sqrt = 1):
-# per face 14 WENO reconstructions + wave speeds + 7 HLLC fluxes + u*,
-# three faces per cell, plus primitive conversion, divergence and update.
-FLOPS_PER_CELL_STAGE = None
+# Algorithmic floating-point operations of one cell-stage, counted by
+# oracle/count_ops (the oracle's face pipeline run with an operation-counting
+# number type; add/sub/mul/div/sqrt/compare/min/max = 1, FMA = 2):
+# 3 faces x 1546 (WENO5 x 14, wave speeds, HLLC, u*) + 13 (primitive
+# conversion, once per cell) + 91 (extra terms, divergence, updates).
+# tests/test_oracle.py checks this constant against the counter.
+FLOPS_PER_CELL_STAGE = 4742
 
 
 def env_rank():
@@ -348,12 +343,14 @@ def main():
 
 
 def pick_tiling(mpcf, s):
-    """Tiling for the bench: the autotuned choice when available."""
+    """Tiling for the bench: MPCF_TILING="ty,dz,persistent" if set, else the
+    library's autotuner on the solver's own state (state left unchanged)."""
     env = os.environ.get("MPCF_TILING")
     if env:
         ty, dz, p = (int(v) for v in env.split(","))
         return ty, dz, bool(p)
-    return s.tiling()
+    best, _ = s.autotune(reps=2)
+    return best
 
 
 def e2e_measure(mpcf, cfg, K, W, cfl, dist):

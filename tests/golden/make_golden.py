@@ -1,0 +1,153 @@
+"""Generate the golden vectors that pin the oracle to the reference.
+
+Run where the reference tree is present, after `make -C oracle ref`:
+
+    python tests/golden/make_golden.py
+
+It calls the reference's own code compiled from its sources (oracle/_ref):
+  * source/GPU/GPUonly.cuh device math (WENO5 +/- with clipping, Einfeldt,
+    Batten s*, HLLC rho/vel/pvel/e, extra-term velocity, stencil reads),
+  * source/BoundaryConditions.h absorbing/reflecting ghost fills,
+  * source/MaxSpeedOfSound.cpp (MaxSpeedOfSound_CPP::compute),
+on seeded inputs, and stores inputs and outputs as .npz fixtures next to
+this script.  The reference has no golden vectors or known-answer tests of
+its own; these fixtures are its outputs, recorded here.
+"""
+import ctypes
+import os
+import sys
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.dirname(HERE))
+import oracle_lib as O  # noqa: E402
+
+F = ctypes.c_float
+
+
+def weno_inputs(rng, n):
+    """Stencils of 6 values: smooth, jumps, flat, tiny, large, mixed signs."""
+    out = []
+    for k in range(n):
+        kind = k % 6
+        if kind == 0:
+            base = rng.uniform(-10, 10)
+            v = base + np.cumsum(rng.normal(0, 0.1, 6))
+        elif kind == 1:
+            lo, hi = rng.uniform(0.5, 2.0), rng.uniform(500, 1000)
+            cut = rng.integers(1, 6)
+            v = np.where(np.arange(6) < cut, lo, hi) * (1 + rng.normal(0, 1e-3, 6))
+        elif kind == 2:
+            v = np.full(6, rng.uniform(-100, 100))
+        elif kind == 3:
+            v = rng.normal(0, 1e-3, 6)
+        elif kind == 4:
+            v = rng.uniform(4000, 5000, 6)
+        else:
+            v = rng.normal(0, 1, 6) * 10 ** rng.uniform(-4, 3)
+        out.append(v.astype(np.float32))
+    return np.array(out, np.float32)
+
+
+def states(rng, n):
+    """Left/right face states: rho, u, v, w, p, G, P on both sides."""
+    liquid = rng.random(n) < 0.5
+    rm = np.where(liquid, rng.uniform(900, 1000, n), rng.uniform(0.5, 20, n))
+    rp = np.where(rng.random(n) < 0.5, rm * (1 + rng.normal(0, 1e-3, n)), rng.uniform(0.5, 1000, n))
+    vel = rng.normal(0, 1, (6, n)) * 10 ** rng.uniform(-4, 0.5, (6, n))
+    pm = rng.uniform(0.02, 2000, n)
+    pp = np.where(rng.random(n) < 0.3, pm, rng.uniform(0.02, 2000, n))
+    Gm = rng.uniform(0.1789, 2.5, n)
+    Gp = rng.uniform(0.1789, 2.5, n)
+    Pm = rng.uniform(0, 4829, n)
+    Pp = rng.uniform(0, 4829, n)
+    return np.array([rm, rp, *vel, pm, pp, Gm, Gp, Pm, Pp], np.float32).T
+
+
+def make_devmath(L, rng):
+    W = weno_inputs(rng, 3000)
+    wm = np.array([L.ref_weno_minus_clipped(*map(float, w[:5])) for w in W], np.float32)
+    wp = np.array([L.ref_weno_pluss_clipped(*map(float, w[1:])) for w in W], np.float32)
+    wmu = np.array([L.ref_weno_minus(*map(float, w[:5])) for w in W], np.float32)
+    wpu = np.array([L.ref_weno_pluss(*map(float, w[1:])) for w in W], np.float32)
+
+    S = states(rng, 3000)
+    out2 = (F * 2)()
+    sm = np.empty(len(S), np.float32)
+    sp = np.empty(len(S), np.float32)
+    ss = np.empty(len(S), np.float32)
+    hr, hv, hpv, he, hx = (np.empty(len(S), np.float32) for _ in range(5))
+    for i, st in enumerate(S):
+        rm, rp, um, up, vm, vp, wm_, wp_, pm, pp, Gm, Gp, Pm, Pp = map(float, st)
+        L.ref_char_vel_einfeldt(rm, rp, um, up, pm, pp, Gm, Gp, Pm, Pp, out2)
+        sm[i], sp[i] = out2[0], out2[1]
+        s_ = L.ref_char_vel_star(rm, rp, um, up, pm, pp, float(sm[i]), float(sp[i]))
+        if i % 7 == 0:
+            s_ = 0.0     # exercise the sign_star == 0 branch
+        ss[i] = s_
+        a = (float(sm[i]), float(sp[i]), float(ss[i]))
+        hr[i] = L.ref_hllc_rho(rm, rp, um, up, *a)
+        hv[i] = L.ref_hllc_vel(rm, rp, vm, vp, um, up, *a)
+        hpv[i] = L.ref_hllc_pvel(rm, rp, um, up, pm, pp, *a)
+        he[i] = L.ref_hllc_e(rm, rp, um, up, vm, vp, wm_, wp_, pm, pp, Gm, Gp, Pm, Pp, *a)
+        hx[i] = L.ref_extraterm_hllc_vel(um, up, Gm, Gp, Pm, Pp, *a)
+    np.savez_compressed(os.path.join(HERE, "ref_devmath.npz"), weno_in=W, weno_minus_clipped=wm,
+                        weno_pluss_clipped=wp, weno_minus=wmu, weno_pluss=wpu, states=S, sm=sm, sp=sp,
+                        ss=ss, hllc_rho=hr, hllc_vel=hv, hllc_pvel=hpv, hllc_e=he, extraterm=hx)
+
+
+def cloud(dims, seed):
+    import mpcf
+    params, bub = mpcf.configs.small_cloud(dims, nb=2, seed=seed)
+    return [np.ascontiguousarray(a) for a in mpcf.ic_cloud_host(dims, params, bub, np.float32)]
+
+
+def make_bc(rng):
+    combos = [(0,) * 6, (1,) * 6, (0, 1, 1, 0, 1, 0), (1, 0, 0, 1, 0, 1)]
+    rec = {}
+    for name in ("libref_bc_8x7x6", "libref_bc_16x16x16"):
+        L = O.ref_lib(name)
+        d = (ctypes.c_int * 3)()
+        L.ref_bc_dims(d)
+        dims = (d[0], d[1], d[2])
+        U = cloud(dims, 5)
+        for ci, bc in enumerate(combos):
+            nx, ny, nz = dims
+            gx = np.zeros(2 * 7 * 3 * ny * nz, np.float32)
+            gy = np.zeros(2 * 7 * nx * 3 * nz, np.float32)
+            gz = np.zeros(2 * 7 * nx * ny * 3, np.float32)
+            L.ref_fill_ghosts(O.bc_arr(bc), O.fptrs(U), gx.ctypes.data_as(ctypes.POINTER(F)),
+                              gy.ctypes.data_as(ctypes.POINTER(F)), gz.ctypes.data_as(ctypes.POINTER(F)))
+            key = f"{dims[0]}x{dims[1]}x{dims[2]}_{ci}"
+            rec[key + "_dims"] = np.array(dims)
+            rec[key + "_bc"] = np.array(bc)
+            rec[key + "_U"] = np.array(U)
+            rec[key + "_gx"], rec[key + "_gy"], rec[key + "_gz"] = gx, gy, gz
+    np.savez_compressed(os.path.join(HERE, "ref_bc.npz"), **rec)
+
+
+def make_sos():
+    L = O.ref_lib("libref_sos")
+    rec = {}
+    for i, dims in enumerate([(24, 20, 16), (40, 33, 7)]):
+        U = cloud(dims, 21 + i)
+        rec[f"U{i}"] = np.array(U)
+        rec[f"sos{i}"] = np.float32(L.ref_max_sos_cpp(U[0].size, O.fptrs(U)))
+    np.savez_compressed(os.path.join(HERE, "ref_sos.npz"), **rec)
+
+
+def main():
+    sys.path.insert(0, os.path.join(os.path.dirname(os.path.dirname(HERE)), "cubism-jr-gpu-mpcf_b200"))
+    L = O.ref_lib("libref_devmath_8x7x6")
+    if L is None:
+        raise SystemExit("oracle/_ref not built (needs the reference tree): make -C oracle ref")
+    rng = np.random.default_rng(20261203)
+    make_devmath(L, rng)
+    make_bc(rng)
+    make_sos()
+    print("wrote", sorted(f for f in os.listdir(HERE) if f.endswith(".npz")))
+
+
+if __name__ == "__main__":
+    main()
