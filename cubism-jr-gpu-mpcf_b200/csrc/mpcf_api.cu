@@ -102,9 +102,9 @@ bool valid_ty(const mpcf_solver* s, int ty)
     return ty == 16 && s->pol == 0;
 }
 
-StageKernelInfo stage_info(const mpcf_solver* s, int ty, bool persist)
+StageKernelInfo stage_info(const mpcf_solver* s, int ty, bool persist, bool sums = false)
 {
-    return s->pol == 0 ? stage_info_ref(ty, persist) : stage_info_fast(s->pol, ty, persist);
+    return s->pol == 0 ? stage_info_ref(ty, persist, sums) : stage_info_fast(s->pol, ty, persist, sums);
 }
 
 void destroy_graphs(mpcf_solver* s)
@@ -369,9 +369,9 @@ int mpcf_create(mpcf_solver** out, int ndomains, const int* dims, const int* bc,
     for (int i = 0; i < 4; ++i)
     {
         if (!valid_ty(s, tys[i])) continue;
-        for (int p = 0; p < 2; ++p)
+        for (int p = 0; p < 4; ++p)
         {
-            StageKernelInfo I = stage_info(s, tys[i], p != 0);
+            StageKernelInfo I = stage_info(s, tys[i], (p & 1) != 0, (p & 2) != 0);
             if (!I.fn) continue;
             if (cudaFuncSetAttribute(I.fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)I.smem) != cudaSuccess)
             { cudaGetLastError(); return bail(fail(MPCF_ERR_CUDA, "cannot grant %zu B shared memory to the stage kernel (ty=%d)", I.smem, tys[i])); }
@@ -915,6 +915,38 @@ int mpcf_time_run(mpcf_solver* s, int nsteps, double cfl, double dt_max, double*
     cudaEventDestroy(e1);
     s->sums_valid = s->track_cons;
     *ms = t;
+    return MPCF_OK;
+}
+
+int mpcf_update(mpcf_solver* s, double b)
+{
+    if (!s) return fail(MPCF_ERR_ARG, "null solver");
+    DeviceGuard g(s->device);
+    CK(launch_update(s->esz == 8, s->ddoms, s->ndom, s->parity, b, s->stream));
+    s->parity ^= 1;
+    s->sums_valid = false;
+    CK(cudaStreamSynchronize(s->stream));
+    return MPCF_OK;
+}
+
+int mpcf_device_info(int device, char* name, int name_len, long long* total_bytes, long long* free_bytes, int* sms)
+{
+    DeviceGuard g(device);
+    cudaDeviceProp p;
+    CK(cudaGetDeviceProperties(&p, device));
+    if (name && name_len > 0) { strncpy(name, p.name, (size_t)name_len - 1); name[name_len - 1] = 0; }
+    if (sms) *sms = p.multiProcessorCount;
+    size_t fr = 0, tot = 0;
+    CK(cudaMemGetInfo(&fr, &tot));
+    if (total_bytes) *total_bytes = (long long)tot;
+    if (free_bytes) *free_bytes = (long long)fr;
+    return MPCF_OK;
+}
+
+int mpcf_device_synchronize(int device)
+{
+    DeviceGuard g(device);
+    CK(cudaDeviceSynchronize());
     return MPCF_OK;
 }
 

@@ -335,4 +335,33 @@ cudaError_t launch_fma_probe(int blocks, int iters, float* out, cudaStream_t st)
     return cudaGetLastError();
 }
 
+// ---------------------------------------------------------------------------
+// State update alone, U_next = b*R + U (the reference's _update,
+// GPUkernels.cu:1142-1179), for callers that run Convection and Update as
+// two separate steps (Convection_CUDA / Update_CUDA).  The fused stage
+// kernel does the same arithmetic inline.
+// ---------------------------------------------------------------------------
+template <class T>
+__global__ void update_kernel(const DomDev* doms, int ndom, int parity, T b)
+{
+    for (int d = 0; d < ndom; ++d)
+    {
+        const DomDev& D = doms[d];
+        const long long N = (long long)D.nx * D.ny * D.nz;
+        const T* U = (const T*)D.U[parity];
+        T* Un = (T*)D.U[parity ^ 1];
+        const T* R = (const T*)D.R;
+        for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < N; i += (long long)gridDim.x * blockDim.x)
+            for (int m = 0; m < 7; ++m)
+                Un[m * D.fs + i] = b * R[m * D.fs + i] + U[m * D.fs + i];
+    }
+}
+
+cudaError_t launch_update(int is_double, const DomDev* doms, int ndom, int parity, double b, cudaStream_t st)
+{
+    if (is_double) update_kernel<double><<<148 * 8, 256, 0, st>>>(doms, ndom, parity, b);
+    else           update_kernel<float><<<148 * 8, 256, 0, st>>>(doms, ndom, parity, (float)b);
+    return cudaGetLastError();
+}
+
 } // namespace mpcf

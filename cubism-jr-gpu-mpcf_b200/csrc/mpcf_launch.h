@@ -16,8 +16,8 @@ struct StageKernelInfo
 // precision policy ids: 0 FP32 reference rounding, 1 fast FP32, 2 mixed, 3 FP64
 cudaError_t launch_stage_ref(int ty, bool persist, const StageArgs& A, int grid, cudaStream_t st);
 cudaError_t launch_stage_fast(int pol, int ty, bool persist, const StageArgs& A, int grid, cudaStream_t st);
-StageKernelInfo stage_info_ref(int ty, bool persist);
-StageKernelInfo stage_info_fast(int pol, int ty, bool persist);
+StageKernelInfo stage_info_ref(int ty, bool persist, bool sums);
+StageKernelInfo stage_info_fast(int pol, int ty, bool persist, bool sums);
 
 // mpcf_aux.cu
 cudaError_t launch_sos(int pol, const SosArgs& A, cudaStream_t st);
@@ -28,6 +28,7 @@ cudaError_t launch_ic_cloud(int is_double, const DomDev* dom, int parity, const 
 cudaError_t launch_fill_ghosts(int is_double, const DomDev* dom, int parity,
                                void* gx, void* gy, void* gz, cudaStream_t st);
 cudaError_t launch_zero(void* p, size_t bytes, cudaStream_t st);
+cudaError_t launch_update(int is_double, const DomDev* doms, int ndom, int parity, double b, cudaStream_t st);
 cudaError_t launch_fma_probe(int blocks, int iters, float* out, cudaStream_t st);
 cudaError_t launch_sum_state(const DomDev* doms, int ndom, int parity, int nchunks, int chunk, int is_double,
                              double* chunk_sums, double* out, cudaStream_t st);

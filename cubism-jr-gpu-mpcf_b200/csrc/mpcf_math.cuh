@@ -15,8 +15,9 @@
 //              operation rounds exactly like the literal C semantics of the
 //              reference source: results are bit-identical to the CPU
 //              restatement built with -ffp-contract=off.
-//   PolFast32  float everywhere; WENO weights from single-precision
-//              reciprocals, fused multiply-adds allowed.
+//   PolFast32  float everywhere; WENO smoothness indicators in factored
+//              (cancellation-free, shared-curvature) form, weights from
+//              single-precision reciprocals, fused multiply-adds allowed.
 //   PolMixed   PolFast32 plus the stiffened-gas pressure recovery in FP64
 //              and FP64 conservation sums.
 //   PolFP64    double storage and arithmetic (the all-FP64 GPU oracle run).
@@ -153,6 +154,50 @@ __device__ __forceinline__ typename Pol::T weno_pluss_clipped(const typename Pol
     return dmin(dmax(r, mn), mx);
 }
 
+// Both reconstructions of one face from its 6-cell stencil s0..s5, in the
+// fast policies: the smoothness indicators are the same Jiang-Shu
+// polynomials as the reference's expanded forms (beta_f, beta_h, beta_g
+// above; the coefficients agree term by term), evaluated in factored form
+//   beta_f = 13/12 (x-2y+z)^2 + 1/4 (x-4y+3z)^2
+//   beta_h = 13/12 (x-2y+z)^2 + 1/4 (x-z)^2
+//   beta_g = 13/12 (x-2y+z)^2 + 1/4 (3x-4y+z)^2
+// so the curvature term of each of the four windows the face touches is
+// computed once and shared by the minus and plus sides, and no term
+// cancels catastrophically (the expanded form cancels ~1e4-sized products
+// down to ~1e-6 on smooth liquid stencils in FP32).
+template <class Pol>
+__device__ __forceinline__ void weno_pair_factored(const typename Pol::T s0, const typename Pol::T s1,
+        const typename Pol::T s2, const typename Pol::T s3, const typename Pol::T s4, const typename Pol::T s5,
+        typename Pol::T& m, typename Pol::T& p)
+{
+    typedef typename Pol::T T;
+    const T c1312 = (T)(13. / 12.), c14 = (T)0.25;
+    // curvature of windows (s0,s1,s2) .. (s3,s4,s5)
+    const T k0 = s0 - (T)2 * s1 + s2;
+    const T k1 = s1 - (T)2 * s2 + s3;
+    const T k2 = s2 - (T)2 * s3 + s4;
+    const T k3 = s3 - (T)2 * s4 + s5;
+    const T K0 = c1312 * k0 * k0, K1 = c1312 * k1 * k1, K2 = c1312 * k2 * k2, K3 = c1312 * k3 * k3;
+    // minus side: f(s0,s1,s2), h(s1,s2,s3), g(s2,s3,s4)
+    {
+        const T a = s0 - (T)4 * s1 + (T)3 * s2, b = s1 - s3, c = (T)3 * s2 - (T)4 * s3 + s4;
+        const T is0 = K0 + c14 * a * a, is1 = K1 + c14 * b * b, is2 = K2 + c14 * c * c;
+        T w0, w1, w2;
+        weno_weights<Pol>(is0, is1, is2, w0, w1, w2);
+        const T r = w0*((T)(1.0/3.)*s0-(T)(7./6.)*s1+(T)(11./6.)*s2) + w1*(-(T)(1./6.)*s1+(T)(5./6.)*s2+(T)(1./3.)*s3) + w2*((T)(1./3.)*s2+(T)(5./6.)*s3-(T)(1./6.)*s4);
+        m = dmin(dmax(r, dmin(dmin(s1, s2), s3)), dmax(dmax(s1, s2), s3));
+    }
+    // plus side: g(s3,s4,s5), h(s2,s3,s4), f(s1,s2,s3)
+    {
+        const T a = (T)3 * s3 - (T)4 * s4 + s5, b = s2 - s4, c = s1 - (T)4 * s2 + (T)3 * s3;
+        const T is0 = K3 + c14 * a * a, is1 = K2 + c14 * b * b, is2 = K1 + c14 * c * c;
+        T w0, w1, w2;
+        weno_weights<Pol>(is0, is1, is2, w0, w1, w2);
+        const T r = w0*((T)(1./3.)*s5-(T)(7./6.)*s4+(T)(11./6.)*s3) + w1*(-(T)(1./6.)*s4+(T)(5./6.)*s3+(T)(1./3.)*s2) + w2*((T)(1./3.)*s3+(T)(5./6.)*s2-(T)(1./6.)*s1);
+        p = dmin(dmax(r, dmin(dmin(s2, s3), s4)), dmax(dmax(s2, s3), s4));
+    }
+}
+
 // ---------------------------------------------------------------------------
 // HLLC pieces.  sign_star in {-1,0,1}; the two weights (1+s)/2 and (1-s)/2.
 // ---------------------------------------------------------------------------
@@ -189,10 +234,13 @@ struct FaceState
     T rm, rp, nm, np, t1m, t1p, t2m, t2p, pm, pp, Gm, Gp, Pm, Pp;
 };
 
-// Wave speeds + HLLC fluxes for direction DIR (GPUkernels.cu:255-289 for x,
-// :636-668 for y, :932-963 for z; GPUonly.cuh:802-1042).
-template <class Pol, int DIR>
-__device__ __forceinline__ void hllc_face(const FaceState<typename Pol::T>& S, FaceOut<typename Pol::T>& o)
+// Wave speeds + HLLC fluxes of one face (GPUkernels.cu:255-289 for x,
+// :636-668 for y, :932-963 for z; GPUonly.cuh:802-1042).  `dir` is a runtime
+// value: the normal / transverse momenta are scattered with selects, so one
+// instance of this code serves all three directions (the face pipeline is
+// ~1000 instructions; one copy keeps it resident in the instruction cache).
+template <class Pol>
+__device__ __forceinline__ void hllc_face(const FaceState<typename Pol::T>& S, const int dir, FaceOut<typename Pol::T>& o)
 {
     typedef typename Pol::T T;
     const T rm = S.rm, rp = S.rp, um = S.nm, up = S.np;
@@ -268,29 +316,35 @@ __device__ __forceinline__ void hllc_face(const FaceState<typename Pol::T>& S, F
     // extra-term velocity: _extraterm_hllc_vel (GPUonly.cuh:1029-1042)
     o.vel = hllc_blend<Pol, false>(s, um + s_minus*(chi_m - (T)1.0f), up + s_pluss*(chi_p - (T)1.0f));
 
-    // scatter normal / transverse momenta to (rho u, rho v, rho w)
-    if (DIR == 0)      { o.f[1] = fn;  o.f[2] = ft1; o.f[3] = ft2; }
-    else if (DIR == 1) { o.f[1] = ft1; o.f[2] = fn;  o.f[3] = ft2; }
-    else               { o.f[1] = ft1; o.f[2] = ft2; o.f[3] = fn;  }
+    // normal / transverse momenta back to (rho u, rho v, rho w):
+    // x: (n, t1, t2), y: (t1, n, t2), z: (t1, t2, n)
+    o.f[1] = dir == 0 ? fn : ft1;
+    o.f[2] = dir == 1 ? fn : (dir == 0 ? ft1 : ft2);
+    o.f[3] = dir == 2 ? fn : ft2;
     o.Gm = Gm; o.Gp = Gp; o.Pm = Pm; o.Pp = Pp;
 }
 
-// Full face: fetch(q, j) returns primitive q of stencil cell j (j = 0..5 for
-// cells i-3..i+2 around face i-1/2).
-template <class Pol, int DIR, class Fetch>
-__device__ __forceinline__ void face_flux(const Fetch& fetch, FaceOut<typename Pol::T>& o)
+// Full face from primitives in shared memory: cell j (j = 0..5 for cells
+// i-3..i+2 around face i-1/2) of primitive plane q sits at
+// sm[base + q*pitch + offs[j]].  The velocity planes are permuted by `dir`
+// into (normal, first transverse, second transverse) as the reference
+// passes them to the HLLC functions.
+template <class Pol>
+__device__ __forceinline__ void face_flux(const typename Pol::T* __restrict__ sm, const int base, const int pitch,
+                                          const int (&offs)[6], const int dir, FaceOut<typename Pol::T>& o)
 {
     typedef typename Pol::T T;
     FaceState<T> S;
-    // component indices of the normal / transverse velocities (1=u,2=v,3=w)
-    constexpr int qn  = 1 + DIR;
-    constexpr int qt1 = DIR == 0 ? 2 : 1;
-    constexpr int qt2 = DIR == 2 ? 2 : 3;
+    const int qn  = 1 + dir;
+    const int qt1 = dir == 0 ? 2 : 1;
+    const int qt2 = dir == 2 ? 2 : 3;
 #define MPCF_RECON(q, M, P) { \
-        const T s0 = fetch(q, 0), s1 = fetch(q, 1), s2 = fetch(q, 2), \
-                s3 = fetch(q, 3), s4 = fetch(q, 4), s5 = fetch(q, 5); \
-        M = weno_minus_clipped<Pol>(s0, s1, s2, s3, s4); \
-        P = weno_pluss_clipped<Pol>(s1, s2, s3, s4, s5); }
+        const T* b_ = sm + base + (q) * pitch; \
+        const T s0 = b_[offs[0]], s1 = b_[offs[1]], s2 = b_[offs[2]], \
+                s3 = b_[offs[3]], s4 = b_[offs[4]], s5 = b_[offs[5]]; \
+        if (Pol::kFastWeno) weno_pair_factored<Pol>(s0, s1, s2, s3, s4, s5, M, P); \
+        else { M = weno_minus_clipped<Pol>(s0, s1, s2, s3, s4); \
+               P = weno_pluss_clipped<Pol>(s1, s2, s3, s4, s5); } }
     MPCF_RECON(0,   S.rm,  S.rp);
     MPCF_RECON(qn,  S.nm,  S.np);
     MPCF_RECON(qt1, S.t1m, S.t1p);
@@ -299,7 +353,7 @@ __device__ __forceinline__ void face_flux(const Fetch& fetch, FaceOut<typename P
     MPCF_RECON(5,   S.Gm,  S.Gp);
     MPCF_RECON(6,   S.Pm,  S.Pp);
 #undef MPCF_RECON
-    hllc_face<Pol, DIR>(S, o);
+    hllc_face<Pol>(S, dir, o);
 }
 
 // Conserved (rho, rho u, rho v, rho w, E, G, P) -> primitives (rho, u, v, w,

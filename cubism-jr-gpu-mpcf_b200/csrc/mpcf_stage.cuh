@@ -39,15 +39,29 @@ namespace mpcf {
 
 constexpr int kTX = 32;
 
+// Shared-memory layout of one CTA, as element offsets into one array of T
+// (so every stencil, x, y or z, is addressed as base + q*pitch + offs[j]):
+//   zwin  [6 slots][7 planes][TY][32]     ring of the tile's own columns
+//   cur   [7 planes][TY+6][38]            slab k with 3-cell x/y halos
+//   fx    [12][TY][33]                    x faces of slab k
+//   fy    [12][TY+1][32]                  y faces of slab k
+// followed by the FP64 reduction scratch [TY][5] and the tile broadcast.
 template <class T, int TY>
-struct StageSmem
+struct StageLayout
 {
-    T zwin[6][7][TY][kTX];          // ring of the tile's own columns
-    T cur[7][TY + 6][kTX + 6];      // slab k with 3-cell x/y halos
-    T fx[12][TY][kTX + 1];          // x faces of slab k
-    T fy[12][TY + 1][kTX];          // y faces of slab k
-    double red[TY][5];              // block reduction of conservation sums
-    int tile;
+    static constexpr int kCurW   = kTX + 6;
+    static constexpr int kZPlane = TY * kTX;               // zwin plane pitch
+    static constexpr int kZSlot  = 7 * kZPlane;            // zwin slot pitch
+    static constexpr int kCurP   = (TY + 6) * kCurW;       // cur plane pitch
+    static constexpr int kFxP    = TY * (kTX + 1);         // fx plane pitch
+    static constexpr int kFyP    = (TY + 1) * kTX;         // fy plane pitch
+    static constexpr int kZwin   = 0;
+    static constexpr int kCur    = kZwin + 6 * kZSlot;
+    static constexpr int kFx     = kCur + 7 * kCurP;
+    static constexpr int kFy     = kFx + 12 * kFxP;
+    static constexpr int kEnd    = kFy + 12 * kFyP;
+    static constexpr size_t kRedBytes = ((kEnd * sizeof(T) + 15) / 16) * 16;
+    static constexpr size_t kBytes = kRedBytes + sizeof(double) * TY * 5 + 16;
 };
 
 // Boundary-condition map of one coordinate: absorbing clamps to the edge
@@ -99,21 +113,26 @@ __device__ __forceinline__ bool physical(const T r, const T e, const T G, const 
 // Register budget: at least kMinWarpsPerSM resident warps per SM.  The
 // face pipeline has 14 independent reconstructions, so the compiler would
 // otherwise trade occupancy for unbounded instruction-level parallelism.
+// FP64 values take two registers, so its budget is half the warps.
 #ifndef MPCF_MIN_WARPS_PER_SM
 #define MPCF_MIN_WARPS_PER_SM 16
 #endif
-template <int TY> struct MinBlocks
+template <class T, int TY> struct MinBlocks
 {
-    static constexpr int v = (MPCF_MIN_WARPS_PER_SM / TY) > 0 ? (MPCF_MIN_WARPS_PER_SM / TY) : 1;
+    static constexpr int w = sizeof(T) == 8 ? MPCF_MIN_WARPS_PER_SM / 2 : MPCF_MIN_WARPS_PER_SM;
+    static constexpr int v = (w / TY) > 0 ? (w / TY) : 1;
 };
 
-template <class Pol, int TY, bool PERSIST>
-__global__ void __launch_bounds__(kTX * TY, MinBlocks<TY>::v)
+template <class Pol, int TY, bool PERSIST, bool SUMS>
+__global__ void __launch_bounds__(kTX * TY, MinBlocks<typename Pol::T, TY>::v)
 stage_kernel(const StageArgs A)
 {
     typedef typename Pol::T T;
+    typedef StageLayout<T, TY> L;
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    StageSmem<T, TY>& S = *reinterpret_cast<StageSmem<T, TY>*>(smem_raw);
+    T* sm = reinterpret_cast<T*>(smem_raw);
+    double* red = reinterpret_cast<double*>(smem_raw + L::kRedBytes);
+    int* tile_bc = reinterpret_cast<int*>(smem_raw + L::kRedBytes + sizeof(double) * TY * 5);
 
     const int tx = threadIdx.x & (kTX - 1);
     const int ty = threadIdx.x >> 5;
@@ -125,9 +144,9 @@ stage_kernel(const StageArgs A)
     int t;
     if (PERSIST)
     {
-        if (threadIdx.x == 0) S.tile = (int)atomicAdd(A.counter, 1u);
+        if (threadIdx.x == 0) *tile_bc = (int)atomicAdd(A.counter, 1u);
         __syncthreads();
-        t = S.tile;
+        t = *tile_bc;
     }
     else t = blockIdx.x;
 
@@ -156,24 +175,25 @@ stage_kernel(const StageArgs A)
         const int z1 = min(z0 + A.dz, D.nz);
         const int gx = x0 + tx, gy = y0 + ty;
         const bool valid = (gx < D.nx) && (gy < D.ny);
+        const int own = ty * kTX + tx;     // own column inside a zwin plane
 
         // ---- prologue: slabs z0-3 .. z0+1 of the own column into the ring
-        for (int s = z0 - 3; s <= z0 + 1; ++s)
+        for (int sl = z0 - 3; sl <= z0 + 1; ++sl)
         {
             T q[7];
-            load_prim<Pol>(D, U, gx, gy, s, q);
-            const int sl = (s + 6) % 6;
+            load_prim<Pol>(D, U, gx, gy, sl, q);
+            const int slot = (sl + 6) % 6;
 #pragma unroll
-            for (int k = 0; k < 7; ++k) S.zwin[sl][k][ty][tx] = q[k];
+            for (int m = 0; m < 7; ++m) sm[L::kZwin + slot * L::kZSlot + m * L::kZPlane + own] = q[m];
         }
 
         T Sp[7];                 // x/y part of the flux bracket of cell k-1
         T sG = 0, sP = 0, dU = 0;
         T zfp[12];               // z face (k-1)-1/2
 #pragma unroll
-        for (int k = 0; k < 7; ++k) Sp[k] = 0;
+        for (int m = 0; m < 7; ++m) Sp[m] = 0;
 #pragma unroll
-        for (int k = 0; k < 12; ++k) zfp[k] = 0;
+        for (int m = 0; m < 12; ++m) zfp[m] = 0;
         double cs[5] = {0, 0, 0, 0, 0};
 
         for (int k = z0; k <= z1; ++k)
@@ -182,16 +202,17 @@ stage_kernel(const StageArgs A)
             {
                 T q[7];
                 load_prim<Pol>(D, U, gx, gy, k + 2, q);
-                const int sl = (k + 2 + 6) % 6;
+                const int slot = (k + 2 + 6) % 6;
 #pragma unroll
-                for (int m = 0; m < 7; ++m) S.zwin[sl][m][ty][tx] = q[m];
+                for (int m = 0; m < 7; ++m) sm[L::kZwin + slot * L::kZSlot + m * L::kZPlane + own] = q[m];
             }
             // (B) slab k with halos into cur
             if (k < z1)
             {
-                const int sl = (k + 6) % 6;
+                const int slot = (k + 6) % 6;
 #pragma unroll
-                for (int m = 0; m < 7; ++m) S.cur[m][ty + 3][tx + 3] = S.zwin[sl][m][ty][tx];
+                for (int m = 0; m < 7; ++m)
+                    sm[L::kCur + m * L::kCurP + (ty + 3) * L::kCurW + tx + 3] = sm[L::kZwin + slot * L::kZSlot + m * L::kZPlane + own];
                 for (int i = threadIdx.x; i < 6 * kTX + 6 * TY; i += kTX * TY)
                 {
                     int lx, ly;
@@ -211,63 +232,56 @@ stage_kernel(const StageArgs A)
                     T q[7];
                     load_prim<Pol>(D, U, x0 + lx, y0 + ly, k, q);
 #pragma unroll
-                    for (int m = 0; m < 7; ++m) S.cur[m][ly + 3][lx + 3] = q[m];
+                    for (int m = 0; m < 7; ++m) sm[L::kCur + m * L::kCurP + (ly + 3) * L::kCurW + lx + 3] = q[m];
                 }
             }
             __syncthreads();
 
-            // (C) x/y faces of slab k
-            if (k < z1)
-            {
-                FaceOut<T> o;
-                {
-                    auto fx_fetch = [&](int q, int j) -> T { return S.cur[q][ty + 3][tx + j]; };
-                    face_flux<Pol, 0>(fx_fetch, o);
-#pragma unroll
-                    for (int m = 0; m < 7; ++m) S.fx[m][ty][tx] = o.f[m];
-                    S.fx[7][ty][tx] = o.Gm; S.fx[8][ty][tx] = o.Gp;
-                    S.fx[9][ty][tx] = o.Pm; S.fx[10][ty][tx] = o.Pp; S.fx[11][ty][tx] = o.vel;
-                }
-                {
-                    auto fy_fetch = [&](int q, int j) -> T { return S.cur[q][ty + j][tx + 3]; };
-                    face_flux<Pol, 1>(fy_fetch, o);
-#pragma unroll
-                    for (int m = 0; m < 7; ++m) S.fy[m][ty][tx] = o.f[m];
-                    S.fy[7][ty][tx] = o.Gm; S.fy[8][ty][tx] = o.Gp;
-                    S.fy[9][ty][tx] = o.Pm; S.fy[10][ty][tx] = o.Pp; S.fy[11][ty][tx] = o.vel;
-                }
-                if (ty == 0)
-                {
-                    // y faces above the tile (row TY)
-                    auto fy_fetch = [&](int q, int j) -> T { return S.cur[q][TY + j][tx + 3]; };
-                    face_flux<Pol, 1>(fy_fetch, o);
-#pragma unroll
-                    for (int m = 0; m < 7; ++m) S.fy[m][TY][tx] = o.f[m];
-                    S.fy[7][TY][tx] = o.Gm; S.fy[8][TY][tx] = o.Gp;
-                    S.fy[9][TY][tx] = o.Pm; S.fy[10][TY][tx] = o.Pp; S.fy[11][TY][tx] = o.vel;
-                }
-                else if (ty == 1 && tx < TY)
-                {
-                    // x faces right of the tile (column 32), one per row
-                    const int row = tx;
-                    auto fx_fetch = [&](int q, int j) -> T { return S.cur[q][row + 3][kTX + j]; };
-                    face_flux<Pol, 0>(fx_fetch, o);
-#pragma unroll
-                    for (int m = 0; m < 7; ++m) S.fx[m][row][kTX] = o.f[m];
-                    S.fx[7][row][kTX] = o.Gm; S.fx[8][row][kTX] = o.Gp;
-                    S.fx[9][row][kTX] = o.Pm; S.fx[10][row][kTX] = o.Pp; S.fx[11][row][kTX] = o.vel;
-                }
-            }
-
-            // (D) z face k-1/2 of the own column
+            // (C) faces of slab k: job 0 = z face k-1/2 of the own column (kept
+            // in registers), job 1 = x face left of the own cell, job 2 = y face
+            // below it, job 3 = warp 0: y face above the tile (row TY),
+            // warp 1: x face right of the tile (column 32, one per row).
+            // One face instance serves every job (runtime direction/offsets).
             FaceOut<T> zf;
             {
-                const int s0 = (k - 3 + 6) % 6;
-                auto fz_fetch = [&](int q, int j) -> T {
-                    int sl = s0 + j; sl = sl >= 6 ? sl - 6 : sl;
-                    return S.zwin[sl][q][ty][tx];
-                };
-                face_flux<Pol, 2>(fz_fetch, zf);
+                const int njobs = (k < z1) ? ((ty == 0 || (ty == 1 && tx < TY)) ? 4 : 3) : 1;
+#pragma unroll 1
+                for (int job = 0; job < njobs; ++job)
+                {
+                    int base, pitch, dir, dst, dpitch;
+                    int offs[6];
+                    if (job == 0)
+                    {
+                        dir = 2; base = L::kZwin + own; pitch = L::kZPlane; dst = -1; dpitch = 0;
+                        const int s0 = (k - 3 + 6) % 6;
+#pragma unroll
+                        for (int j = 0; j < 6; ++j) { const int sl = s0 + j; offs[j] = (sl >= 6 ? sl - 6 : sl) * L::kZSlot; }
+                    }
+                    else
+                    {
+                        const bool xdir = (job == 1) || (job == 3 && ty == 1);
+                        dir = xdir ? 0 : 1;
+                        pitch = L::kCurP;
+                        const int step = xdir ? 1 : L::kCurW;
+#pragma unroll
+                        for (int j = 0; j < 6; ++j) offs[j] = j * step;
+                        if (job == 1)      { base = L::kCur + (ty + 3) * L::kCurW + tx;  dst = L::kFx + ty * (kTX + 1) + tx; dpitch = L::kFxP; }
+                        else if (job == 2) { base = L::kCur + ty * L::kCurW + tx + 3;    dst = L::kFy + ty * kTX + tx;       dpitch = L::kFyP; }
+                        else if (ty == 0)  { base = L::kCur + TY * L::kCurW + tx + 3;    dst = L::kFy + TY * kTX + tx;       dpitch = L::kFyP; }
+                        else               { base = L::kCur + (tx + 3) * L::kCurW + kTX; dst = L::kFx + tx * (kTX + 1) + kTX; dpitch = L::kFxP; }
+                    }
+                    FaceOut<T> o;
+                    face_flux<Pol>(sm, base, pitch, offs, dir, o);
+                    if (dst < 0) zf = o;
+                    else
+                    {
+#pragma unroll
+                        for (int m = 0; m < 7; ++m) sm[dst + m * dpitch] = o.f[m];
+                        sm[dst + 7 * dpitch] = o.Gm;  sm[dst + 8 * dpitch] = o.Gp;
+                        sm[dst + 9 * dpitch] = o.Pm;  sm[dst + 10 * dpitch] = o.Pp;
+                        sm[dst + 11 * dpitch] = o.vel;
+                    }
+                }
             }
             __syncthreads();
 
@@ -292,7 +306,7 @@ stage_kernel(const StageArgs A)
                     Un[m * D.fs + idx] = un[m];
                 }
                 ok = ok && physical<T>(un[0], un[4], un[5], un[6]);
-                if (A.tile_sums)
+                if (SUMS)
                 {
 #pragma unroll
                     for (int m = 0; m < 5; ++m) cs[m] += (double)un[m];
@@ -302,23 +316,25 @@ stage_kernel(const StageArgs A)
             // (F) x/y part of cell k, carried to the next slab
             if (k < z1)
             {
+                const T* fx = sm + L::kFx + ty * (kTX + 1) + tx;
+                const T* fy = sm + L::kFy + ty * kTX + tx;
 #pragma unroll
                 for (int m = 0; m < 7; ++m)
-                    Sp[m] = ((S.fx[m][ty][tx + 1] - S.fx[m][ty][tx]) + S.fy[m][ty + 1][tx]) - S.fy[m][ty][tx];
-                sG = S.fx[8][ty][tx] + S.fx[7][ty][tx + 1];
-                sP = S.fx[10][ty][tx] + S.fx[9][ty][tx + 1];
-                dU = S.fx[11][ty][tx + 1] - S.fx[11][ty][tx];
-                sG = sG + (S.fy[8][ty][tx] + S.fy[7][ty + 1][tx]);
-                sP = sP + (S.fy[10][ty][tx] + S.fy[9][ty + 1][tx]);
-                dU = dU + (S.fy[11][ty + 1][tx] - S.fy[11][ty][tx]);
+                    Sp[m] = ((fx[m * L::kFxP + 1] - fx[m * L::kFxP]) + fy[m * L::kFyP + kTX]) - fy[m * L::kFyP];
+                sG = fx[8 * L::kFxP] + fx[7 * L::kFxP + 1];
+                sP = fx[10 * L::kFxP] + fx[9 * L::kFxP + 1];
+                dU = fx[11 * L::kFxP + 1] - fx[11 * L::kFxP];
+                sG = sG + (fy[8 * L::kFyP] + fy[7 * L::kFyP + kTX]);
+                sP = sP + (fy[10 * L::kFyP] + fy[9 * L::kFyP + kTX]);
+                dU = dU + (fy[11 * L::kFyP + kTX] - fy[11 * L::kFyP]);
             }
-            zfp[0] = zf.f[0]; zfp[1] = zf.f[1]; zfp[2] = zf.f[2]; zfp[3] = zf.f[3];
-            zfp[4] = zf.f[4]; zfp[5] = zf.f[5]; zfp[6] = zf.f[6];
+#pragma unroll
+            for (int m = 0; m < 7; ++m) zfp[m] = zf.f[m];
             zfp[7] = zf.Gm; zfp[8] = zf.Gp; zfp[9] = zf.Pm; zfp[10] = zf.Pp; zfp[11] = zf.vel;
         }
 
         // ---- per-tile FP64 conservation sums (deterministic: fixed order)
-        if (A.tile_sums)
+        if (SUMS)
         {
 #pragma unroll
             for (int m = 0; m < 5; ++m)
@@ -326,28 +342,28 @@ stage_kernel(const StageArgs A)
                 double v = cs[m];
 #pragma unroll
                 for (int off = 16; off > 0; off >>= 1) v += __shfl_xor_sync(0xffffffffu, v, off);
-                if (tx == 0) S.red[ty][m] = v;
+                if (tx == 0) red[ty * 5 + m] = v;
             }
             __syncthreads();
             if (threadIdx.x < 5)
             {
                 double v = 0;
-                for (int w = 0; w < TY; ++w) v += S.red[w][threadIdx.x];
+                for (int w = 0; w < TY; ++w) v += red[w * 5 + threadIdx.x];
                 A.tile_sums[(long long)t * 5 + threadIdx.x] = v;
             }
         }
 
         if (!PERSIST) break;
         __syncthreads();
-        if (threadIdx.x == 0) S.tile = (int)atomicAdd(A.counter, 1u);
+        if (threadIdx.x == 0) *tile_bc = (int)atomicAdd(A.counter, 1u);
         __syncthreads();
-        t = S.tile;
+        t = *tile_bc;
     }
 
     if (!__all_sync(0xffffffffu, ok) && tx == 0) atomicOr(A.err, (unsigned)ERRBIT_NONPHYSICAL);
 }
 
 template <class T, int TY>
-constexpr size_t stage_smem_bytes() { return sizeof(StageSmem<T, TY>); }
+constexpr size_t stage_smem_bytes() { return StageLayout<T, TY>::kBytes; }
 
 } // namespace mpcf

@@ -58,6 +58,7 @@ SIGNATURES = {
     "mpcf_step": (_I, [_P, _D, _D, _PD]),
     "mpcf_run": (_I, [_P, _I, _D, _D, _I, _PD]),
     "mpcf_synchronize": (_I, [_P]),
+    "mpcf_update": (_I, [_P, _D]),
     "mpcf_conserved_sums": (_I, [_P, _PD]),
     "mpcf_set_track_conservation": (_I, [_P, _I]),
     "mpcf_error_word": (_I, [_P, _c.POINTER(_c.c_uint), _I]),
@@ -73,6 +74,8 @@ SIGNATURES = {
     "mpcf_time_stages": (_I, [_P, _I, _D, _PD]),
     "mpcf_probe_fp32_peak": (_I, [_I, _PD]),
     "mpcf_time_run": (_I, [_P, _I, _D, _D, _PD]),
+    "mpcf_device_info": (_I, [_I, _c.c_char_p, _I, _c.POINTER(_c.c_longlong), _c.POINTER(_c.c_longlong), _PI]),
+    "mpcf_device_synchronize": (_I, [_I]),
 }
 
 _lib = None

@@ -112,6 +112,10 @@ class Solver:
             arr = (ctypes.c_double * self.ndom)(*dtinvh)
         check(lib().mpcf_stage(self._h, float(a), float(b), arr))
 
+    def update(self, b):
+        """U <- U + b*R alone (the reference's _update)."""
+        check(lib().mpcf_update(self._h, float(b)))
+
     def compute_dt(self, cfl, dt_max=1e30):
         out = (ctypes.c_double * self.ndom)()
         check(lib().mpcf_compute_dt(self._h, float(cfl), float(dt_max), out))

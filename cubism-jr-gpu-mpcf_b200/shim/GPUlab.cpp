@@ -1,0 +1,164 @@
+// GPUlab.cpp -- the B200 lab: GPUlab's interface over a libmpcf_b200 solver.
+#include "GPUlab.h"
+
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <map>
+#include <mutex>
+#include <utility>
+#include <sys/time.h>
+
+#include "../../include/mpcf_b200.h"
+
+namespace
+{
+    double now_s()
+    {
+        struct timeval t;
+        gettimeofday(&t, nullptr);
+        return t.tv_sec + 1e-6 * t.tv_usec;
+    }
+
+    // halo buffer -> (lab, face): lets BoundaryConditions calls made from a
+    // subclass's _apply_bc reach the lab that owns the halo
+    std::mutex g_mu;
+    std::map<const RealPtrVec_t*, std::pair<GPUlab*, int> >& registry()
+    {
+        static std::map<const RealPtrVec_t*, std::pair<GPUlab*, int> > r;
+        return r;
+    }
+
+    int precision_for_real()
+    {
+        if (sizeof(Real) == 8) return MPCF_PREC_FP64;
+        const char* e = getenv("MPCF_PRECISION");
+        if (e && !strcmp(e, "fp32")) return MPCF_PREC_FP32;
+        if (e && !strcmp(e, "mixed")) return MPCF_PREC_MIXED;
+        return MPCF_PREC_FP32_REF;
+    }
+}
+
+namespace mpcf_shim
+{
+    void record_bc(const RealPtrVec_t* halo, int dir, int side, int type)
+    {
+        std::lock_guard<std::mutex> lk(g_mu);
+        auto it = registry().find(halo);
+        if (it == registry().end())
+        {
+            fprintf(stderr, "[BoundaryConditions ERROR: halo buffer does not belong to a GPUlab]\n");
+            exit(1);
+        }
+        const int face = 2 * dir + side;
+        if (it->second.second != face)
+        {
+            fprintf(stderr, "[BoundaryConditions ERROR: boundary <%d,%d> applied to the halo of face %d]\n", dir, side, it->second.second);
+            exit(1);
+        }
+        it->second.first->record_bc_face(face, type);
+    }
+}
+
+GPUlab::GPUlab(GridMPI& G, const uint_t nslices_, const int verbosity)
+    : grid(G), halox(3 * sizeY * sizeZ), haloy(sizeX * 3 * sizeZ), haloz(sizeX * sizeY * 3),
+      nslices(nslices_), m_verbosity(verbosity), m_solver(nullptr), m_bc_dirty(false), m_host_sync(true)
+{
+    // the reference's configuration checks and messages (GPUlab.cpp:37-47)
+    if (nslices_ == 0 || sizeZ % nslices_ != 0)
+    {
+        fprintf(stderr, "[GPUlab ERROR: CURRENTLY nslices MUST BE AN INTEGER MULTIPLE of GridMPI::sizeZ\n");
+        exit(1);
+    }
+    int mycoords[3];
+    grid.peindex(mycoords);
+    for (int i = 0; i < 3; ++i)
+    {
+        myFeature[i * 2 + 0] = mycoords[i] == 0 ? SKIN : FLESH;
+        myFeature[i * 2 + 1] = mycoords[i] == grid.getBlocksPerDimension(i) - 1 ? SKIN : FLESH;
+    }
+    for (int f = 0; f < 6; ++f) m_bc[f] = MPCF_BC_ABSORBING;
+
+    const int dims[3] = {(int)sizeX, (int)sizeY, (int)sizeZ};
+    const int dev = getenv("MPCF_DEVICE") ? atoi(getenv("MPCF_DEVICE")) : 0;
+    GPU::check(mpcf_create(&m_solver, 1, dims, m_bc, precision_for_real(), dev), "GPUlab: mpcf_create");
+    GPU::set_current_solver(m_solver);
+    {
+        std::lock_guard<std::mutex> lk(g_mu);
+        registry()[&halox.left]  = std::make_pair(this, 0);
+        registry()[&halox.right] = std::make_pair(this, 1);
+        registry()[&haloy.left]  = std::make_pair(this, 2);
+        registry()[&haloy.right] = std::make_pair(this, 3);
+        registry()[&haloz.left]  = std::make_pair(this, 4);
+        registry()[&haloz.right] = std::make_pair(this, 5);
+    }
+    upload();
+    if (m_verbosity)
+        printf("[GPUlab: %ux%ux%u block device resident, precision %d]\n", sizeX, sizeY, sizeZ, precision_for_real());
+}
+
+GPUlab::~GPUlab()
+{
+    {
+        std::lock_guard<std::mutex> lk(g_mu);
+        for (const RealPtrVec_t* h : {&halox.left, &halox.right, &haloy.left, &haloy.right, &haloz.left, &haloz.right})
+            registry().erase(h);
+    }
+    if (GPU::current_solver() == m_solver) GPU::set_current_solver(nullptr);
+    mpcf_destroy(m_solver);
+}
+
+void GPUlab::record_bc_face(const int face, const int type)
+{
+    if (m_bc[face] != type) { m_bc[face] = type; m_bc_dirty = true; }
+}
+
+void GPUlab::upload()
+{
+    const void* st[7];
+    const void* rg[7];
+    for (int q = 0; q < 7; ++q) { st[q] = grid.pdata()[q]; rg[q] = grid.ptmp()[q]; }
+    GPU::check(mpcf_set_state(m_solver, 0, st, rg, 0), "GPUlab: upload");
+}
+
+void GPUlab::download()
+{
+    void* st[7];
+    void* rg[7];
+    for (int q = 0; q < 7; ++q) { st[q] = grid.pdata()[q]; rg[q] = grid.ptmp()[q]; }
+    GPU::check(mpcf_get_state(m_solver, 0, st, rg, 0), "GPUlab: download");
+}
+
+void GPUlab::load_ghosts(const double t)
+{
+    // one rank: every face is a physical boundary (SKIN), no halo messages
+    // (GPUlab.cpp:622-644); the subclass states its boundary conditions
+    _apply_bc(t);
+    if (m_bc_dirty)
+    {
+        GPU::check(mpcf_set_bc(m_solver, 0, m_bc), "GPUlab: boundary conditions");
+        m_bc_dirty = false;
+    }
+}
+
+double GPUlab::max_sos(float& sos)
+{
+    const double t0 = now_s();
+    // the reference reads the host state for the reduction (GPUlab.cpp:671);
+    // with host synchronisation the host register is current too, so both go up
+    if (m_host_sync) upload();
+    double s = 0;
+    GPU::check(mpcf_max_sos(m_solver, &s), "GPUlab: max_sos");
+    sos = (float)s;
+    return now_s() - t0;
+}
+
+double GPUlab::process_all(const Real a, const Real b, const Real dtinvh)
+{
+    const double t0 = now_s();
+    if (m_host_sync) upload();
+    const double dt = (double)dtinvh;
+    GPU::check(mpcf_stage(m_solver, (double)a, (double)b, &dt), "GPUlab: process_all");
+    if (m_host_sync) download();
+    return now_s() - t0;
+}

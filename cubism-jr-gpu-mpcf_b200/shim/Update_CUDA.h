@@ -1,0 +1,21 @@
+// Update_CUDA.h -- update facade (source/Update_CUDA.h:13-27).
+#pragma once
+
+#include "Types.h"
+
+class Update_CUDA
+{
+protected:
+    Real m_b;
+
+    inline bool _is_aligned(const void* const ptr, unsigned int alignment) const
+    {
+        return ((size_t)ptr) % alignment == 0;
+    }
+
+public:
+    Update_CUDA(const Real b = 1) : m_b(b) {}
+
+    // U <- U + b*register for the whole block
+    void compute(const int nslices);
+};

@@ -121,6 +121,11 @@ int mpcf_compute_dt(mpcf_solver* s, double cfl, double dt_max, double* dt_out);
 int mpcf_step(mpcf_solver* s, double cfl, double dt_max, double* dt_out);
 int mpcf_run(mpcf_solver* s, int nsteps, double cfl, double dt_max, int use_graph, double* time_out);
 int mpcf_synchronize(mpcf_solver* s);
+/* The state update alone, U <- U + b*R (Update_CUDA::compute ->
+ * GPU::update -> _update, Update_CUDA.cpp:12-17, GPUkernels.cu:1142-1179),
+ * for callers that split a stage into Convection_CUDA (mpcf_stage with
+ * b = 0) and Update_CUDA; the pair is bit-identical to one mpcf_stage. */
+int mpcf_update(mpcf_solver* s, double b);
 
 /* FP64 sums of (rho, rho u, rho v, rho w, E) over each domain's current
  * state, out[5*d..5*d+4]; deterministic order. */
@@ -176,6 +181,13 @@ int mpcf_time_stages(mpcf_solver* s, int reps, double dtinvh, double* ms_per_sta
 /* Replay nsteps captured step graphs back to back and return their device
  * time (CUDA events on the solver's stream), ms. */
 int mpcf_time_run(mpcf_solver* s, int nsteps, double cfl, double dt_max, double* ms);
+
+/* Device facts for host code that does not link the CUDA runtime itself
+ * (GPU::tell_GPU / tell_memUsage_GPU of the reference, GPUhousehold.cu:390-418):
+ * name (optional), total and free memory, SM count. */
+int mpcf_device_info(int device, char* name, int name_len, long long* total_bytes, long long* free_bytes, int* sms);
+/* Wait for all work on a device (GPU::syncGPU, GPUhousehold.cu:367-372). */
+int mpcf_device_synchronize(int device);
 
 /* Measured FP32 CUDA-core throughput of the device (FMA chains), TFLOP/s:
  * the denominator of the stage kernel's compute roofline. */

@@ -109,3 +109,16 @@ def test_configs_build(mpcf):
     assert len(c4["dims"]) == 64
     assert all(e in (32, 48, 64, 96, 128) for d in c4["dims"] for e in d)
     assert all(1 <= len(b) <= 8 for b in c4["bubbles"])
+
+
+def test_dropin_driver_library_loads():
+    """The reference integrator + shim driver (oracle/_ref, built where the
+    reference tree is present) resolves all its symbols against
+    libmpcf_b200 without a GPU."""
+    p = os.path.join(REPO, "oracle", "_ref", "libref_lsrk3_driver.so")
+    if not os.path.exists(p):
+        pytest.skip("oracle/_ref not built")
+    L = ctypes.CDLL(p)
+    d = (ctypes.c_int * 3)()
+    L.drv_dims(d)
+    assert (d[0], d[1], d[2]) == (32, 24, 16)
