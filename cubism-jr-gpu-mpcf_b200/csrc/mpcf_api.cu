@@ -39,6 +39,22 @@ int fail(int code, const char* fmt, ...)
     return code;
 }
 
+} // namespace
+
+// error recording for entry points defined in other translation units
+int mpcf_fail_external(int code, const char* fmt, ...)
+{
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof(buf), fmt, ap);
+    va_end(ap);
+    g_err = buf;
+    return code;
+}
+
+namespace {
+
 #define CK(call) do { cudaError_t e_ = (call); if (e_ != cudaSuccess) \
     return fail(MPCF_ERR_CUDA, "%s failed: %s (%s:%d)", #call, cudaGetErrorString(e_), __FILE__, __LINE__); } while (0)
 

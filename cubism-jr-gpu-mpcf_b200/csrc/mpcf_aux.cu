@@ -3,6 +3,7 @@
 // bubble-cloud initial condition and an explicit ghost-buffer fill.
 #include <cuda_runtime.h>
 #include <math.h>
+#include <mutex>
 #include "mpcf_math.cuh"
 #include "mpcf_stage.cuh"
 #include "mpcf_launch.h"
@@ -364,4 +365,129 @@ cudaError_t launch_update(int is_double, const DomDev* doms, int ndom, int parit
     return cudaGetLastError();
 }
 
+// ===========================================================================
+// Conservation sums without allocating (mpcf_conserved_sums_noalloc).
+//
+// For callers that may not allocate device memory themselves or through a
+// library: hosts that give a plug-in a fixed device-memory budget at start-up
+// and forbid cudaMalloc afterwards, and tight loops where cudaMalloc/cudaFree
+// (which can synchronise the whole device) are not acceptable.  The caller
+// passes its own device field pointers and an output; the per-chunk partials
+// live in a fixed array of this library instead of solver-owned memory.
+// ===========================================================================
+namespace {
+
+// cells per chunk and chunk limit: inputs up to 8192 * 32768 = 2^28 cells
+constexpr int kNoAllocChunk = 32768;
+constexpr int kNoAllocMaxChunks = 8192;
+
+// per-chunk partials [chunk][5], then 5 totals; every device that loads the
+// library keeps this ~320 KB array until the process exits
+static __device__ __align__(256) double g_noalloc_scratch[kNoAllocMaxChunks * 5 + 8];
+
+// device address of g_noalloc_scratch per device, looked up on the first call
+// made with that device current (the name is only a host-side handle)
+constexpr int kMaxDevices = 64;
+void* g_noalloc_addr[kMaxDevices] = {nullptr};
+std::mutex g_noalloc_mu;
+
+template <class T>
+__global__ void __launch_bounds__(256) sum_fields_kernel(const T* __restrict__ f0, const T* __restrict__ f1,
+        const T* __restrict__ f2, const T* __restrict__ f3, const T* __restrict__ f4,
+        long long n, int chunk, double* partial)
+{
+    // same chunking, accumulation and reduction tree as sum_state_kernel, so
+    // the result is bit-identical to the solver's mpcf_conserved_sums
+    __shared__ double red[5][256];
+    const long long beg = (long long)blockIdx.x * chunk;
+    const long long end = min(beg + (long long)chunk, n);
+    const T* f[5] = {f0, f1, f2, f3, f4};
+    double acc[5] = {0, 0, 0, 0, 0};
+    for (long long i = beg + threadIdx.x; i < end; i += 256)
+        for (int m = 0; m < 5; ++m) acc[m] += (double)f[m][i];
+    for (int m = 0; m < 5; ++m) red[m][threadIdx.x] = acc[m];
+    __syncthreads();
+    for (int w = 128; w > 0; w >>= 1)
+    {
+        if ((int)threadIdx.x < w)
+            for (int m = 0; m < 5; ++m) red[m][threadIdx.x] += red[m][threadIdx.x + w];
+        __syncthreads();
+    }
+    if (threadIdx.x < 5) partial[(long long)blockIdx.x * 5 + threadIdx.x] = red[threadIdx.x][0];
+}
+
+__global__ void sum_partials_kernel(const double* partial, int nchunks, double* out)
+{
+    const int m = threadIdx.x;
+    if (m >= 5) return;
+    double s = 0;
+    for (int c = 0; c < nchunks; ++c) s += partial[(long long)c * 5 + m];
+    out[m] = s;
+}
+
+} // namespace
+
 } // namespace mpcf
+
+#include "../../include/mpcf_b200.h"
+
+extern "C" int mpcf_conserved_sums_noalloc(const void* const* state7, long long ncells, int elem_size,
+                                           double* out5, int out_is_device, int device, void* stream)
+{
+    using namespace mpcf;
+    if (!state7 || !out5) return mpcf_fail_external(MPCF_ERR_ARG, "null state or output pointer");
+    if (elem_size != 4 && elem_size != 8) return mpcf_fail_external(MPCF_ERR_ARG, "elem_size must be 4 or 8");
+    if (ncells < 1) return mpcf_fail_external(MPCF_ERR_ARG, "ncells must be positive");
+    if (ncells > (long long)kNoAllocMaxChunks * kNoAllocChunk)
+        return mpcf_fail_external(MPCF_ERR_ARG, "ncells = %lld exceeds the no-allocation limit of %lld cells "
+                                  "(%d chunks of %d); use mpcf_conserved_sums", ncells,
+                                  (long long)kNoAllocMaxChunks * kNoAllocChunk, kNoAllocMaxChunks, kNoAllocChunk);
+    if (device < 0 || device >= kMaxDevices) return mpcf_fail_external(MPCF_ERR_ARG, "device %d out of range", device);
+    for (int q = 0; q < 5; ++q)
+        if (!state7[q]) return mpcf_fail_external(MPCF_ERR_ARG, "field %d pointer is null", q);
+
+    int prev = -1;
+    if (cudaGetDevice(&prev) != cudaSuccess) { cudaGetLastError(); prev = -1; }
+    if (prev != device && cudaSetDevice(device) != cudaSuccess)
+    { cudaGetLastError(); return mpcf_fail_external(MPCF_ERR_CUDA, "cannot make device %d current", device); }
+    struct Restore { int p; int d; ~Restore() { if (p >= 0 && p != d) cudaSetDevice(p); } } restore{prev, device};
+
+    // one-time set-up on this device: the device address of the scratch array
+    double* scratch = nullptr;
+    {
+        std::lock_guard<std::mutex> lk(g_noalloc_mu);
+        if (!g_noalloc_addr[device])
+        {
+            void* addr = nullptr;
+            cudaError_t e = cudaGetSymbolAddress(&addr, g_noalloc_scratch);
+            if (e != cudaSuccess || !addr)
+            {
+                cudaGetLastError();
+                return mpcf_fail_external(MPCF_ERR_CUDA, "cudaGetSymbolAddress(no-allocation scratch) failed on device %d: %s",
+                                          device, cudaGetErrorString(e));
+            }
+            g_noalloc_addr[device] = addr;
+        }
+        scratch = (double*)g_noalloc_addr[device];
+    }
+    cudaStream_t st = (cudaStream_t)stream;
+    const int nchunks = (int)((ncells + kNoAllocChunk - 1) / kNoAllocChunk);
+    double* totals = scratch + (size_t)kNoAllocMaxChunks * 5;
+    // every partial slot the second kernel reads is written by the first, so
+    // nothing left by an earlier call is read
+    if (elem_size == 8)
+        sum_fields_kernel<double><<<nchunks, 256, 0, st>>>((const double*)state7[0], (const double*)state7[1],
+            (const double*)state7[2], (const double*)state7[3], (const double*)state7[4], ncells, kNoAllocChunk, scratch);
+    else
+        sum_fields_kernel<float><<<nchunks, 256, 0, st>>>((const float*)state7[0], (const float*)state7[1],
+            (const float*)state7[2], (const float*)state7[3], (const float*)state7[4], ncells, kNoAllocChunk, scratch);
+    sum_partials_kernel<<<1, 32, 0, st>>>(scratch, nchunks, out_is_device ? out5 : totals);
+    cudaError_t e = cudaGetLastError();
+    if (e == cudaSuccess && !out_is_device)
+    {
+        e = cudaMemcpyAsync(out5, totals, 5 * sizeof(double), cudaMemcpyDeviceToHost, st);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    }
+    if (e != cudaSuccess) return mpcf_fail_external(MPCF_ERR_CUDA, "no-allocation sums: %s", cudaGetErrorString(e));
+    return MPCF_OK;
+}

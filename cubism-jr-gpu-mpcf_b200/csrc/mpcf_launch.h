@@ -5,6 +5,10 @@
 #include <cuda_runtime.h>
 #include "mpcf_types.h"
 
+// records the calling thread's last error message (mpcf_last_error) and
+// returns `code`; defined in mpcf_api.cu
+int mpcf_fail_external(int code, const char* fmt, ...);
+
 namespace mpcf {
 
 struct StageKernelInfo

@@ -60,6 +60,7 @@ SIGNATURES = {
     "mpcf_synchronize": (_I, [_P]),
     "mpcf_update": (_I, [_P, _D]),
     "mpcf_conserved_sums": (_I, [_P, _PD]),
+    "mpcf_conserved_sums_noalloc": (_I, [_PP, _c.c_longlong, _I, _PD, _I, _I, _P]),
     "mpcf_set_track_conservation": (_I, [_P, _I]),
     "mpcf_error_word": (_I, [_P, _c.POINTER(_c.c_uint), _I]),
     "mpcf_set_bc": (_I, [_P, _I, _PI]),

@@ -135,6 +135,29 @@ int mpcf_conserved_sums(mpcf_solver* s, double* out);
  * returns them without another reduction. */
 int mpcf_set_track_conservation(mpcf_solver* s, int on);
 
+/* The same FP64 sums without allocating anything.  This entry point has no
+ * counterpart in the reference.  It is for callers that may not allocate
+ * device memory, directly or through a library: hosts that give a plug-in a
+ * fixed device-memory budget at start-up and forbid cudaMalloc afterwards,
+ * and tight loops that cannot afford cudaMalloc/cudaFree, which may
+ * synchronise the whole device.  The caller passes device pointers to the 7
+ * fields of a state of `ncells` cells (elem_size 4 or 8; only the first five
+ * fields are read) and receives rho, rho u, rho v, rho w, E totals in out5,
+ * host memory or, with out_is_device, device memory.  Work goes on `stream`
+ * (a cudaStream_t, NULL for the default stream); a host output is ready when
+ * the call returns.  The result is bit-identical to mpcf_conserved_sums on
+ * the same state.
+ * Limit: ncells <= 268435456 (8192 chunks of 32768 cells); larger inputs are
+ * rejected with MPCF_ERR_ARG.  The partial sums live in a fixed 320 KB
+ * device array of this library, which every GPU that loads it keeps until
+ * the process exits.  The first call on a device looks up that array's
+ * device address, with the device current; make that first call before any
+ * stream capture.  All calls share the array: calls that overlap on a GPU
+ * (concurrent streams or threads) race and must be serialised by the
+ * caller.  Every partial a call reads is written by that same call. */
+int mpcf_conserved_sums_noalloc(const void* const* state7, long long ncells, int elem_size,
+                                double* out5, int out_is_device, int device, void* stream);
+
 /* device error word (MPCF_ERRBIT_*); clear != 0 resets it */
 int mpcf_error_word(mpcf_solver* s, unsigned* word, int clear);
 
