@@ -223,6 +223,8 @@ def main():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-fp64", action="store_true")
     ap.add_argument("--only-mixed-fp64", action="store_true", help="skip the fp32_ref / fp32 throughput runs")
+    ap.add_argument("--precision", default="mixed", choices=["mixed", "fp32", "fp32_ref", "fp64"],
+                    help="precision of the headline run (profiling of the other forms)")
     ap.add_argument("--workload", default=WORKLOAD)
     args = ap.parse_args()
     if args.impl == "reference":
@@ -251,7 +253,7 @@ def main():
         return float(np.max(np.abs(a - b)) / np.max(np.abs(b)))
 
     # ---------------- mixed (headline): W warm-up + K timed graph replays
-    s = make_solver(mpcf, cfg, "mixed")
+    s = make_solver(mpcf, cfg, args.precision)
     s.set_tiling(*pick_tiling(mpcf, s))
     s.track_conservation(True)
     sums0 = s.conserved_sums()
