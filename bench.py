@@ -125,6 +125,12 @@ def make_solver(mpcf, cfg, precision):
     return s
 
 
+def all_state(s):
+    """First 7 fields of every domain, concatenated (precision comparisons)."""
+    parts = [s.get_state(dom=d, with_reg=False) for d in range(s.ndom)]
+    return [np.concatenate([p[q] for p in parts]) for q in range(7)]
+
+
 def derived_fields(st, dtype=np.float64):
     rho = st[0].astype(dtype)
     ke = 0.5 * (st[1].astype(dtype) ** 2 + st[2].astype(dtype) ** 2 + st[3].astype(dtype) ** 2) / rho
@@ -148,9 +154,8 @@ def time_steps(mpcf, s, steps, warmup, cfl, dist=None):
     ms = run_timed(mpcf, s, steps, cfl)
     torch.cuda.synchronize()
     if dist is not None:
-        t = torch.tensor([ms], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
+        import mpcf.replicas as rp
+        ms = rp.max_over_ranks(dist, ms, device="cuda")
         dist.barrier()
     return ms
 
@@ -168,13 +173,17 @@ def stage_kernel_ms(mpcf, s, reps=6):
     return s.time_stages(reps, dtinvh=0.0)
 
 
-def cpu_sample(cfg_params, bub, dims, threads):
-    """Oracle (C restatement, OpenMP) on a sub-block of the workload: cell-stage updates/s."""
+def cpu_sample(cfg_params, bub, dims, threads, U0=None):
+    """Oracle (C restatement, OpenMP) on a sub-block of the workload: one
+    LSRK3 step, timed; returns (cell-stage updates/s, seconds).  U0 (the
+    sub-block's initial state) is generated when not given."""
     import mpcf
     sys.path.insert(0, os.path.join(REPO, "tests"))
     import oracle_lib as O
     os.environ["OMP_NUM_THREADS"] = str(threads)
-    U = mpcf.ic_cloud_host(dims, cfg_params, bub, np.float32)
+    if U0 is None:
+        U0 = mpcf.ic_cloud_host(dims, cfg_params, bub, np.float32)
+    U = [a.copy() for a in U0]
     R = [np.zeros_like(a) for a in U]
     t0 = time.perf_counter()
     O.step(dims, (0,) * 6, U, R, cfl=0.3)
@@ -194,9 +203,10 @@ def reference_arm(args):
     # bounded sample: a 512 x 512 x 16 slab of the 512^3 cloud (same cell
     # spacing, bubbles and material data), one full LSRK3 step per timed step
     sub = (512, 512, 16)
+    U0 = mpcf.ic_cloud_host(sub, cfg["params"], cfg["bubbles"][0], np.float32)
     vals = []
     for i in range(args.warmup + args.steps):
-        v, dt = cpu_sample(cfg["params"], cfg["bubbles"][0], sub, cores)
+        v, dt = cpu_sample(cfg["params"], cfg["bubbles"][0], sub, cores, U0)
         if i >= args.warmup:
             vals.append(v)
     value = statistics.median(vals)
@@ -266,7 +276,7 @@ def main():
     sums1 = s.conserved_sums()
     derived = {}
     if rank == 0:
-        derived["mixed"] = derived_fields(s.get_state(with_reg=False))
+        derived[args.precision] = derived_fields(all_state(s))
     # roofline of the dominant kernel (the stage) on this same solver
     st_ms = stage_kernel_ms(mpcf, s)
     nt, grid, threads = s.launch_shape()
@@ -280,7 +290,8 @@ def main():
     others = {}
     precs = [] if args.no_fp64 else ["fp64"]
     if not args.no_fp64 and not args.only_mixed_fp64:
-        precs += ["fp32_ref", "fp32"]
+        precs += ["fp32_ref", "fp32", "mixed"]
+    precs = [p for p in precs if p != args.precision]
     for prec in precs:
         so = make_solver(mpcf, cfg, prec)
         so.set_tiling(*pick_tiling(mpcf, so))
@@ -288,14 +299,14 @@ def main():
         others[prec] = {"value": world * ncell * 3.0 * K / (mso * 1e-3), "ms_per_step": mso / K,
                         "tiling": so.tiling()}
         if rank == 0:
-            derived[prec] = derived_fields(so.get_state(with_reg=False))
+            derived[prec] = derived_fields(all_state(so))
         so.close()
     err = None
     if rank == 0 and "fp64" in derived:
         r64, p64, G64 = derived["fp64"]
         err = {}
         for prec in ("mixed", "fp32_ref", "fp32"):
-            if prec not in derived:
+            if prec not in derived or prec == "fp64":
                 continue
             r, p, G = derived[prec]
             err[prec] = {"L1_rho": l1(r, r64), "Linf_rho": linf(r, r64), "L1_p": l1(p, p64),
@@ -307,7 +318,7 @@ def main():
     # ---------------- e2e through the C ABI with host buffers
     e2e = None
     if not args.no_e2e:
-        e2e = e2e_measure(mpcf, cfg, K=max(2, min(K, 4)), W=1, cfl=cfl, dist=dist)
+        e2e = e2e_measure(mpcf, cfg, K=max(2, min(K, 4)), W=1, cfl=cfl, dist=dist, precision=args.precision)
 
     # ---------------- CPU baseline (rank 0, N=1 only)
     cpu = None
@@ -331,17 +342,18 @@ def main():
             "config": {"workload": cfg["name"] + ": " + cfg["desc"] + ", absorbing, CFL 0.3, mixed form",
                        "cells_per_gpu": ncell, "l2": "inputs 11 GB > 126 MB L2 (no flush needed)",
                        "parallelism": "replicas" if world > 1 else "single GPU",
-                       "tiling": {"ty": tiling[0], "dz": tiling[1], "persistent": tiling[2]},
+                       "tiling": {"ty": tiling[0], "dz": tiling[1], "persistent": tiling[2], "tma": tiling[3]},
                        "graph": True},
             "fp64_value": fp64, "mixed_over_fp64": (value / fp64) if fp64 else None,
             "other_precisions": others,
             "precision_error": err,
-            "conservation_drift": {"mass": float((sums1[0][0] - sums0[0][0]) / sums0[0][0]),
-                                   "energy": float((sums1[0][4] - sums0[0][4]) / sums0[0][4]),
+            "conservation_drift": {"mass": float((sums1[:, 0].sum() - sums0[:, 0].sum()) / sums0[:, 0].sum()),
+                                   "energy": float((sums1[:, 4].sum() - sums0[:, 4].sum()) / sums0[:, 4].sum()),
                                    "note": "FP64 sums over W+K steps, absorbing boundaries (boundary fluxes included)"},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
                          "frac": achieved / hbm, "traffic": None,
-                         "kernel": "stage_kernel<PolMixed>", "ms_per_launch": st_ms,
+                         "kernel": "stage_kernel<Pol%s>" % {"mixed": "Mixed", "fp32": "Fast32", "fp32_ref": "Ref32", "fp64": "FP64"}[args.precision],
+                         "ms_per_launch": st_ms,
                          "algorithmic_bytes_per_launch": bytes_launch, "peak_kind": peak_kind,
                          "note": "the stage kernel is bound by the FP32 pipe, not HBM: see roofline_fp32"},
             "roofline_fp32": {"bound": "fp32", "achieved": ach_tf, "peak": fp32_peak.value, "unit": "TFLOP/s",
@@ -364,33 +376,42 @@ def pick_tiling(mpcf, s):
     library's autotuner on the solver's own state (state left unchanged)."""
     env = os.environ.get("MPCF_TILING")
     if env:
-        ty, dz, p = (int(v) for v in env.split(","))
-        return ty, dz, bool(p)
+        v = [int(x) for x in env.split(",")]
+        return v[0], v[1], bool(v[2]), bool(v[3]) if len(v) > 3 else True
     best, _ = s.autotune(reps=2)
     return best
 
 
-def e2e_measure(mpcf, cfg, K, W, cfl, dist):
+def e2e_measure(mpcf, cfg, K, W, cfl, dist, precision="mixed"):
     """Same metric through the C ABI with pinned host buffers: every step
-    uploads state + register, advances one LSRK3 step, downloads both."""
+    uploads state + register of every domain, advances one LSRK3 step,
+    downloads both."""
     import torch
-    dims = cfg["dims"][0]
-    n = dims[0] * dims[1] * dims[2]
-    s = make_solver(mpcf, cfg, "mixed")
-    hst = [torch.empty(n, dtype=torch.float32, pin_memory=True) for _ in range(14)]
-    st = s.get_state()
-    for q in range(7):
-        hst[q].numpy()[:] = st[0][q]
-        hst[7 + q].numpy()[:] = st[1][q]
-    del st
+    s = make_solver(mpcf, cfg, precision)
     L = mpcf.lib()
-    up = (ctypes.c_void_p * 7)(*[hst[q].data_ptr() for q in range(7)])
-    ur = (ctypes.c_void_p * 7)(*[hst[7 + q].data_ptr() for q in range(7)])
+    dtype = torch.float64 if precision == "fp64" else torch.float32
+    esz = 8 if precision == "fp64" else 4
+    bufs = []
+    ncell = 0
+    for d, dims in enumerate(cfg["dims"]):
+        n = dims[0] * dims[1] * dims[2]
+        ncell += n
+        h = [torch.empty(n, dtype=dtype, pin_memory=True) for _ in range(14)]
+        st = s.get_state(dom=d)
+        for q in range(7):
+            h[q].numpy()[:] = st[0][q]
+            h[7 + q].numpy()[:] = st[1][q]
+        del st
+        up = (ctypes.c_void_p * 7)(*[h[q].data_ptr() for q in range(7)])
+        ur = (ctypes.c_void_p * 7)(*[h[7 + q].data_ptr() for q in range(7)])
+        bufs.append((h, up, ur))
 
     def one():
-        mpcf._lib.check(L.mpcf_set_state(s._h, 0, up, ur, 0))
+        for d, (_, up, ur) in enumerate(bufs):
+            mpcf._lib.check(L.mpcf_set_state(s._h, d, up, ur, 0))
         mpcf._lib.check(L.mpcf_step(s._h, cfl, 1e30, None))
-        mpcf._lib.check(L.mpcf_get_state(s._h, 0, up, ur, 0))
+        for d, (_, up, ur) in enumerate(bufs):
+            mpcf._lib.check(L.mpcf_get_state(s._h, d, up, ur, 0))
 
     for _ in range(W):
         one()
@@ -402,15 +423,12 @@ def e2e_measure(mpcf, cfg, K, W, cfl, dist):
         one()
     torch.cuda.synchronize()
     sec = time.perf_counter() - t0
-    if dist is not None:
-        t = torch.tensor([sec], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        sec = float(t.item())
-    world = dist.get_world_size() if dist is not None else 1
+    import mpcf.replicas as rp
+    value, _ = rp.throughput(dist, ncell, 3.0 * K, sec * 1e3, device="cuda" if dist is not None else None)
     s.close()
-    return {"value": world * n * 3.0 * K / sec, "unit": UNIT, "h2d_bytes_per_step": 14 * 4 * n,
-            "d2h_bytes_per_step": 14 * 4 * n,
-            "path": "mpcf_set_state (pinned host) + mpcf_step + mpcf_get_state, host wall clock"}
+    return {"value": value, "unit": UNIT, "h2d_bytes_per_step": 14 * esz * ncell,
+            "d2h_bytes_per_step": 14 * esz * ncell,
+            "path": "mpcf_set_state (pinned host) + mpcf_step + mpcf_get_state per step, host wall clock"}
 
 
 if __name__ == "__main__":

@@ -7,6 +7,8 @@
 // (GPUlab.cpp:202-372,703-793) and its host-side halo fills
 // (BoundaryConditions.h:60-109) are replaced by the fused stage kernel.
 #include <cuda_runtime.h>
+#include <cuda.h>
+#include <cudaTypedefs.h>
 #include <algorithm>
 #include <cstdarg>
 #include <cstdio>
@@ -97,8 +99,10 @@ struct mpcf_solver
     int bubbles_cap = 0;
     void* host_stage = nullptr;     // pinned host scratch (ndom doubles/elems)
 
+    void* tmaps = nullptr;          // ndom * 4 CUtensorMap (128 B each)
+
     // launch configuration
-    int ty = 4, dz = 64, persist = 0;
+    int ty = 4, dz = 64, persist = 0, tma = 0;
     int ntiles = 0;
     int sos_chunk = 32768, nchunks = 0;
     bool track_cons = false;
@@ -114,13 +118,91 @@ namespace {
 
 bool valid_ty(const mpcf_solver* s, int ty)
 {
-    if (ty == 2 || ty == 4 || ty == 8) return true;
+    if (ty == 4 || ty == 8) return true;
     return ty == 16 && s->pol == 0;
 }
 
-StageKernelInfo stage_info(const mpcf_solver* s, int ty, bool persist, bool sums = false)
+StageKernelInfo stage_info(const mpcf_solver* s, int ty, bool persist, bool sums, bool tma)
 {
-    return s->pol == 0 ? stage_info_ref(ty, persist, sums) : stage_info_fast(s->pol, ty, persist, sums);
+    switch (s->pol)
+    {
+        case 0: return stage_info_ref(ty, persist, sums, tma);
+        case 1: return stage_info_fast32(ty, persist, sums, tma);
+        case 2: return stage_info_mixed(ty, persist, sums, tma);
+        default: return stage_info_fp64(ty, persist, sums, tma);
+    }
+}
+
+cudaError_t launch_stage(const mpcf_solver* s, const StageArgs& A, int grid, cudaStream_t st)
+{
+    switch (s->pol)
+    {
+        case 0: return launch_stage_ref(s->ty, s->persist != 0, s->tma != 0, A, grid, st);
+        case 1: return launch_stage_fast32(s->ty, s->persist != 0, s->tma != 0, A, grid, st);
+        case 2: return launch_stage_mixed(s->ty, s->persist != 0, s->tma != 0, A, grid, st);
+        default: return launch_stage_fp64(s->ty, s->persist != 0, s->tma != 0, A, grid, st);
+    }
+}
+
+// cuTensorMapEncodeTiled through the runtime's driver entry point (no link
+// against the driver library needed)
+PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder()
+{
+    static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+    static bool tried = false;
+    if (!tried)
+    {
+        tried = true;
+        void* p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = (PFN_cuTensorMapEncodeTiled_v12000)p;
+        else
+            cudaGetLastError();
+    }
+    return fn;
+}
+
+// Tensor maps of every domain for the current tile height: per state buffer a
+// 40 x (ty+6) x 1 x 7 halo box and a 32 x ty x 1 x 7 interior box over the
+// 4-D view (x, y, z, field) of the buffer.  A domain qualifies when its row
+// and plane pitches are multiples of 16 bytes (nx*elem % 16 == 0).
+bool any_tma_ok(const mpcf_solver* s)
+{
+    for (const auto& D : s->hdoms) if (D.tma_ok) return true;
+    return false;
+}
+
+int encode_tensor_maps(mpcf_solver* s)
+{
+    std::vector<CUtensorMap> h((size_t)s->ndom * 4);
+    memset(h.data(), 0, h.size() * sizeof(CUtensorMap));
+    PFN_cuTensorMapEncodeTiled_v12000 enc = tensor_map_encoder();
+    for (int d = 0; d < s->ndom; ++d)
+    {
+        DomDev& D = s->hdoms[d];
+        const size_t e = s->esz;
+        bool ok = enc != nullptr && ((size_t)D.nx * e) % 16 == 0 && ((size_t)D.nx * D.ny * e) % 16 == 0 &&
+                  ((size_t)D.fs * e) % 16 == 0;
+        for (int b = 0; b < 2 && ok; ++b)
+            for (int box = 0; box < 2 && ok; ++box)
+            {
+                const cuuint64_t dims[4] = {(cuuint64_t)D.nx, (cuuint64_t)D.ny, (cuuint64_t)D.nz, 7};
+                const cuuint64_t strides[3] = {(cuuint64_t)D.nx * e, (cuuint64_t)D.nx * D.ny * e, (cuuint64_t)D.fs * e};
+                const cuuint32_t boxd[4] = {box == 0 ? 40u : 32u, (cuuint32_t)(box == 0 ? s->ty + 6 : s->ty), 1u, 7u};
+                const cuuint32_t estr[4] = {1, 1, 1, 1};
+                CUresult r = enc(&h[(size_t)d * 4 + b * 2 + box],
+                                 e == 8 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32,
+                                 4, D.U[b], dims, strides, boxd, estr,
+                                 CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                                 CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+                ok = (r == CUDA_SUCCESS);
+            }
+        D.tma_ok = ok ? 1 : 0;
+    }
+    CK(cudaMemcpyAsync(s->tmaps, h.data(), h.size() * sizeof(CUtensorMap), cudaMemcpyHostToDevice, s->stream));
+    return MPCF_OK;
 }
 
 void destroy_graphs(mpcf_solver* s)
@@ -170,6 +252,8 @@ int apply_tiling(mpcf_solver* s)
     if (rc) return rc;
     if (!s->chunk_sums)
         if ((rc = dev_alloc(s, (void**)&s->chunk_sums, sizeof(double) * 5 * (size_t)std::max(c, 1)))) return rc;
+    if ((rc = encode_tensor_maps(s))) return rc;
+    if (s->tma && !any_tma_ok(s)) s->tma = 0;
     CK(cudaMemcpyAsync(s->ddoms, s->hdoms.data(), sizeof(DomDev) * s->ndom, cudaMemcpyHostToDevice, s->stream));
     CK(cudaStreamSynchronize(s->stream));
     destroy_graphs(s);
@@ -178,7 +262,7 @@ int apply_tiling(mpcf_solver* s)
 
 int persistent_grid(mpcf_solver* s, int ty)
 {
-    StageKernelInfo I = stage_info(s, ty, true);
+    StageKernelInfo I = stage_info(s, ty, true, false, s->tma != 0);
     int nb = 0;
     if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, I.fn, 32 * ty, I.smem) != cudaSuccess || nb < 1)
     {
@@ -202,6 +286,7 @@ StageArgs stage_args(mpcf_solver* s, double a, double b, bool sums)
     A.counter = s->counter;
     A.err = s->err;
     A.tile_sums = sums ? s->tile_sums : nullptr;
+    A.tmaps = s->tmaps;
     return A;
 }
 
@@ -215,8 +300,7 @@ int enqueue_stage(mpcf_solver* s, double a, double b, bool sums)
         grid = persistent_grid(s, s->ty);
         CK(cudaMemsetAsync(s->counter, 0, sizeof(unsigned), s->stream));
     }
-    cudaError_t e = s->pol == 0 ? launch_stage_ref(s->ty, s->persist != 0, A, grid, s->stream)
-                                : launch_stage_fast(s->pol, s->ty, s->persist != 0, A, grid, s->stream);
+    cudaError_t e = launch_stage(s, A, grid, s->stream);
     if (e != cudaSuccess) return fail(MPCF_ERR_CUDA, "stage launch failed: %s", cudaGetErrorString(e));
     s->parity ^= 1;
     if (sums)
@@ -370,6 +454,7 @@ int mpcf_create(mpcf_solver** out, int ndomains, const int* dims, const int* bc,
     if ((rc = dev_alloc(s, (void**)&s->sums, 8 * 5 * ndomains))) return bail(rc);
     if ((rc = dev_alloc(s, (void**)&s->err, 16))) return bail(rc);
     if ((rc = dev_alloc(s, (void**)&s->counter, 16))) return bail(rc);
+    if ((rc = dev_alloc(s, &s->tmaps, (size_t)128 * 4 * ndomains))) return bail(rc);
     cudaMemsetAsync(s->sos_bits, 0, 8 * ndomains, s->stream);
     cudaMemsetAsync(s->dtinvh, 0, 8 * ndomains, s->stream);
     cudaMemsetAsync(s->dt, 0, 8 * ndomains, s->stream);
@@ -381,21 +466,22 @@ int mpcf_create(mpcf_solver** out, int ndomains, const int* dims, const int* bc,
     { cudaGetLastError(); return bail(fail(MPCF_ERR_NOMEM, "cudaMallocHost failed")); }
 
     // allow the large shared-memory footprints of every tiling variant
-    const int tys[4] = {2, 4, 8, 16};
-    for (int i = 0; i < 4; ++i)
+    const int tys[3] = {4, 8, 16};
+    for (int i = 0; i < 3; ++i)
     {
         if (!valid_ty(s, tys[i])) continue;
-        for (int p = 0; p < 4; ++p)
+        for (int p = 0; p < 8; ++p)
         {
-            StageKernelInfo I = stage_info(s, tys[i], (p & 1) != 0, (p & 2) != 0);
+            StageKernelInfo I = stage_info(s, tys[i], (p & 1) != 0, (p & 2) != 0, (p & 4) != 0);
             if (!I.fn) continue;
             if (cudaFuncSetAttribute(I.fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)I.smem) != cudaSuccess)
             { cudaGetLastError(); return bail(fail(MPCF_ERR_CUDA, "cannot grant %zu B shared memory to the stage kernel (ty=%d)", I.smem, tys[i])); }
         }
     }
-    s->ty = 4;
+    s->ty = 8;
     s->dz = 64;
     s->persist = 0;
+    s->tma = 1;                       // dropped by apply_tiling when no domain qualifies
     if ((rc = apply_tiling(s))) return bail(rc);
     *out = s;
     return MPCF_OK;
@@ -737,24 +823,26 @@ int mpcf_bubbles(unsigned long long seed, int n, double rmin, double rmax,
     return placed;
 }
 
-int mpcf_set_tiling(mpcf_solver* s, int ty, int dz, int persistent)
+int mpcf_set_tiling(mpcf_solver* s, int ty, int dz, int flags)
 {
     if (!s) return fail(MPCF_ERR_ARG, "null solver");
     if (!valid_ty(s, ty)) return fail(MPCF_ERR_ARG, "unsupported tile height ty=%d for this precision", ty);
     if (dz < 1) return fail(MPCF_ERR_ARG, "dz must be >= 1");
+    if (flags & ~(MPCF_TILE_PERSISTENT | MPCF_TILE_TMA)) return fail(MPCF_ERR_ARG, "unknown tiling flags 0x%x", flags);
     DeviceGuard g(s->device);
     s->ty = ty;
     s->dz = dz;
-    s->persist = persistent != 0;
+    s->persist = (flags & MPCF_TILE_PERSISTENT) != 0;
+    s->tma = (flags & MPCF_TILE_TMA) != 0;
     return apply_tiling(s);
 }
 
-int mpcf_get_tiling(const mpcf_solver* s, int* ty, int* dz, int* persistent)
+int mpcf_get_tiling(const mpcf_solver* s, int* ty, int* dz, int* flags)
 {
     if (!s) return fail(MPCF_ERR_ARG, "null solver");
     if (ty) *ty = s->ty;
     if (dz) *dz = s->dz;
-    if (persistent) *persistent = s->persist;
+    if (flags) *flags = (s->persist ? MPCF_TILE_PERSISTENT : 0) | (s->tma ? MPCF_TILE_TMA : 0);
     return MPCF_OK;
 }
 
@@ -815,27 +903,30 @@ int mpcf_autotune(mpcf_solver* s, int reps, int* best3, double* best_ms)
         if (cudaMalloc(&scratch[d], bytes) != cudaSuccess) { cudaGetLastError(); rc = fail(MPCF_ERR_NOMEM, "autotune scratch"); break; }
         saved_R[d] = D.R;
     }
-    const int saved_ty = s->ty, saved_dz = s->dz, saved_p = s->persist, saved_parity = s->parity;
+    const int saved_ty = s->ty, saved_dz = s->dz, saved_p = s->persist, saved_m = s->tma, saved_parity = s->parity;
     std::vector<char> saved_dtinvh(s->esz * s->ndom);
     CK(cudaMemcpy(saved_dtinvh.data(), s->dtinvh, saved_dtinvh.size(), cudaMemcpyDeviceToHost));
-    int bty = saved_ty, bdz = saved_dz, bp = saved_p;
+    int bty = saved_ty, bdz = saved_dz, bp = saved_p, bm = saved_m;
     double bms = 1e300;
+    const bool can_tma = any_tma_ok(s);
     if (!rc)
     {
         int maxn = 0;
         for (auto& D : s->hdoms) maxn = std::max(maxn, D.nz);
-        std::vector<int> dzs = {16, 32, 64, 128};
+        std::vector<int> dzs;
+        for (int v : {16, 32, 64, 128}) if (v < maxn) dzs.push_back(v);
         dzs.push_back(maxn);
-        const int tys[4] = {2, 4, 8, 16};
-        for (int i = 0; i < 4 && !rc; ++i)
+        const int tys[3] = {4, 8, 16};
+        for (int i = 0; i < 3 && !rc; ++i)
         {
             if (!valid_ty(s, tys[i])) continue;
             for (int dz : dzs)
             {
-                if (dz > maxn && dz != maxn) continue;
-                for (int p = 0; p < 2 && !rc; ++p)
+                for (int f = 0; f < 4 && !rc; ++f)
                 {
-                    s->ty = tys[i]; s->dz = dz; s->persist = p;
+                    const int p = f & 1, m = (f >> 1) & 1;
+                    if (m && !can_tma) continue;
+                    s->ty = tys[i]; s->dz = dz; s->persist = p; s->tma = m;
                     for (int d = 0; d < s->ndom; ++d)
                     {
                         s->hdoms[d].R = scratch[d];
@@ -855,7 +946,7 @@ int mpcf_autotune(mpcf_solver* s, int reps, int* best3, double* best_ms)
                         s->parity = saved_parity;
                         tot += ms;
                     }
-                    if (!rc && tot / reps < bms) { bms = tot / reps; bty = tys[i]; bdz = dz; bp = p; }
+                    if (!rc && tot / reps < bms) { bms = tot / reps; bty = tys[i]; bdz = dz; bp = p; bm = m; }
                 }
             }
         }
@@ -865,13 +956,14 @@ int mpcf_autotune(mpcf_solver* s, int reps, int* best3, double* best_ms)
     s->ty = rc ? saved_ty : bty;
     s->dz = rc ? saved_dz : bdz;
     s->persist = rc ? saved_p : bp;
+    s->tma = rc ? saved_m : bm;
     int rc2 = apply_tiling(s);
     for (void* p : scratch) if (p) cudaFree(p);
     if (cudaMemcpy(s->dtinvh, saved_dtinvh.data(), saved_dtinvh.size(), cudaMemcpyHostToDevice) != cudaSuccess && !rc2)
         rc2 = fail(MPCF_ERR_CUDA, "restoring dt/h after autotune failed");
     if (rc) return rc;
     if (rc2) return rc2;
-    if (best3) { best3[0] = s->ty; best3[1] = s->dz; best3[2] = s->persist; }
+    if (best3) { best3[0] = s->ty; best3[1] = s->dz; best3[2] = (s->persist ? MPCF_TILE_PERSISTENT : 0) | (s->tma ? MPCF_TILE_TMA : 0); }
     if (best_ms) *best_ms = bms;
     return MPCF_OK;
 }

@@ -28,6 +28,17 @@
 // ping-ponged (read U[parity], write U[parity^1]) so neighbouring tiles
 // always see the old state.
 //
+// Loads.  Without TMA every thread loads its cells with ordinary global
+// loads (the generic path, any domain shape).  With TMA (domains whose rows
+// are multiples of 16 bytes), one elected thread issues two bulk tensor
+// copies per slab into shared memory -- the 40 x (TY+6) halo box of the next
+// slab and the 32 x TY interior of the slab three ahead -- which land while
+// the current slab's faces are evaluated; out-of-domain cells of the staged
+// box are mapped to their mirror / clamp source inside the box.  Waits on
+// the copies are bounded: a copy that does not complete sets an error bit,
+// the CTA stops waiting for copies and carries on (its data are then stale,
+// never out of bounds), so a failed copy cannot stall the launch.
+//
 // DRAM traffic per cell-stage: read U (7 T) + read R (7 T) + write R and
 // U_next (14 T) = 112 B in FP32.  Halo and ring re-reads hit L2.
 #pragma once
@@ -39,14 +50,19 @@ namespace mpcf {
 
 constexpr int kTX = 32;
 
-// Shared-memory layout of one CTA, as element offsets into one array of T
-// (so every stencil, x, y or z, is addressed as base + q*pitch + offs[j]):
+__host__ __device__ constexpr size_t align_up(size_t v, size_t a) { return (v + a - 1) / a * a; }
+
+// Shared-memory layout of one CTA.  The T region is addressed in elements
+// (so every stencil, x, y or z, is base + q*pitch + offs[j]):
 //   zwin  [6 slots][7 planes][TY][32]     ring of the tile's own columns
 //   cur   [7 planes][TY+6][38]            slab k with 3-cell x/y halos
 //   fx    [12][TY][33]                    x faces of slab k
 //   fy    [12][TY+1][32]                  y faces of slab k
-// followed by the FP64 reduction scratch [TY][5] and the tile broadcast.
-template <class T, int TY>
+// then, in bytes: the FP64 reduction scratch [TY][5], the tile broadcast,
+// two mbarriers and, with TMA, the two staging buffers (128-byte aligned):
+//   A     [7][TY+6][40]                   halo box, x from x0-4, y from y0-3
+//   B     [7][TY][32]                     interior of a slab
+template <class T, int TY, bool TMA>
 struct StageLayout
 {
     static constexpr int kCurW   = kTX + 6;
@@ -60,8 +76,17 @@ struct StageLayout
     static constexpr int kFx     = kCur + 7 * kCurP;
     static constexpr int kFy     = kFx + 12 * kFxP;
     static constexpr int kEnd    = kFy + 12 * kFyP;
-    static constexpr size_t kRedBytes = ((kEnd * sizeof(T) + 15) / 16) * 16;
-    static constexpr size_t kBytes = kRedBytes + sizeof(double) * TY * 5 + 16;
+    static constexpr int kAW     = kTX + 8;                // staged halo box width
+    static constexpr int kAH     = TY + 6;                 // staged halo box height
+    static constexpr size_t kRedBytes  = align_up(kEnd * sizeof(T), 16);
+    static constexpr size_t kTileBytes = kRedBytes + sizeof(double) * TY * 5;
+    static constexpr size_t kMbarBytes = align_up(kTileBytes + 16, 16);
+    static constexpr size_t kABytes    = sizeof(T) * 7 * kAH * kAW;
+    static constexpr size_t kBBytes    = sizeof(T) * 7 * TY * kTX;
+    static constexpr size_t kStageA    = align_up(kMbarBytes + 16, 128);
+    static constexpr size_t kStageB    = align_up(kStageA + kABytes, 128);
+    // + 128: the kernel rounds the dynamic shared-memory base up to 128 B
+    static constexpr size_t kBytes     = (TMA ? kStageB + kBBytes : kMbarBytes + 16) + 128;
 };
 
 // Boundary-condition map of one coordinate: absorbing clamps to the edge
@@ -110,6 +135,60 @@ __device__ __forceinline__ bool physical(const T r, const T e, const T G, const 
     return (r > (T)0) && (e > (T)0) && (G > (T)0) && (P >= (T)0) && (e < (T)INFINITY) && (r < (T)INFINITY);
 }
 
+// ---------------------------------------------------------------------------
+// Bulk tensor copies (TMA) and mbarriers, hand-written PTX for sm_100a.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ void mbar_init(uint32_t bar, uint32_t count)
+{
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" :: "r"(bar), "r"(count) : "memory");
+}
+
+__device__ __forceinline__ void mbar_init_fence()
+{
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+
+__device__ __forceinline__ void mbar_expect_tx(uint32_t bar, uint32_t bytes)
+{
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" :: "r"(bar), "r"(bytes) : "memory");
+}
+
+__device__ __forceinline__ bool mbar_try_wait(uint32_t bar, uint32_t parity)
+{
+    uint32_t ok;
+    asm volatile("{\n\t.reg .pred p;\n\t"
+                 "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+                 "selp.u32 %0, 1, 0, p;\n\t}"
+                 : "=r"(ok) : "r"(bar), "r"(parity) : "memory");
+    return ok != 0;
+}
+
+// Bounded wait for the phase with parity `parity`; false after the limit.
+__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity)
+{
+    for (int i = 0; i < (1 << 20); ++i)
+        if (mbar_try_wait(bar, parity)) return true;
+    return false;
+}
+
+// Generic-proxy accesses of this thread before async-proxy (bulk copy)
+// accesses that follow: orders shared-memory reuse of a staging buffer.
+__device__ __forceinline__ void fence_proxy_async()
+{
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+
+// 4-D tile copy global -> shared, completion counted on `bar` (no multicast).
+__device__ __forceinline__ void tma_load_4d(uint32_t dst, const void* tmap, int c0, int c1, int c2, int c3, uint32_t bar)
+{
+    asm volatile("cp.async.bulk.tensor.4d.shared::cluster.global.tile.mbarrier::complete_tx::bytes"
+                 " [%0], [%1, {%2, %3, %4, %5}], [%6];"
+                 :: "r"(dst), "l"(tmap), "r"(c0), "r"(c1), "r"(c2), "r"(c3), "r"(bar) : "memory");
+}
+
 // Register budget: at least kMinWarpsPerSM resident warps per SM.  The
 // face pipeline has 14 independent reconstructions, so the compiler would
 // otherwise trade occupancy for unbounded instruction-level parallelism.
@@ -123,16 +202,22 @@ template <class T, int TY> struct MinBlocks
     static constexpr int v = (w / TY) > 0 ? (w / TY) : 1;
 };
 
-template <class Pol, int TY, bool PERSIST, bool SUMS>
+template <class Pol, int TY, bool PERSIST, bool SUMS, bool TMA>
 __global__ void __launch_bounds__(kTX * TY, MinBlocks<typename Pol::T, TY>::v)
 stage_kernel(const StageArgs A)
 {
     typedef typename Pol::T T;
-    typedef StageLayout<T, TY> L;
-    extern __shared__ __align__(16) unsigned char smem_raw[];
+    typedef StageLayout<T, TY, TMA> L;
+    extern __shared__ __align__(16) unsigned char smem_dyn[];
+    // 128-byte aligned base (bulk tensor copies need it for their targets)
+    unsigned char* smem_raw = smem_dyn + ((128u - (smem_u32(smem_dyn) & 127u)) & 127u);
     T* sm = reinterpret_cast<T*>(smem_raw);
     double* red = reinterpret_cast<double*>(smem_raw + L::kRedBytes);
-    int* tile_bc = reinterpret_cast<int*>(smem_raw + L::kRedBytes + sizeof(double) * TY * 5);
+    int* tile_bc = reinterpret_cast<int*>(smem_raw + L::kTileBytes);
+    const uint32_t barA = smem_u32(smem_raw + L::kMbarBytes);
+    const uint32_t barB = barA + 8;
+    T* stA = reinterpret_cast<T*>(smem_raw + L::kStageA);
+    T* stB = reinterpret_cast<T*>(smem_raw + L::kStageB);
 
     const int tx = threadIdx.x & (kTX - 1);
     const int ty = threadIdx.x >> 5;
@@ -140,6 +225,14 @@ stage_kernel(const StageArgs A)
     const T b = (T)A.b;
     const T factor6 = (T)1.0f / (T)6.0f;   // GPUkernels.cu:1103
     bool ok = true;
+    uint32_t phA = 0, phB = 0;             // mbarrier phase parities
+    bool tma_late = false;
+
+    if (TMA)
+    {
+        if (threadIdx.x == 0) { mbar_init(barA, 1); mbar_init(barB, 1); mbar_init_fence(); }
+        __syncthreads();
+    }
 
     int t;
     if (PERSIST)
@@ -165,6 +258,9 @@ stage_kernel(const StageArgs A)
         T* __restrict__       Un   = (T*)DD.U[A.parity ^ 1];
         T* __restrict__       R    = (T*)DD.R;
         const T dtinvh = ((const T*)A.dtinvh)[d];
+        const bool use_tma = TMA && DD.tma_ok;
+        // tensor maps of the buffer read in this stage: halo box, interior box
+        const char* tm = (const char*)A.tmaps + ((size_t)d * 4 + (size_t)A.parity * 2) * 128;
 
         const int lt = t - DD.tile_begin;
         const int bx = lt % DD.tiles_x;
@@ -186,6 +282,16 @@ stage_kernel(const StageArgs A)
 #pragma unroll
             for (int m = 0; m < 7; ++m) sm[L::kZwin + slot * L::kZSlot + m * L::kZPlane + own] = q[m];
         }
+        if (use_tma && threadIdx.x == 0)
+        {
+            // first copies: halo box of slab z0 and interior of slab z0+2
+            bool fz;
+            fence_proxy_async();
+            mbar_expect_tx(barA, (uint32_t)L::kABytes);
+            tma_load_4d(smem_u32(stA), tm, x0 - 4, y0 - 3, bc_map(z0, D.nz, D.bc4, D.bc5, fz), 0, barA);
+            mbar_expect_tx(barB, (uint32_t)L::kBBytes);
+            tma_load_4d(smem_u32(stB), tm + 128, x0, y0, bc_map(z0 + 2, D.nz, D.bc4, D.bc5, fz), 0, barB);
+        }
 
         T Sp[7];                 // x/y part of the flux bracket of cell k-1
         T sG = 0, sP = 0, dU = 0;
@@ -199,6 +305,26 @@ stage_kernel(const StageArgs A)
         for (int k = z0; k <= z1; ++k)
         {
             // (A) leading slab k+2 of the own column
+            if (use_tma)
+            {
+                if (!tma_late && !mbar_wait(barB, phB)) tma_late = true;
+                phB ^= 1;
+                bool fx, fy, fz;
+                const int mx = min(max(bc_map(gx, D.nx, D.bc0, D.bc1, fx) - x0, 0), kTX - 1);
+                const int my = min(max(bc_map(gy, D.ny, D.bc2, D.bc3, fy) - y0, 0), TY - 1);
+                bc_map(k + 2, D.nz, D.bc4, D.bc5, fz);
+                T c[7], q[7];
+#pragma unroll
+                for (int m = 0; m < 7; ++m) c[m] = stB[(m * TY + my) * kTX + mx];
+                if (fx) c[1] = -c[1];
+                if (fy) c[2] = -c[2];
+                if (fz) c[3] = -c[3];
+                to_primitive<Pol>(c, q);
+                const int slot = (k + 2 + 6) % 6;
+#pragma unroll
+                for (int m = 0; m < 7; ++m) sm[L::kZwin + slot * L::kZSlot + m * L::kZPlane + own] = q[m];
+            }
+            else
             {
                 T q[7];
                 load_prim<Pol>(D, U, gx, gy, k + 2, q);
@@ -209,33 +335,76 @@ stage_kernel(const StageArgs A)
             // (B) slab k with halos into cur
             if (k < z1)
             {
-                const int slot = (k + 6) % 6;
-#pragma unroll
-                for (int m = 0; m < 7; ++m)
-                    sm[L::kCur + m * L::kCurP + (ty + 3) * L::kCurW + tx + 3] = sm[L::kZwin + slot * L::kZSlot + m * L::kZPlane + own];
-                for (int i = threadIdx.x; i < 6 * kTX + 6 * TY; i += kTX * TY)
+                if (use_tma)
                 {
-                    int lx, ly;
-                    if (i < 6 * kTX)
+                    if (!tma_late && !mbar_wait(barA, phA)) tma_late = true;
+                    phA ^= 1;
+                    bool fz;
+                    bc_map(k, D.nz, D.bc4, D.bc5, fz);
+                    for (int i = threadIdx.x; i < (TY + 6) * L::kCurW; i += kTX * TY)
                     {
-                        const int r = i >> 5;
-                        lx = i & (kTX - 1);
-                        ly = r < 3 ? r - 3 : TY + r - 3;
-                    }
-                    else
-                    {
-                        const int j = i - 6 * kTX;
-                        const int c = j % 6;
-                        ly = j / 6;
-                        lx = c < 3 ? c - 3 : kTX + c - 3;
-                    }
-                    T q[7];
-                    load_prim<Pol>(D, U, x0 + lx, y0 + ly, k, q);
+                        const int ly = i / L::kCurW - 3, lx = i % L::kCurW - 3;
+                        bool fx, fy;
+                        const int mx = min(max(bc_map(x0 + lx, D.nx, D.bc0, D.bc1, fx) - x0 + 4, 0), L::kAW - 1);
+                        const int my = min(max(bc_map(y0 + ly, D.ny, D.bc2, D.bc3, fy) - y0 + 3, 0), L::kAH - 1);
+                        T c[7], q[7];
 #pragma unroll
-                    for (int m = 0; m < 7; ++m) sm[L::kCur + m * L::kCurP + (ly + 3) * L::kCurW + lx + 3] = q[m];
+                        for (int m = 0; m < 7; ++m) c[m] = stA[(m * L::kAH + my) * L::kAW + mx];
+                        if (fx) c[1] = -c[1];
+                        if (fy) c[2] = -c[2];
+                        if (fz) c[3] = -c[3];
+                        to_primitive<Pol>(c, q);
+#pragma unroll
+                        for (int m = 0; m < 7; ++m) sm[L::kCur + m * L::kCurP + (ly + 3) * L::kCurW + lx + 3] = q[m];
+                    }
+                }
+                else
+                {
+                    const int slot = (k + 6) % 6;
+#pragma unroll
+                    for (int m = 0; m < 7; ++m)
+                        sm[L::kCur + m * L::kCurP + (ty + 3) * L::kCurW + tx + 3] = sm[L::kZwin + slot * L::kZSlot + m * L::kZPlane + own];
+                    for (int i = threadIdx.x; i < 6 * kTX + 6 * TY; i += kTX * TY)
+                    {
+                        int lx, ly;
+                        if (i < 6 * kTX)
+                        {
+                            const int r = i >> 5;
+                            lx = i & (kTX - 1);
+                            ly = r < 3 ? r - 3 : TY + r - 3;
+                        }
+                        else
+                        {
+                            const int j = i - 6 * kTX;
+                            const int c = j % 6;
+                            ly = j / 6;
+                            lx = c < 3 ? c - 3 : kTX + c - 3;
+                        }
+                        T q[7];
+                        load_prim<Pol>(D, U, x0 + lx, y0 + ly, k, q);
+#pragma unroll
+                        for (int m = 0; m < 7; ++m) sm[L::kCur + m * L::kCurP + (ly + 3) * L::kCurW + lx + 3] = q[m];
+                    }
                 }
             }
             __syncthreads();
+            // the staging buffers are free again: copy the next slab's data
+            // while this slab's faces are evaluated
+            if (use_tma && threadIdx.x == 0)
+            {
+                bool fz;
+                fence_proxy_async();
+                if (k + 1 <= z1)
+                {
+                    mbar_expect_tx(barB, (uint32_t)L::kBBytes);
+                    tma_load_4d(smem_u32(stB), tm + 128, x0, y0, bc_map(k + 3, D.nz, D.bc4, D.bc5, fz), 0, barB);
+                }
+                if (k + 1 < z1)
+                {
+                    mbar_expect_tx(barA, (uint32_t)L::kABytes);
+                    tma_load_4d(smem_u32(stA), tm, x0 - 4, y0 - 3, bc_map(k + 1, D.nz, D.bc4, D.bc5, fz), 0, barA);
+                }
+            }
 
             // (C) faces of slab k: job 0 = z face k-1/2 of the own column (kept
             // in registers), job 1 = x face left of the own cell, job 2 = y face
@@ -361,9 +530,10 @@ stage_kernel(const StageArgs A)
     }
 
     if (!__all_sync(0xffffffffu, ok) && tx == 0) atomicOr(A.err, (unsigned)ERRBIT_NONPHYSICAL);
+    if (TMA && tma_late) atomicOr(A.err, (unsigned)ERRBIT_TMA_TIMEOUT);
 }
 
-template <class T, int TY>
-constexpr size_t stage_smem_bytes() { return StageLayout<T, TY>::kBytes; }
+template <class T, int TY, bool TMA>
+constexpr size_t stage_smem_bytes() { return StageLayout<T, TY, TMA>::kBytes; }
 
 } // namespace mpcf

@@ -16,6 +16,7 @@ enum { BC_ABSORBING = 0, BC_REFLECTING = 1 };
 enum {
     ERRBIT_NONPHYSICAL = 1u << 0,   // rho <= 0, E <= 0, G <= 0, P < 0 or non-finite after an update
     ERRBIT_SOS_NONFINITE = 1u << 1, // max sound speed not finite or not positive
+    ERRBIT_TMA_TIMEOUT = 1u << 2,   // a bulk tensor copy did not complete within the wait limit
 };
 
 // One domain as the kernels see it.  All 7 fields of a buffer live in one
@@ -32,6 +33,7 @@ struct DomDev
     int    tile_begin;  // first global tile id of this domain
     int    sos_chunk_begin;   // first global sound-speed chunk of this domain
     int    sos_chunks;
+    int    tma_ok;      // 1: tensor maps of this domain are valid (rows of 16-byte multiples)
     double h;
 };
 
@@ -48,6 +50,7 @@ struct StageArgs
     unsigned* counter;  // persistent-launch work counter (zeroed before launch)
     unsigned* err;      // device error word
     double* tile_sums;  // [ntiles][5] FP64 partial conservation sums, or null
+    const void* tmaps;  // per domain 4 CUtensorMap (128 B each): [buffer 0, 1] x [halo box, interior box]
 };
 
 struct SosArgs

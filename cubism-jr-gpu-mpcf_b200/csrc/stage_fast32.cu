@@ -1,0 +1,20 @@
+// stage_fast32.cu -- stage kernels of the PolFast32 precision policy (one
+// translation unit per policy, so they compile in parallel).  Built with
+// fused multiply-adds allowed; the single-precision policies also use
+// approximate division and square root (-prec-div=false -prec-sqrt=false),
+// which leaves double-precision operations untouched.
+#include "stage_dispatch.cuh"
+
+namespace mpcf {
+
+cudaError_t launch_stage_fast32(int ty, bool persist, bool tma, const StageArgs& A, int grid, cudaStream_t st)
+{
+    return StageDispatch<PolFast32, false>::launch(ty, persist, tma, A, grid, st);
+}
+
+StageKernelInfo stage_info_fast32(int ty, bool persist, bool sums, bool tma)
+{
+    return StageDispatch<PolFast32, false>::info(ty, persist, sums, tma);
+}
+
+} // namespace mpcf

@@ -5,8 +5,6 @@
 // -ftz=false: every floating-point operation then rounds like the literal
 // C semantics of the reference source, so the results are bit-identical to
 // the CPU restatement.  The build refuses to compile it otherwise.
-#include "mpcf_stage.cuh"
-#include "mpcf_launch.h"
 #include "stage_dispatch.cuh"
 
 #if defined(__CUDA_ARCH__) && !defined(MPCF_NO_FMAD)
@@ -15,14 +13,14 @@
 
 namespace mpcf {
 
-cudaError_t launch_stage_ref(int ty, bool persist, const StageArgs& A, int grid, cudaStream_t st)
+cudaError_t launch_stage_ref(int ty, bool persist, bool tma, const StageArgs& A, int grid, cudaStream_t st)
 {
-    return StageDispatch<PolRef32, true>::launch(ty, persist, A, grid, st);
+    return StageDispatch<PolRef32, true>::launch(ty, persist, tma, A, grid, st);
 }
 
-StageKernelInfo stage_info_ref(int ty, bool persist, bool sums)
+StageKernelInfo stage_info_ref(int ty, bool persist, bool sums, bool tma)
 {
-    return StageDispatch<PolRef32, true>::info(ty, persist, sums);
+    return StageDispatch<PolRef32, true>::info(ty, persist, sums, tma);
 }
 
 } // namespace mpcf

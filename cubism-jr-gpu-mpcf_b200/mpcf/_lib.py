@@ -23,6 +23,9 @@ BC_REFLECTING = 1
 ERR_ARG, ERR_CUDA, ERR_NOMEM, ERR_STATE, ERR_NUMERIC = -1, -2, -3, -4, -5
 ERRBIT_NONPHYSICAL = 1
 ERRBIT_SOS = 2
+ERRBIT_TMA_TIMEOUT = 4
+TILE_PERSISTENT = 1
+TILE_TMA = 2
 
 # every symbol the header declares, with (restype, argtypes)
 _c = ctypes

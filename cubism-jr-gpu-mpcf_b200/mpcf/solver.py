@@ -167,19 +167,21 @@ class Solver:
                                   b.ctypes.data_as(ctypes.POINTER(ctypes.c_double)) if nb else None))
 
     # -- launch configuration ----------------------------------------------
-    def set_tiling(self, ty, dz, persistent=False):
-        check(lib().mpcf_set_tiling(self._h, int(ty), int(dz), 1 if persistent else 0))
+    def set_tiling(self, ty, dz, persistent=False, tma=True):
+        flags = (_lib.TILE_PERSISTENT if persistent else 0) | (_lib.TILE_TMA if tma else 0)
+        check(lib().mpcf_set_tiling(self._h, int(ty), int(dz), flags))
 
     def tiling(self):
-        ty, dz, p = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
-        check(lib().mpcf_get_tiling(self._h, ctypes.byref(ty), ctypes.byref(dz), ctypes.byref(p)))
-        return ty.value, dz.value, bool(p.value)
+        """(ty, dz, persistent, tma) of the current launch configuration."""
+        ty, dz, f = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
+        check(lib().mpcf_get_tiling(self._h, ctypes.byref(ty), ctypes.byref(dz), ctypes.byref(f)))
+        return ty.value, dz.value, bool(f.value & _lib.TILE_PERSISTENT), bool(f.value & _lib.TILE_TMA)
 
     def autotune(self, reps=3):
         best = (ctypes.c_int * 3)()
         ms = ctypes.c_double()
         check(lib().mpcf_autotune(self._h, int(reps), best, ctypes.byref(ms)))
-        return (best[0], best[1], bool(best[2])), ms.value
+        return (best[0], best[1], bool(best[2] & _lib.TILE_PERSISTENT), bool(best[2] & _lib.TILE_TMA)), ms.value
 
     def launch_shape(self):
         nt, g, th = ctypes.c_longlong(), ctypes.c_longlong(), ctypes.c_int()

@@ -54,6 +54,11 @@ typedef struct mpcf_solver mpcf_solver;
 /* bits of the device error word */
 #define MPCF_ERRBIT_NONPHYSICAL  1u  /* rho<=0, E<=0, G<=0, P<0 or non-finite after an update */
 #define MPCF_ERRBIT_SOS          2u  /* maximum speed of sound not finite or not positive */
+#define MPCF_ERRBIT_TMA_TIMEOUT  4u  /* a bulk tensor copy did not complete within the wait limit */
+
+/* stage-kernel tiling flags (mpcf_set_tiling / mpcf_get_tiling / mpcf_autotune) */
+#define MPCF_TILE_PERSISTENT 1  /* one CTA per resident slot pulling tiles from a work counter */
+#define MPCF_TILE_TMA        2  /* stage slabs with bulk tensor copies (domains with nx*elem % 16 == 0) */
 
 /* Bubble-cloud initial condition (liquid with gas bubbles; indicator
  * alpha = 0.5*(1 - tanh(phi/(width*h))), phi = distance to the nearest
@@ -186,12 +191,15 @@ int mpcf_bubbles(unsigned long long seed, int n, double rmin, double rmax,
                  const double* lo3, const double* hi3, double gap, int max_tries, double* out4);
 
 /* ---- launch configuration ------------------------------------------------- *
- * tile = 32 x ty columns x dz slabs; persistent = one CTA per resident slot
- * pulling tiles from a work counter.  mpcf_autotune times the candidates on
- * the solver's own state (which it leaves unchanged) and keeps the fastest;
- * best[3] (optional) = {ty, dz, persistent}, best_ms (optional) = stage time. */
-int mpcf_set_tiling(mpcf_solver* s, int ty, int dz, int persistent);
-int mpcf_get_tiling(const mpcf_solver* s, int* ty, int* dz, int* persistent);
+ * tile = 32 x ty columns x dz slabs (ty 4 or 8; 16 for MPCF_PREC_FP32_REF);
+ * flags = MPCF_TILE_PERSISTENT | MPCF_TILE_TMA.  With MPCF_TILE_TMA, domains
+ * whose rows are multiples of 16 bytes stage their slabs with bulk tensor
+ * copies (other domains keep ordinary loads).  mpcf_autotune times the
+ * candidates on the solver's own state (which it leaves unchanged) and
+ * keeps the fastest; best3 (optional) = {ty, dz, flags}, best_ms (optional)
+ * = stage time. */
+int mpcf_set_tiling(mpcf_solver* s, int ty, int dz, int flags);
+int mpcf_get_tiling(const mpcf_solver* s, int* ty, int* dz, int* flags);
 int mpcf_autotune(mpcf_solver* s, int reps, int* best3, double* best_ms);
 
 /* number of tiles one stage launch processes, and of stage-kernel CTAs */

@@ -69,7 +69,8 @@ def test_ref32_stage_bitexact(mpcf, dims, bc):
     assert_bitwise(Rg, Ro, "register")
 
 
-@pytest.mark.parametrize("tiling", [(2, 3, False), (4, 64, False), (8, 5, True), (16, 7, False), (4, 1, True)])
+@pytest.mark.parametrize("tiling", [(4, 3, False, False), (4, 64, False, True), (8, 5, True, True), (16, 7, False, True),
+                                    (4, 1, True, True), (8, 9, True, False), (16, 2, True, True)])
 def test_ref32_tiling_invariant(mpcf, tiling):
     dims, bc = (45, 19, 14), (ABS, REF, ABS, ABS, REF, ABS)
     U0 = cloud_state(dims, nb=3)

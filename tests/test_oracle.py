@@ -6,10 +6,11 @@
    MaxSpeedOfSound_CPP.  Bit-exact.
 2. The same comparisons live against oracle/_ref when it was built here.
 3. Known-answer properties of the whole stage (the reference's kernels have
-   no golden outputs): uniform states are invariant, axis permutations
-   commute, mirror-symmetric states stay symmetric, mass and energy are
-   conserved between reflecting walls, and the two sound-speed formulas
-   agree.
+   no golden outputs): uniform states are invariant, x <-> y permutations
+   commute bit for bit (x <-> z to rounding: the extra-term sums are
+   accumulated x, y, z), mirror-symmetric states stay symmetric, mass and
+   energy are conserved between reflecting walls, and the two sound-speed
+   formulas agree.
 4. The FP32 roofline constant of bench.py equals the operation counter.
 """
 import ctypes
@@ -246,7 +247,13 @@ def test_axis_permutation_equivalence():
         O.step(pd, bc, U, R)
         back = permute(U, pd, tuple(np.argsort(axes)))
         for q in range(7):
-            assert np.array_equal(back[q], Ux[q]), (axes, q)
+            if axes == (1, 0, 2):
+                assert np.array_equal(back[q], Ux[q]), (axes, q)
+            else:
+                # x <-> z moves the varying term of the extra-term sums
+                # ((X + Y) + Z) from first to last place: equal to rounding
+                d = np.abs(back[q].astype(np.float64) - Ux[q]).max()
+                assert d <= 1e-6 * max(np.abs(Ux[q]).max(), 1.0), (axes, q)
 
 
 def test_mirror_symmetry_preserved():
