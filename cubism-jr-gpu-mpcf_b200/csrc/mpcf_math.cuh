@@ -199,6 +199,69 @@ __device__ __forceinline__ void weno_pair_factored(const typename Pol::T s0, con
 }
 
 // ---------------------------------------------------------------------------
+// Packed single-precision pairs.  sm_100 executes fma / add / mul on two
+// FP32 lanes in one instruction (round-to-nearest per lane, the same result
+// as two scalar instructions).  The face pipeline is bound by instruction
+// issue, so every left/right-symmetric computation runs as one pair.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ float2 f2(const float a, const float b) { return make_float2(a, b); }
+__device__ __forceinline__ float2 f2s(const float a) { return make_float2(a, a); }
+__device__ __forceinline__ float2 add2(const float2 a, const float2 b) { return __fadd2_rn(a, b); }
+__device__ __forceinline__ float2 sub2(const float2 a, const float2 b) { return __fadd2_rn(a, make_float2(-b.x, -b.y)); }
+__device__ __forceinline__ float2 mul2(const float2 a, const float2 b) { return __fmul2_rn(a, b); }
+__device__ __forceinline__ float2 fma2(const float2 a, const float2 b, const float2 c) { return __ffma2_rn(a, b, c); }
+__device__ __forceinline__ float2 rcp2(const float2 a) { return make_float2(rcp_approx(a.x), rcp_approx(a.y)); }
+// HLLC upwind blend w.x * F.x + w.y * F.y of a (left, right) flux pair
+__device__ __forceinline__ float blend2(const float2 w, const float2 F) { const float2 t = mul2(F, w); return t.x + t.y; }
+
+// Both reconstructions of one face (fast policies) as one packed pair.
+// The plus side is the mirror image of the minus side: with
+//   lane x (minus): (x0..x4) = (s0, s1, s2, s3, s4)
+//   lane y (plus):  (x0..x4) = (s5, s4, s3, s2, s1)
+// both lanes evaluate the same expressions (GPUonly.cuh:99-194):
+//   is0 = 13/12 (x0-2x1+x2)^2 + 1/4 (x0-4x1+3x2)^2
+//   is1 = 13/12 (x1-2x2+x3)^2 + 1/4 (x1-x3)^2
+//   is2 = 13/12 (x2-2x3+x4)^2 + 1/4 (3x2-4x3+x4)^2
+//   p0 = (2x0-7x1+11x2)/6, p1 = (-x1+5x2+2x3)/6, p2 = (2x2+5x3-x4)/6
+//   r  = (a0 p0 + 6 a1 p1 + 3 a2 p2) / (a0 + 6 a1 + 3 a2), a_k = 1/(is_k+eps)^2
+// with the smoothness indicators in the factored, cancellation-free form
+// (the same polynomials as the reference's expanded beta_f / beta_h /
+// beta_g, coefficient by coefficient), scaled by 12 (the scale cancels in
+// the ratio), and the ratio in difference form
+//   r = p2 + (a0 (p0-p2) + a1 * 6(p1-p2)) / (a0 + 6 a1 + 3 a2)
+// so no normalised weight is formed.  Each lane is then clipped to
+// [min, max] of its three central cells.
+__device__ __forceinline__ void weno_pair_packed(const float s0, const float s1, const float s2,
+                                                 const float s3, const float s4, const float s5,
+                                                 float& m, float& p)
+{
+    const float2 X = f2(s0, s5), Y = f2(s1, s4), Z = f2(s2, s3), W = f2(s3, s2), V = f2(s4, s1);
+    const float2 k0 = fma2(Y, f2s(-2.f), add2(X, Z));
+    const float2 k1 = fma2(Z, f2s(-2.f), add2(Y, W));
+    const float2 k2 = fma2(W, f2s(-2.f), add2(Z, V));
+    const float2 a0 = fma2(Z, f2s(3.f), fma2(Y, f2s(-4.f), X));
+    const float2 a1 = sub2(Y, W);
+    const float2 a2 = fma2(Z, f2s(3.f), fma2(W, f2s(-4.f), V));
+    const float2 eps12 = f2s((float)(12.0 * MPCF_WENOEPS));
+    // 12 (is_k + eps) = 13 k^2 + 3 a^2 + 12 eps
+    const float2 i0 = fma2(mul2(k0, f2s(13.f)), k0, fma2(mul2(a0, f2s(3.f)), a0, eps12));
+    const float2 i1 = fma2(mul2(k1, f2s(13.f)), k1, fma2(mul2(a1, f2s(3.f)), a1, eps12));
+    const float2 i2 = fma2(mul2(k2, f2s(13.f)), k2, fma2(mul2(a2, f2s(3.f)), a2, eps12));
+    const float2 r0 = rcp2(mul2(i0, i0));
+    const float2 r1 = rcp2(mul2(i1, i1));
+    const float2 r2 = rcp2(mul2(i2, i2));
+    const float2 inv = rcp2(fma2(r2, f2s(3.f), fma2(r1, f2s(6.f), r0)));
+    const float2 p2 = fma2(V, f2s(-1.f / 6.f), fma2(W, f2s(5.f / 6.f), mul2(Z, f2s(1.f / 3.f))));
+    const float2 p0 = fma2(Z, f2s(11.f / 6.f), fma2(Y, f2s(-7.f / 6.f), mul2(X, f2s(1.f / 3.f))));
+    const float2 d1 = fma2(sub2(Z, W), f2s(3.f), sub2(V, Y));         // 6 (p1 - p2)
+    const float2 num = fma2(r1, d1, mul2(r0, sub2(p0, p2)));
+    const float2 r = fma2(num, inv, p2);
+    const float lo23 = fminf(s2, s3), hi23 = fmaxf(s2, s3);
+    m = fminf(fmaxf(r.x, fminf(s1, lo23)), fmaxf(s1, hi23));
+    p = fminf(fmaxf(r.y, fminf(s4, lo23)), fmaxf(s4, hi23));
+}
+
+// ---------------------------------------------------------------------------
 // HLLC pieces.  sign_star in {-1,0,1}; the two weights (1+s)/2 and (1-s)/2.
 // ---------------------------------------------------------------------------
 __device__ __forceinline__ int sign_star_of(const float ss)  { return ss == 0 ? 0 : (ss < 0 ? -1 : 1); }
@@ -324,6 +387,78 @@ __device__ __forceinline__ void hllc_face(const FaceState<typename Pol::T>& S, c
     o.Gm = Gm; o.Gp = Gp; o.Pm = Pm; o.Pp = Pp;
 }
 
+// The same face in the fast policies: every left/right-symmetric quantity is
+// one packed pair (lane x = minus / left, lane y = plus / right) and the
+// divisions are single-precision reciprocals.  The operations follow
+// hllc_face above term by term.
+__device__ __forceinline__ void hllc_face_packed(const FaceState<float>& S, const int dir, FaceOut<float>& o)
+{
+    const float2 Rh = f2(S.rm, S.rp), Uh = f2(S.nm, S.np), Ph = f2(S.pm, S.pp);
+    const float2 Gh = f2(S.Gm, S.Gp), Qh = f2(S.Pm, S.Pp);
+    const float2 T1 = f2(S.t1m, S.t1p), T2 = f2(S.t2m, S.t2p);
+    const float um = S.nm, up = S.np;
+
+    // Einfeldt bounds
+    const float2 ir = rcp2(Rh);
+    const float Rr   = sqrtf(S.rp * ir.x);
+    const float Rinv = rcp_approx(1.0f + Rr);
+    const float2 c2 = mul2(fma2(add2(Ph, Qh), rcp2(Gh), Ph), ir);
+    const float cm = sqrtf(c2.x), cp = sqrtf(c2.y);
+    const float eta_2 = 0.5f * Rr * Rinv * Rinv;
+    const float du = up - um;
+    const float d  = sqrtf((c2.x + Rr * c2.y) * Rinv + eta_2 * du * du);
+    const float uu = (um + Rr * up) * Rinv;
+    const float sm = fminf(uu - d, um - cm);
+    const float sp = fmaxf(uu + d, up + cp);
+
+    // Batten star speed
+    const float2 SU  = sub2(f2(sm, sp), Uh);                  // (sm - um, sp - up)
+    const float2 fac = mul2(Rh, SU);
+    const float ss = (S.pp - S.pm + um * fac.x - up * fac.y) * rcp_approx(fac.x - fac.y);
+    const int s = sign_star_of(ss);
+    const float2 Sg  = f2(fminf(0.0f, sm), fmaxf(0.0f, sp));
+    const float2 SS  = f2s(ss);
+    const float2 chi = mul2(SU, rcp2(sub2(f2(sm, sp), SS)));
+    const float2 Wb  = f2(0.5f * (float)(1 + s), 0.5f * (float)(1 - s));
+
+    // rho, G, P (passive)
+    o.f[0] = blend2(Wb, fma2(Sg, fma2(Rh, chi, f2(-S.rm, -S.rp)), mul2(Rh, Uh)));
+    o.f[5] = blend2(Wb, fma2(Sg, fma2(Gh, chi, f2(-S.Gm, -S.Gp)), mul2(Gh, Uh)));
+    o.f[6] = blend2(Wb, fma2(Sg, fma2(Qh, chi, f2(-S.Pm, -S.Pp)), mul2(Qh, Uh)));
+    // normal momentum
+    float fn;
+    {
+        const float2 Q = mul2(Rh, Uh);
+        const float2 qd = sub2(mul2(mul2(Rh, SS), chi), Q);
+        fn = blend2(Wb, fma2(Sg, qd, fma2(Q, Uh, Ph)));
+    }
+    // transverse momenta
+    float ft1, ft2;
+    {
+        const float2 Q = mul2(Rh, T1);
+        ft1 = blend2(Wb, fma2(Sg, sub2(mul2(Q, chi), Q), mul2(Q, Uh)));
+    }
+    {
+        const float2 Q = mul2(Rh, T2);
+        ft2 = blend2(Wb, fma2(Sg, sub2(mul2(Q, chi), Q), mul2(Q, Uh)));
+    }
+    // energy
+    {
+        const float2 ke = fma2(T2, T2, fma2(T1, T1, mul2(Uh, Uh)));
+        const float2 Q  = fma2(mul2(f2s(0.5f), Rh), ke, fma2(Gh, Ph, Qh));
+        const float2 inner = fma2(Rh, SS, mul2(Ph, rcp2(SU)));
+        const float2 qd = sub2(mul2(chi, fma2(sub2(SS, Uh), inner, Q)), Q);
+        o.f[4] = blend2(Wb, fma2(Sg, qd, mul2(Uh, add2(Q, Ph))));
+    }
+    // extra-term velocity
+    o.vel = blend2(Wb, fma2(Sg, add2(chi, f2s(-1.0f)), Uh));
+
+    o.f[1] = dir == 0 ? fn : ft1;
+    o.f[2] = dir == 1 ? fn : (dir == 0 ? ft1 : ft2);
+    o.f[3] = dir == 2 ? fn : ft2;
+    o.Gm = S.Gm; o.Gp = S.Gp; o.Pm = S.Pm; o.Pp = S.Pp;
+}
+
 // Full face from primitives in shared memory: cell j (j = 0..5 for cells
 // i-3..i+2 around face i-1/2) of primitive plane q sits at
 // sm[base + q*pitch + offs[j]].  The velocity planes are permuted by `dir`
@@ -342,7 +477,7 @@ __device__ __forceinline__ void face_flux(const typename Pol::T* __restrict__ sm
         const T* b_ = sm + base + (q) * pitch; \
         const T s0 = b_[offs[0]], s1 = b_[offs[1]], s2 = b_[offs[2]], \
                 s3 = b_[offs[3]], s4 = b_[offs[4]], s5 = b_[offs[5]]; \
-        if (Pol::kFastWeno) weno_pair_factored<Pol>(s0, s1, s2, s3, s4, s5, M, P); \
+        if constexpr (Pol::kFastWeno) weno_pair_packed(s0, s1, s2, s3, s4, s5, M, P); \
         else { M = weno_minus_clipped<Pol>(s0, s1, s2, s3, s4); \
                P = weno_pluss_clipped<Pol>(s1, s2, s3, s4, s5); } }
     MPCF_RECON(0,   S.rm,  S.rp);
@@ -353,7 +488,8 @@ __device__ __forceinline__ void face_flux(const typename Pol::T* __restrict__ sm
     MPCF_RECON(5,   S.Gm,  S.Gp);
     MPCF_RECON(6,   S.Pm,  S.Pp);
 #undef MPCF_RECON
-    hllc_face<Pol>(S, dir, o);
+    if constexpr (Pol::kFastWeno) hllc_face_packed(S, dir, o);
+    else                          hllc_face<Pol>(S, dir, o);
 }
 
 // Conserved (rho, rho u, rho v, rho w, E, G, P) -> primitives (rho, u, v, w,

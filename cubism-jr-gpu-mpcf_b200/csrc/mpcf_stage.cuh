@@ -452,12 +452,21 @@ stage_kernel(const StageArgs A)
                     }
                 }
             }
+            // R and U of cell k-1 are loaded before the barrier: their DRAM
+            // latency overlaps the wait for the other warps' faces
+            const bool fin = (k > z0) && valid;
+            const long long idx = (long long)gx + (long long)D.nx * ((long long)gy + (long long)D.ny * (k - 1));
+            T Rold[7], Uold[7];
+            if (fin)
+            {
+#pragma unroll
+                for (int m = 0; m < 7; ++m) { Rold[m] = R[m * D.fs + idx]; Uold[m] = __ldg(U + m * D.fs + idx); }
+            }
             __syncthreads();
 
             // (E) finalise cell k-1 of the own column
-            if (k > z0 && valid)
+            if (fin)
             {
-                const long long idx = (long long)gx + (long long)D.nx * ((long long)gy + (long long)D.ny * (k - 1));
                 const T sumG = sG + (zfp[8] + zf.Gm);
                 const T sumP = sP + (zfp[10] + zf.Pm);
                 const T divU = dU + (zf.vel - zfp[11]);
@@ -469,9 +478,9 @@ stage_kernel(const StageArgs A)
                     if (m == 5) br = br - divU * sumG * factor6;
                     if (m == 6) br = br - divU * sumP * factor6;
                     const T rhs_m = dtinvh * br;
-                    const T rhs = a * R[m * D.fs + idx] - rhs_m;
+                    const T rhs = a * Rold[m] - rhs_m;
                     R[m * D.fs + idx] = rhs;
-                    un[m] = b * rhs + __ldg(U + m * D.fs + idx);
+                    un[m] = b * rhs + Uold[m];
                     Un[m * D.fs + idx] = un[m];
                 }
                 ok = ok && physical<T>(un[0], un[4], un[5], un[6]);
