@@ -461,58 +461,87 @@ __device__ __forceinline__ void hllc_face_packed(const FaceState<float>& S, cons
 
 // Full face from primitives in shared memory: cell j (j = 0..5 for cells
 // i-3..i+2 around face i-1/2) of primitive plane q sits at
-// sm[base + q*pitch + offs[j]].  The velocity planes are permuted by `dir`
+// sm[addr[j] + q*PP].  PP, the plane pitch, is a compile-time constant, so
+// every plane's six loads share the six addresses (immediate offsets).  The
+// velocity planes are reconstructed in (u, v, w) order and permuted by `dir`
 // into (normal, first transverse, second transverse) as the reference
-// passes them to the HLLC functions.
-template <class Pol>
-__device__ __forceinline__ void face_flux(const typename Pol::T* __restrict__ sm, const int base, const int pitch,
-                                          const int (&offs)[6], const int dir, FaceOut<typename Pol::T>& o)
+// passes them to the HLLC functions (x: u,v,w; y: v,u,w; z: w,u,v).
+template <class Pol, int PP>
+__device__ __forceinline__ void face_flux(const typename Pol::T* __restrict__ sm, const int (&addr)[6],
+                                          const int dir, FaceOut<typename Pol::T>& o)
 {
     typedef typename Pol::T T;
     FaceState<T> S;
-    const int qn  = 1 + dir;
-    const int qt1 = dir == 0 ? 2 : 1;
-    const int qt2 = dir == 2 ? 2 : 3;
+    T m1, p1, m2, p2, m3, p3;
 #define MPCF_RECON(q, M, P) { \
-        const T* b_ = sm + base + (q) * pitch; \
-        const T s0 = b_[offs[0]], s1 = b_[offs[1]], s2 = b_[offs[2]], \
-                s3 = b_[offs[3]], s4 = b_[offs[4]], s5 = b_[offs[5]]; \
+        const T s0 = sm[addr[0] + (q) * PP], s1 = sm[addr[1] + (q) * PP], s2 = sm[addr[2] + (q) * PP], \
+                s3 = sm[addr[3] + (q) * PP], s4 = sm[addr[4] + (q) * PP], s5 = sm[addr[5] + (q) * PP]; \
         if constexpr (Pol::kFastWeno) weno_pair_packed(s0, s1, s2, s3, s4, s5, M, P); \
         else { M = weno_minus_clipped<Pol>(s0, s1, s2, s3, s4); \
                P = weno_pluss_clipped<Pol>(s1, s2, s3, s4, s5); } }
-    MPCF_RECON(0,   S.rm,  S.rp);
-    MPCF_RECON(qn,  S.nm,  S.np);
-    MPCF_RECON(qt1, S.t1m, S.t1p);
-    MPCF_RECON(qt2, S.t2m, S.t2p);
-    MPCF_RECON(4,   S.pm,  S.pp);
-    MPCF_RECON(5,   S.Gm,  S.Gp);
-    MPCF_RECON(6,   S.Pm,  S.Pp);
+    MPCF_RECON(0, S.rm, S.rp);
+    MPCF_RECON(1, m1, p1);
+    MPCF_RECON(2, m2, p2);
+    MPCF_RECON(3, m3, p3);
+    MPCF_RECON(4, S.pm, S.pp);
+    MPCF_RECON(5, S.Gm, S.Gp);
+    MPCF_RECON(6, S.Pm, S.Pp);
 #undef MPCF_RECON
+    S.nm  = dir == 0 ? m1 : (dir == 1 ? m2 : m3);
+    S.np  = dir == 0 ? p1 : (dir == 1 ? p2 : p3);
+    S.t1m = dir == 0 ? m2 : m1;
+    S.t1p = dir == 0 ? p2 : p1;
+    S.t2m = dir == 2 ? m2 : m3;
+    S.t2p = dir == 2 ? p2 : p3;
     if constexpr (Pol::kFastWeno) hllc_face_packed(S, dir, o);
     else                          hllc_face<Pol>(S, dir, o);
+}
+
+// Reciprocal in double precision without a division: the special-function
+// unit's approximate reciprocal refined by two Newton-Raphson steps
+// y <- y + y (1 - x y) (each step doubles the number of correct bits).
+__device__ __forceinline__ double rcp_f64(const double x)
+{
+    double y;
+    asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(y) : "d"(x));
+    double e = fma(-x, y, 1.0);
+    y = fma(y, e, y);
+    e = fma(-x, y, 1.0);
+    return fma(y, e, y);
 }
 
 // Conserved (rho, rho u, rho v, rho w, E, G, P) -> primitives (rho, u, v, w,
 // p, G, P).  Reference form (GPUkernels.cu:209-244):
 //   u = (rho u)/rho, ...;  p = (E - 0.5f*rho*(u*u + v*v + w*w) - P) / G
-// The mixed policy evaluates the pressure recovery in FP64 from the stored
-// conserved values: p = (E - 0.5*((rho u)^2+(rho v)^2+(rho w)^2)/rho - P)/G.
+// in the reference-rounding and FP64 policies.  The fast policies multiply
+// by reciprocals; the mixed policy evaluates the pressure recovery in FP64
+// from the stored conserved values:
+//   p = (E - 0.5*((rho u)^2+(rho v)^2+(rho w)^2)/rho - P)/G.
 template <class Pol>
 __device__ __forceinline__ void to_primitive(const typename Pol::T c[7], typename Pol::T q[7])
 {
     typedef typename Pol::T T;
     q[0] = c[0];
-    q[1] = c[1] / c[0];
-    q[2] = c[2] / c[0];
-    q[3] = c[3] / c[0];
-    if (Pol::kP64)
+    if constexpr (Pol::kFastWeno)
     {
-        const double r = (double)c[0];
-        const double ke = 0.5 * ((double)c[1]*(double)c[1] + (double)c[2]*(double)c[2] + (double)c[3]*(double)c[3]) / r;
-        q[4] = (T)(((double)c[4] - ke - (double)c[6]) / (double)c[5]);
+        const float ir = rcp_approx(c[0]);
+        q[1] = c[1] * ir;
+        q[2] = c[2] * ir;
+        q[3] = c[3] * ir;
+        if constexpr (Pol::kP64)
+        {
+            const double m2 = (double)c[1]*(double)c[1] + (double)c[2]*(double)c[2] + (double)c[3]*(double)c[3];
+            const double ke = 0.5 * m2 * rcp_f64((double)c[0]);
+            q[4] = (T)(((double)c[4] - ke - (double)c[6]) * rcp_f64((double)c[5]));
+        }
+        else
+            q[4] = (c[4] - 0.5f*c[0]*(q[1]*q[1] + q[2]*q[2] + q[3]*q[3]) - c[6]) * rcp_approx(c[5]);
     }
     else
     {
+        q[1] = c[1] / c[0];
+        q[2] = c[2] / c[0];
+        q[3] = c[3] / c[0];
         q[4] = (c[4] - (T)0.5f*c[0]*(q[1]*q[1] + q[2]*q[2] + q[3]*q[3]) - c[6]) / c[5];
     }
     q[5] = c[5];

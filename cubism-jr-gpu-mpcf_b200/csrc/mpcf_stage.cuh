@@ -52,12 +52,15 @@ constexpr int kTX = 32;
 
 __host__ __device__ constexpr size_t align_up(size_t v, size_t a) { return (v + a - 1) / a * a; }
 
-// Shared-memory layout of one CTA.  The T region is addressed in elements
-// (so every stencil, x, y or z, is base + q*pitch + offs[j]):
-//   zwin  [6 slots][7 planes][TY][32]     ring of the tile's own columns
-//   cur   [7 planes][TY+6][38]            slab k with 3-cell x/y halos
-//   fx    [12][TY][33]                    x faces of slab k
-//   fy    [12][TY+1][32]                  y faces of slab k
+// Shared-memory layout of one CTA.  The T region is addressed in elements.
+// Every primitive plane q (rho, u, v, w, p, G, P) has the same pitch kPP and
+// holds both stencil sources, so a stencil of any direction is
+// addr[j] + q*kPP with kPP a compile-time constant:
+//   plane q:  ring [6 slots][TY][32]      z-ring of the tile's own columns
+//             cur  [TY+6][38]             slab k with 3-cell x/y halos
+// Face results, 12 planes each, pitch kFP = (TY+1)*32:
+//   fx   [12][TY][33]                     x faces of slab k
+//   fy   [12][TY+1][32]                   y faces of slab k
 // then, in bytes: the FP64 reduction scratch [TY][5], the tile broadcast,
 // two mbarriers and, with TMA, the two staging buffers (128-byte aligned):
 //   A     [7][TY+6][40]                   halo box, x from x0-4, y from y0-3
@@ -65,17 +68,14 @@ __host__ __device__ constexpr size_t align_up(size_t v, size_t a) { return (v + 
 template <class T, int TY, bool TMA>
 struct StageLayout
 {
-    static constexpr int kCurW   = kTX + 6;
-    static constexpr int kZPlane = TY * kTX;               // zwin plane pitch
-    static constexpr int kZSlot  = 7 * kZPlane;            // zwin slot pitch
-    static constexpr int kCurP   = (TY + 6) * kCurW;       // cur plane pitch
-    static constexpr int kFxP    = TY * (kTX + 1);         // fx plane pitch
-    static constexpr int kFyP    = (TY + 1) * kTX;         // fy plane pitch
-    static constexpr int kZwin   = 0;
-    static constexpr int kCur    = kZwin + 6 * kZSlot;
-    static constexpr int kFx     = kCur + 7 * kCurP;
-    static constexpr int kFy     = kFx + 12 * kFxP;
-    static constexpr int kEnd    = kFy + 12 * kFyP;
+    static constexpr int kCurW   = kTX + 6;                // cur row width
+    static constexpr int kRing   = TY * kTX;               // one ring slot of a plane
+    static constexpr int kCurOff = 6 * kRing;              // cur inside a plane
+    static constexpr int kPP     = kCurOff + (TY + 6) * kCurW;
+    static constexpr int kFP     = (TY + 1) * kTX;         // >= TY * 33 for TY <= 32
+    static constexpr int kFx     = 7 * kPP;
+    static constexpr int kFy     = kFx + 12 * kFP;
+    static constexpr int kEnd    = kFy + 12 * kFP;
     static constexpr int kAW     = kTX + 8;                // staged halo box width
     static constexpr int kAH     = TY + 6;                 // staged halo box height
     static constexpr size_t kRedBytes  = align_up(kEnd * sizeof(T), 16);
@@ -87,6 +87,7 @@ struct StageLayout
     static constexpr size_t kStageB    = align_up(kStageA + kABytes, 128);
     // + 128: the kernel rounds the dynamic shared-memory base up to 128 B
     static constexpr size_t kBytes     = (TMA ? kStageB + kBBytes : kMbarBytes + 16) + 128;
+    static_assert(kFP >= TY * (kTX + 1), "x-face plane");
 };
 
 // Boundary-condition map of one coordinate: absorbing clamps to the edge
@@ -172,6 +173,12 @@ __device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity)
     for (int i = 0; i < (1 << 20); ++i)
         if (mbar_try_wait(bar, parity)) return true;
     return false;
+}
+
+// Prefetch the 128-byte line holding `p` into L1 (no register written).
+__device__ __forceinline__ void prefetch_l1(const void* p)
+{
+    asm volatile("prefetch.global.L1 [%0];" :: "l"(p));
 }
 
 // Generic-proxy accesses of this thread before async-proxy (bulk copy)
@@ -271,7 +278,12 @@ stage_kernel(const StageArgs A)
         const int z1 = min(z0 + A.dz, D.nz);
         const int gx = x0 + tx, gy = y0 + ty;
         const bool valid = (gx < D.nx) && (gy < D.ny);
-        const int own = ty * kTX + tx;     // own column inside a zwin plane
+        const int own = ty * kTX + tx;     // own column inside a ring slot
+        // the tile's columns are all inside the domain: its ring holds the
+        // exact primitives of every cur interior cell
+        const bool full = (x0 + kTX <= D.nx) && (y0 + TY <= D.ny);
+        // the staged halo box needs no boundary mapping in x and y
+        const bool inner = (x0 >= 4) && (x0 + kTX + 4 <= D.nx) && (y0 >= 3) && (y0 + TY + 3 <= D.ny);
 
         // ---- prologue: slabs z0-3 .. z0+1 of the own column into the ring
         for (int sl = z0 - 3; sl <= z0 + 1; ++sl)
@@ -280,7 +292,7 @@ stage_kernel(const StageArgs A)
             load_prim<Pol>(D, U, gx, gy, sl, q);
             const int slot = (sl + 6) % 6;
 #pragma unroll
-            for (int m = 0; m < 7; ++m) sm[L::kZwin + slot * L::kZSlot + m * L::kZPlane + own] = q[m];
+            for (int m = 0; m < 7; ++m) sm[m * L::kPP + slot * L::kRing + own] = q[m];
         }
         if (use_tma && threadIdx.x == 0)
         {
@@ -305,42 +317,43 @@ stage_kernel(const StageArgs A)
         for (int k = z0; k <= z1; ++k)
         {
             // (A) leading slab k+2 of the own column
-            if (use_tma)
             {
-                if (!tma_late && !mbar_wait(barB, phB)) tma_late = true;
-                phB ^= 1;
-                bool fx, fy, fz;
-                const int mx = min(max(bc_map(gx, D.nx, D.bc0, D.bc1, fx) - x0, 0), kTX - 1);
-                const int my = min(max(bc_map(gy, D.ny, D.bc2, D.bc3, fy) - y0, 0), TY - 1);
-                bc_map(k + 2, D.nz, D.bc4, D.bc5, fz);
-                T c[7], q[7];
-#pragma unroll
-                for (int m = 0; m < 7; ++m) c[m] = stB[(m * TY + my) * kTX + mx];
-                if (fx) c[1] = -c[1];
-                if (fy) c[2] = -c[2];
-                if (fz) c[3] = -c[3];
-                to_primitive<Pol>(c, q);
                 const int slot = (k + 2 + 6) % 6;
-#pragma unroll
-                for (int m = 0; m < 7; ++m) sm[L::kZwin + slot * L::kZSlot + m * L::kZPlane + own] = q[m];
-            }
-            else
-            {
                 T q[7];
-                load_prim<Pol>(D, U, gx, gy, k + 2, q);
-                const int slot = (k + 2 + 6) % 6;
-#pragma unroll
-                for (int m = 0; m < 7; ++m) sm[L::kZwin + slot * L::kZSlot + m * L::kZPlane + own] = q[m];
-            }
-            // (B) slab k with halos into cur
-            if (k < z1)
-            {
                 if (use_tma)
                 {
+                    if (!tma_late && !mbar_wait(barB, phB)) tma_late = true;
+                    phB ^= 1;
+                    bool fx = false, fy = false, fz;
+                    int mx = tx, my = ty;
+                    if (!full)
+                    {
+                        mx = min(max(bc_map(gx, D.nx, D.bc0, D.bc1, fx) - x0, 0), kTX - 1);
+                        my = min(max(bc_map(gy, D.ny, D.bc2, D.bc3, fy) - y0, 0), TY - 1);
+                    }
+                    bc_map(k + 2, D.nz, D.bc4, D.bc5, fz);
+                    T c[7];
+#pragma unroll
+                    for (int m = 0; m < 7; ++m) c[m] = stB[(m * TY + my) * kTX + mx];
+                    if (fx) c[1] = -c[1];
+                    if (fy) c[2] = -c[2];
+                    if (fz) c[3] = -c[3];
+                    to_primitive<Pol>(c, q);
+                }
+                else load_prim<Pol>(D, U, gx, gy, k + 2, q);
+#pragma unroll
+                for (int m = 0; m < 7; ++m) sm[m * L::kPP + slot * L::kRing + own] = q[m];
+            }
+            // (B) slab k with halos into cur (slab k < nz: no z mapping)
+            if (k < z1)
+            {
+                const int slot = k % 6;
+                if (use_tma && !full)
+                {
+                    // tile reaching past the domain: convert the whole staged
+                    // box, mapping out-of-domain cells to their sources
                     if (!tma_late && !mbar_wait(barA, phA)) tma_late = true;
                     phA ^= 1;
-                    bool fz;
-                    bc_map(k, D.nz, D.bc4, D.bc5, fz);
                     for (int i = threadIdx.x; i < (TY + 6) * L::kCurW; i += kTX * TY)
                     {
                         const int ly = i / L::kCurW - 3, lx = i % L::kCurW - 3;
@@ -352,18 +365,23 @@ stage_kernel(const StageArgs A)
                         for (int m = 0; m < 7; ++m) c[m] = stA[(m * L::kAH + my) * L::kAW + mx];
                         if (fx) c[1] = -c[1];
                         if (fy) c[2] = -c[2];
-                        if (fz) c[3] = -c[3];
                         to_primitive<Pol>(c, q);
 #pragma unroll
-                        for (int m = 0; m < 7; ++m) sm[L::kCur + m * L::kCurP + (ly + 3) * L::kCurW + lx + 3] = q[m];
+                        for (int m = 0; m < 7; ++m) sm[m * L::kPP + L::kCurOff + (ly + 3) * L::kCurW + lx + 3] = q[m];
                     }
                 }
                 else
                 {
-                    const int slot = (k + 6) % 6;
+                    // interior from the ring, then the 6*32 + 6*TY halo cells
+                    // the x/y stencils read (the corners are never read)
 #pragma unroll
                     for (int m = 0; m < 7; ++m)
-                        sm[L::kCur + m * L::kCurP + (ty + 3) * L::kCurW + tx + 3] = sm[L::kZwin + slot * L::kZSlot + m * L::kZPlane + own];
+                        sm[m * L::kPP + L::kCurOff + (ty + 3) * L::kCurW + tx + 3] = sm[m * L::kPP + slot * L::kRing + own];
+                    if (use_tma)
+                    {
+                        if (!tma_late && !mbar_wait(barA, phA)) tma_late = true;
+                        phA ^= 1;
+                    }
                     for (int i = threadIdx.x; i < 6 * kTX + 6 * TY; i += kTX * TY)
                     {
                         int lx, ly;
@@ -381,9 +399,25 @@ stage_kernel(const StageArgs A)
                             lx = c < 3 ? c - 3 : kTX + c - 3;
                         }
                         T q[7];
-                        load_prim<Pol>(D, U, x0 + lx, y0 + ly, k, q);
+                        if (use_tma)
+                        {
+                            bool fx = false, fy = false;
+                            int mx = lx + 4, my = ly + 3;
+                            if (!inner)
+                            {
+                                mx = min(max(bc_map(x0 + lx, D.nx, D.bc0, D.bc1, fx) - x0 + 4, 0), L::kAW - 1);
+                                my = min(max(bc_map(y0 + ly, D.ny, D.bc2, D.bc3, fy) - y0 + 3, 0), L::kAH - 1);
+                            }
+                            T c[7];
 #pragma unroll
-                        for (int m = 0; m < 7; ++m) sm[L::kCur + m * L::kCurP + (ly + 3) * L::kCurW + lx + 3] = q[m];
+                            for (int m = 0; m < 7; ++m) c[m] = stA[(m * L::kAH + my) * L::kAW + mx];
+                            if (fx) c[1] = -c[1];
+                            if (fy) c[2] = -c[2];
+                            to_primitive<Pol>(c, q);
+                        }
+                        else load_prim<Pol>(D, U, x0 + lx, y0 + ly, k, q);
+#pragma unroll
+                        for (int m = 0; m < 7; ++m) sm[m * L::kPP + L::kCurOff + (ly + 3) * L::kCurW + lx + 3] = q[m];
                     }
                 }
             }
@@ -410,63 +444,65 @@ stage_kernel(const StageArgs A)
             // in registers), job 1 = x face left of the own cell, job 2 = y face
             // below it, job 3 = warp 0: y face above the tile (row TY),
             // warp 1: x face right of the tile (column 32, one per row).
-            // One face instance serves every job (runtime direction/offsets).
+            // One face instance serves every job (runtime direction and
+            // stencil addresses).  R and U of cell k-1 are first prefetched
+            // into L1, so that the finalisation after the faces finds them.
+            const bool fin = (k > z0) && valid;
+            const long long idx = (long long)gx + (long long)D.nx * ((long long)gy + (long long)D.ny * (k - 1));
+            if (fin)
+            {
+#pragma unroll
+                for (int m = 0; m < 7; ++m) { prefetch_l1(R + m * D.fs + idx); prefetch_l1(U + m * D.fs + idx); }
+            }
             FaceOut<T> zf;
             {
                 const int njobs = (k < z1) ? ((ty == 0 || (ty == 1 && tx < TY)) ? 4 : 3) : 1;
+                const int zs0 = (k + 3) % 6;          // ring slot of slab k-3
 #pragma unroll 1
                 for (int job = 0; job < njobs; ++job)
                 {
-                    int base, pitch, dir, dst, dpitch;
-                    int offs[6];
+                    int addr[6];
+                    int dir, dst;
                     if (job == 0)
                     {
-                        dir = 2; base = L::kZwin + own; pitch = L::kZPlane; dst = -1; dpitch = 0;
-                        const int s0 = (k - 3 + 6) % 6;
+                        dir = 2; dst = -1;
 #pragma unroll
-                        for (int j = 0; j < 6; ++j) { const int sl = s0 + j; offs[j] = (sl >= 6 ? sl - 6 : sl) * L::kZSlot; }
+                        for (int j = 0; j < 6; ++j) { const int sl = zs0 + j; addr[j] = (sl >= 6 ? sl - 6 : sl) * L::kRing + own; }
                     }
                     else
                     {
                         const bool xdir = (job == 1) || (job == 3 && ty == 1);
                         dir = xdir ? 0 : 1;
-                        pitch = L::kCurP;
+                        int base;
+                        if (job == 1)      { base = (ty + 3) * L::kCurW + tx;  dst = L::kFx + ty * (kTX + 1) + tx; }
+                        else if (job == 2) { base = ty * L::kCurW + tx + 3;    dst = L::kFy + ty * kTX + tx; }
+                        else if (ty == 0)  { base = TY * L::kCurW + tx + 3;    dst = L::kFy + TY * kTX + tx; }
+                        else               { base = (tx + 3) * L::kCurW + kTX; dst = L::kFx + tx * (kTX + 1) + kTX; }
                         const int step = xdir ? 1 : L::kCurW;
 #pragma unroll
-                        for (int j = 0; j < 6; ++j) offs[j] = j * step;
-                        if (job == 1)      { base = L::kCur + (ty + 3) * L::kCurW + tx;  dst = L::kFx + ty * (kTX + 1) + tx; dpitch = L::kFxP; }
-                        else if (job == 2) { base = L::kCur + ty * L::kCurW + tx + 3;    dst = L::kFy + ty * kTX + tx;       dpitch = L::kFyP; }
-                        else if (ty == 0)  { base = L::kCur + TY * L::kCurW + tx + 3;    dst = L::kFy + TY * kTX + tx;       dpitch = L::kFyP; }
-                        else               { base = L::kCur + (tx + 3) * L::kCurW + kTX; dst = L::kFx + tx * (kTX + 1) + kTX; dpitch = L::kFxP; }
+                        for (int j = 0; j < 6; ++j) addr[j] = L::kCurOff + base + j * step;
                     }
                     FaceOut<T> o;
-                    face_flux<Pol>(sm, base, pitch, offs, dir, o);
+                    face_flux<Pol, L::kPP>(sm, addr, dir, o);
                     if (dst < 0) zf = o;
                     else
                     {
 #pragma unroll
-                        for (int m = 0; m < 7; ++m) sm[dst + m * dpitch] = o.f[m];
-                        sm[dst + 7 * dpitch] = o.Gm;  sm[dst + 8 * dpitch] = o.Gp;
-                        sm[dst + 9 * dpitch] = o.Pm;  sm[dst + 10 * dpitch] = o.Pp;
-                        sm[dst + 11 * dpitch] = o.vel;
+                        for (int m = 0; m < 7; ++m) sm[dst + m * L::kFP] = o.f[m];
+                        sm[dst + 7 * L::kFP] = o.Gm;  sm[dst + 8 * L::kFP] = o.Gp;
+                        sm[dst + 9 * L::kFP] = o.Pm;  sm[dst + 10 * L::kFP] = o.Pp;
+                        sm[dst + 11 * L::kFP] = o.vel;
                     }
                 }
             }
-            // R and U of cell k-1 are loaded before the barrier: their DRAM
-            // latency overlaps the wait for the other warps' faces
-            const bool fin = (k > z0) && valid;
-            const long long idx = (long long)gx + (long long)D.nx * ((long long)gy + (long long)D.ny * (k - 1));
-            T Rold[7], Uold[7];
+            // (E) finalise cell k-1 of the own column.  It reads only this
+            // thread's registers and global memory, so it runs before the
+            // barrier, while the warps with a fourth face finish it.
             if (fin)
             {
+                T Rold[7], Uold[7];
 #pragma unroll
                 for (int m = 0; m < 7; ++m) { Rold[m] = R[m * D.fs + idx]; Uold[m] = __ldg(U + m * D.fs + idx); }
-            }
-            __syncthreads();
-
-            // (E) finalise cell k-1 of the own column
-            if (fin)
-            {
                 const T sumG = sG + (zfp[8] + zf.Gm);
                 const T sumP = sP + (zfp[10] + zf.Pm);
                 const T divU = dU + (zf.vel - zfp[11]);
@@ -491,6 +527,8 @@ stage_kernel(const StageArgs A)
                 }
             }
 
+            __syncthreads();
+
             // (F) x/y part of cell k, carried to the next slab
             if (k < z1)
             {
@@ -498,13 +536,13 @@ stage_kernel(const StageArgs A)
                 const T* fy = sm + L::kFy + ty * kTX + tx;
 #pragma unroll
                 for (int m = 0; m < 7; ++m)
-                    Sp[m] = ((fx[m * L::kFxP + 1] - fx[m * L::kFxP]) + fy[m * L::kFyP + kTX]) - fy[m * L::kFyP];
-                sG = fx[8 * L::kFxP] + fx[7 * L::kFxP + 1];
-                sP = fx[10 * L::kFxP] + fx[9 * L::kFxP + 1];
-                dU = fx[11 * L::kFxP + 1] - fx[11 * L::kFxP];
-                sG = sG + (fy[8 * L::kFyP] + fy[7 * L::kFyP + kTX]);
-                sP = sP + (fy[10 * L::kFyP] + fy[9 * L::kFyP + kTX]);
-                dU = dU + (fy[11 * L::kFyP + kTX] - fy[11 * L::kFyP]);
+                    Sp[m] = ((fx[m * L::kFP + 1] - fx[m * L::kFP]) + fy[m * L::kFP + kTX]) - fy[m * L::kFP];
+                sG = fx[8 * L::kFP] + fx[7 * L::kFP + 1];
+                sP = fx[10 * L::kFP] + fx[9 * L::kFP + 1];
+                dU = fx[11 * L::kFP + 1] - fx[11 * L::kFP];
+                sG = sG + (fy[8 * L::kFP] + fy[7 * L::kFP + kTX]);
+                sP = sP + (fy[10 * L::kFP] + fy[9 * L::kFP + kTX]);
+                dU = dU + (fy[11 * L::kFP + kTX] - fy[11 * L::kFP]);
             }
 #pragma unroll
             for (int m = 0; m < 7; ++m) zfp[m] = zf.f[m];
