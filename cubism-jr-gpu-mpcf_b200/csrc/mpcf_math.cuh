@@ -214,27 +214,46 @@ __device__ __forceinline__ float2 rcp2(const float2 a) { return make_float2(rcp_
 // HLLC upwind blend w.x * F.x + w.y * F.y of a (left, right) flux pair
 __device__ __forceinline__ float blend2(const float2 w, const float2 F) { const float2 t = mul2(F, w); return t.x + t.y; }
 
+// Minimum / maximum of three values in one operation (sm_100).
+__device__ __forceinline__ float min3f(const float a, const float b, const float c)
+{
+    float r;
+    asm("min.f32 %0, %1, %2, %3;" : "=f"(r) : "f"(a), "f"(b), "f"(c));
+    return r;
+}
+__device__ __forceinline__ float max3f(const float a, const float b, const float c)
+{
+    float r;
+    asm("max.f32 %0, %1, %2, %3;" : "=f"(r) : "f"(a), "f"(b), "f"(c));
+    return r;
+}
+
 // Both reconstructions of one face (fast policies) as one packed pair.
 // The plus side is the mirror image of the minus side: with
 //   lane x (minus): (x0..x4) = (s0, s1, s2, s3, s4)
 //   lane y (plus):  (x0..x4) = (s5, s4, s3, s2, s1)
 // both lanes evaluate the same expressions (GPUonly.cuh:99-194):
-//   is0 = 13/12 (x0-2x1+x2)^2 + 1/4 (x0-4x1+3x2)^2
-//   is1 = 13/12 (x1-2x2+x3)^2 + 1/4 (x1-x3)^2
-//   is2 = 13/12 (x2-2x3+x4)^2 + 1/4 (3x2-4x3+x4)^2
+//   is0 = 13/12 k0^2 + 1/4 (x0-4x1+3x2)^2,  k0 = x0-2x1+x2
+//   is1 = 13/12 k1^2 + 1/4 (x1-x3)^2,       k1 = x1-2x2+x3
+//   is2 = 13/12 k2^2 + 1/4 (3x2-4x3+x4)^2,  k2 = x2-2x3+x4
 //   p0 = (2x0-7x1+11x2)/6, p1 = (-x1+5x2+2x3)/6, p2 = (2x2+5x3-x4)/6
-//   r  = (a0 p0 + 6 a1 p1 + 3 a2 p2) / (a0 + 6 a1 + 3 a2), a_k = 1/(is_k+eps)^2
+//   r  = (a0 p0 + a1 p1 + a2 p2) / (a0 + a1 + a2),  a_k = d_k/(is_k+eps)^2,
+//   d = (1, 6, 3)
 // with the smoothness indicators in the factored, cancellation-free form
 // (the same polynomials as the reference's expanded beta_f / beta_h /
-// beta_g, coefficient by coefficient), scaled by 12 (the scale cancels in
-// the ratio), and the ratio in difference form
-//   r = p2 + (a0 (p0-p2) + a1 * 6(p1-p2)) / (a0 + 6 a1 + 3 a2)
-// so no normalised weight is formed.  Each lane is then clipped to
-// [min, max] of its three central cells.
+// beta_g, coefficient by coefficient).  The candidate differences are the
+// curvature differences p0 - p1 = (k0-k1)/3 and p2 - p1 = (k1-k2)/6, so
+//   r = p1 + (b0 (k0-k1) + b2 (k1-k2)) / (3 b0 + b1 + 6 b2),
+//   b = (a0/3, a1, a2/6) = (1/3, 6, 1/2) / (is+eps)^2 up to a common factor,
+// and each b_k is the reciprocal square of i_k = c_k (13 k^2 + 3 a^2 +
+// 12 eps) with c = (sqrt 3, 1/sqrt 6, sqrt 2).  Each lane is then clipped
+// to [min, max] of its three central cells.
 __device__ __forceinline__ void weno_pair_packed(const float s0, const float s1, const float s2,
                                                  const float s3, const float s4, const float s5,
                                                  float& m, float& p)
 {
+    constexpr double e12 = 12.0 * MPCF_WENOEPS;
+    constexpr float c0 = 1.7320508075688772f, c1 = 0.40824829046386302f, c2 = 1.4142135623730951f;
     const float2 X = f2(s0, s5), Y = f2(s1, s4), Z = f2(s2, s3), W = f2(s3, s2), V = f2(s4, s1);
     const float2 k0 = fma2(Y, f2s(-2.f), add2(X, Z));
     const float2 k1 = fma2(Z, f2s(-2.f), add2(Y, W));
@@ -242,23 +261,19 @@ __device__ __forceinline__ void weno_pair_packed(const float s0, const float s1,
     const float2 a0 = fma2(Z, f2s(3.f), fma2(Y, f2s(-4.f), X));
     const float2 a1 = sub2(Y, W);
     const float2 a2 = fma2(Z, f2s(3.f), fma2(W, f2s(-4.f), V));
-    const float2 eps12 = f2s((float)(12.0 * MPCF_WENOEPS));
-    // 12 (is_k + eps) = 13 k^2 + 3 a^2 + 12 eps
-    const float2 i0 = fma2(mul2(k0, f2s(13.f)), k0, fma2(mul2(a0, f2s(3.f)), a0, eps12));
-    const float2 i1 = fma2(mul2(k1, f2s(13.f)), k1, fma2(mul2(a1, f2s(3.f)), a1, eps12));
-    const float2 i2 = fma2(mul2(k2, f2s(13.f)), k2, fma2(mul2(a2, f2s(3.f)), a2, eps12));
-    const float2 r0 = rcp2(mul2(i0, i0));
-    const float2 r1 = rcp2(mul2(i1, i1));
-    const float2 r2 = rcp2(mul2(i2, i2));
-    const float2 inv = rcp2(fma2(r2, f2s(3.f), fma2(r1, f2s(6.f), r0)));
-    const float2 p2 = fma2(V, f2s(-1.f / 6.f), fma2(W, f2s(5.f / 6.f), mul2(Z, f2s(1.f / 3.f))));
-    const float2 p0 = fma2(Z, f2s(11.f / 6.f), fma2(Y, f2s(-7.f / 6.f), mul2(X, f2s(1.f / 3.f))));
-    const float2 d1 = fma2(sub2(Z, W), f2s(3.f), sub2(V, Y));         // 6 (p1 - p2)
-    const float2 num = fma2(r1, d1, mul2(r0, sub2(p0, p2)));
-    const float2 r = fma2(num, inv, p2);
-    const float lo23 = fminf(s2, s3), hi23 = fmaxf(s2, s3);
-    m = fminf(fmaxf(r.x, fminf(s1, lo23)), fmaxf(s1, hi23));
-    p = fminf(fmaxf(r.y, fminf(s4, lo23)), fmaxf(s4, hi23));
+    const float2 i0 = fma2(mul2(k0, f2s(13.f * c0)), k0, fma2(mul2(a0, f2s(3.f * c0)), a0, f2s((float)(e12 * 1.7320508075688772))));
+    const float2 i1 = fma2(mul2(k1, f2s(13.f * c1)), k1, fma2(mul2(a1, f2s(3.f * c1)), a1, f2s((float)(e12 * 0.40824829046386302))));
+    const float2 i2 = fma2(mul2(k2, f2s(13.f * c2)), k2, fma2(mul2(a2, f2s(3.f * c2)), a2, f2s((float)(e12 * 1.4142135623730951))));
+    const float2 b0 = rcp2(mul2(i0, i0));
+    const float2 b1 = rcp2(mul2(i1, i1));
+    const float2 b2 = rcp2(mul2(i2, i2));
+    const float2 inv = rcp2(fma2(b2, f2s(6.f), fma2(b0, f2s(3.f), b1)));
+    const float2 num = fma2(b0, sub2(k0, k1), mul2(b2, sub2(k1, k2)));
+    // p1 = (x2 + x3)/2 - k1/6
+    const float2 p1 = fma2(k1, f2s(-1.f / 6.f), mul2(add2(Z, W), f2s(0.5f)));
+    const float2 r = fma2(num, inv, p1);
+    m = fminf(fmaxf(r.x, min3f(s1, s2, s3)), max3f(s1, s2, s3));
+    p = fminf(fmaxf(r.y, min3f(s2, s3, s4)), max3f(s2, s3, s4));
 }
 
 // ---------------------------------------------------------------------------
