@@ -137,23 +137,36 @@ cudaError_t launch_dt(int pol, const DtArgs& A, cudaStream_t st)
     return cudaGetLastError();
 }
 
-// Per-domain totals of the per-tile FP64 partial sums, in tile order
-// (deterministic, independent of scheduling).
-__global__ void sum_tiles_kernel(const DomDev* doms, const double* tile_sums, double* out)
+// Per-domain totals of the per-tile FP64 partial sums.  One block per
+// domain: thread i adds tiles i, i+256, ... in order, then a fixed-shape
+// tree combines the 256 partials, so the result does not depend on
+// scheduling (deterministic run to run).
+constexpr int kSumTilesThreads = 256;
+
+__global__ void __launch_bounds__(kSumTilesThreads) sum_tiles_kernel(const DomDev* doms, const double* tile_sums, double* out)
 {
+    __shared__ double red[5][kSumTilesThreads];
     const int d = blockIdx.x;
-    const int m = threadIdx.x;
-    if (m >= 5) return;
-    const int b = doms[d].tile_begin;
+    const int tid = threadIdx.x;
+    const long long b = doms[d].tile_begin;
     const int n = doms[d].tiles_x * doms[d].tiles_y * doms[d].tiles_z;
-    double s = 0;
-    for (int t = 0; t < n; ++t) s += tile_sums[(long long)(b + t) * 5 + m];
-    out[d * 5 + m] = s;
+    double s[5] = {0, 0, 0, 0, 0};
+    for (int t = tid; t < n; t += kSumTilesThreads)
+        for (int m = 0; m < 5; ++m) s[m] += tile_sums[(b + t) * 5 + m];
+    for (int m = 0; m < 5; ++m) red[m][tid] = s[m];
+    __syncthreads();
+    for (int w = kSumTilesThreads / 2; w > 0; w >>= 1)
+    {
+        if (tid < w)
+            for (int m = 0; m < 5; ++m) red[m][tid] += red[m][tid + w];
+        __syncthreads();
+    }
+    if (tid < 5) out[d * 5 + tid] = red[tid][0];
 }
 
 cudaError_t launch_sum_tiles(const DomDev* doms, int ndom, const double* tile_sums, double* out, cudaStream_t st)
 {
-    sum_tiles_kernel<<<ndom, 32, 0, st>>>(doms, tile_sums, out);
+    sum_tiles_kernel<<<ndom, kSumTilesThreads, 0, st>>>(doms, tile_sums, out);
     return cudaGetLastError();
 }
 
