@@ -41,6 +41,11 @@ WORKLOAD = "c3_512"
 METRIC = "cell-stage updates/s on 1 B200: mixed vs plain FP64 at stated L1 error"
 UNIT = "cell-stage updates/s"
 BYTES_PER_CELL_STAGE = {"fp32_ref": 112, "fp32": 112, "mixed": 112, "fp64": 224}
+# DRAM bytes per cell-stage of the mixed stage kernel measured by ncu
+# (dram__bytes_read.sum + dram__bytes_write.sum = 1.863 GB for one launch
+# over the 256^3 cloud, 16.78 M cells).  Traffic grows in proportion to the
+# cells, so the per-launch figure of a larger workload is this times its cells.
+MEASURED_DRAM_BYTES_PER_CELL_STAGE = {"mixed": 1.863e9 / 256 ** 3}
 
 
 # Algorithmic floating-point operations of one cell-stage, counted by
@@ -351,7 +356,10 @@ def main():
                                    "energy": float((sums1[:, 4].sum() - sums0[:, 4].sum()) / sums0[:, 4].sum()),
                                    "note": "FP64 sums over W+K steps, absorbing boundaries (boundary fluxes included)"},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
-                         "frac": achieved / hbm, "traffic": None,
+                         "frac": achieved / hbm,
+                         "traffic": (MEASURED_DRAM_BYTES_PER_CELL_STAGE[args.precision] * ncell
+                                     if args.precision in MEASURED_DRAM_BYTES_PER_CELL_STAGE else None),
+                         "traffic_note": "ncu DRAM bytes of one 256^3 launch scaled by cells",
                          "kernel": "stage_kernel<Pol%s>" % {"mixed": "Mixed", "fp32": "Fast32", "fp32_ref": "Ref32", "fp64": "FP64"}[args.precision],
                          "ms_per_launch": st_ms,
                          "algorithmic_bytes_per_launch": bytes_launch, "peak_kind": peak_kind,
