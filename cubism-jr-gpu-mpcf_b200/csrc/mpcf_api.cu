@@ -102,7 +102,7 @@ struct mpcf_solver
     void* tmaps = nullptr;          // ndom * 4 CUtensorMap (128 B each)
 
     // launch configuration
-    int ty = 4, dz = 64, persist = 0, tma = 0;
+    int ty = 7, dz = 64, persist = 0, tma = 0;
     int ntiles = 0;
     int sos_chunk = 32768, nchunks = 0;
     bool track_cons = false;
@@ -116,10 +116,13 @@ struct mpcf_solver
 
 namespace {
 
+// Tile heights with stage-kernel instances: 3 and 7 rows (CTAs of 4 and 8
+// warps: one warp per row plus the helper warp), and 15 rows (16 warps) for
+// the FP32 reference-rounding form.
 bool valid_ty(const mpcf_solver* s, int ty)
 {
-    if (ty == 4 || ty == 8) return true;
-    return ty == 16 && s->pol == 0;
+    if (ty == 3 || ty == 7) return true;
+    return ty == 15 && s->pol == 0;
 }
 
 StageKernelInfo stage_info(const mpcf_solver* s, int ty, bool persist, bool sums, bool tma)
@@ -264,7 +267,7 @@ int persistent_grid(mpcf_solver* s, int ty)
 {
     StageKernelInfo I = stage_info(s, ty, true, false, s->tma != 0);
     int nb = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, I.fn, 32 * ty, I.smem) != cudaSuccess || nb < 1)
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, I.fn, 32 * (ty + 1), I.smem) != cudaSuccess || nb < 1)
     {
         cudaGetLastError();
         nb = 1;
@@ -466,7 +469,7 @@ int mpcf_create(mpcf_solver** out, int ndomains, const int* dims, const int* bc,
     { cudaGetLastError(); return bail(fail(MPCF_ERR_NOMEM, "cudaMallocHost failed")); }
 
     // allow the large shared-memory footprints of every tiling variant
-    const int tys[3] = {4, 8, 16};
+    const int tys[3] = {3, 7, 15};
     for (int i = 0; i < 3; ++i)
     {
         if (!valid_ty(s, tys[i])) continue;
@@ -478,7 +481,7 @@ int mpcf_create(mpcf_solver** out, int ndomains, const int* dims, const int* bc,
             { cudaGetLastError(); return bail(fail(MPCF_ERR_CUDA, "cannot grant %zu B shared memory to the stage kernel (ty=%d)", I.smem, tys[i])); }
         }
     }
-    s->ty = 8;
+    s->ty = 7;
     s->dz = 64;
     s->persist = 0;
     s->tma = 1;                       // dropped by apply_tiling when no domain qualifies
@@ -851,7 +854,7 @@ int mpcf_launch_shape(const mpcf_solver* s, long long* ntiles, long long* grid, 
     if (!s) return fail(MPCF_ERR_ARG, "null solver");
     if (ntiles) *ntiles = s->ntiles;
     if (grid) *grid = s->persist ? persistent_grid(const_cast<mpcf_solver*>(s), s->ty) : s->ntiles;
-    if (threads) *threads = 32 * s->ty;
+    if (threads) *threads = 32 * (s->ty + 1);
     return MPCF_OK;
 }
 
@@ -916,7 +919,7 @@ int mpcf_autotune(mpcf_solver* s, int reps, int* best3, double* best_ms)
         std::vector<int> dzs;
         for (int v : {16, 32, 64, 128}) if (v < maxn) dzs.push_back(v);
         dzs.push_back(maxn);
-        const int tys[3] = {4, 8, 16};
+        const int tys[3] = {3, 7, 15};
         for (int i = 0; i < 3 && !rc; ++i)
         {
             if (!valid_ty(s, tys[i])) continue;

@@ -11,14 +11,16 @@
 // PCIe streaming (GPUlab.cpp:202-372,703-793); all state stays in HBM.
 //
 // Work decomposition.  A tile is 32 x TY columns in x-y and a z-chunk of
-// depth dz.  A CTA has 32*TY threads, one per column; warp w owns row w.
-// The CTA marches up the chunk one slab at a time:
+// depth dz.  A CTA has 32*(TY+1) threads: warp w < TY owns row w, one
+// thread per column, and warp TY (the helper) owns no column.  The CTA
+// marches up the chunk one slab at a time:
 //   * a 6-slab ring of primitives (rho,u,v,w,p,G,P) of the tile's own
 //     columns lives in shared memory (z-stencil of the z faces);
 //   * slab k with its 3-cell x/y halo is staged in `cur` (x/y stencils);
-//   * every thread evaluates the x face at its left, the y face below it
-//     and the z face below it; warp 0 adds the y faces of the row above the
-//     tile, warp 1 the x faces right of the tile (32 + TY extra faces);
+//   * every column thread evaluates the x face at its left, the y face below
+//     it and the z face below it; the helper evaluates the 32 y faces above
+//     the tile and the TY x faces right of it, so no warp runs more than
+//     three faces per slab and none waits on a fourth at the barrier;
 //   * x/y face results go through shared memory, the z face result stays
 //     in registers for the next slab, and the cell below is finalised:
 //     rhs = a*R - dtinvh*div(F) (with the G/P extra terms), R <- rhs,
@@ -206,11 +208,14 @@ __device__ __forceinline__ void tma_load_4d(uint32_t dst, const void* tmap, int 
 template <class T, int TY> struct MinBlocks
 {
     static constexpr int w = sizeof(T) == 8 ? MPCF_MIN_WARPS_PER_SM / 2 : MPCF_MIN_WARPS_PER_SM;
-    static constexpr int v = (w / TY) > 0 ? (w / TY) : 1;
+    static constexpr int v = (w / (TY + 1)) > 0 ? (w / (TY + 1)) : 1;
 };
 
+// Threads of one CTA: TY column warps and the helper warp.
+template <int TY> __host__ __device__ constexpr int stage_threads() { return kTX * (TY + 1); }
+
 template <class Pol, int TY, bool PERSIST, bool SUMS, bool TMA>
-__global__ void __launch_bounds__(kTX * TY, MinBlocks<typename Pol::T, TY>::v)
+__global__ void __launch_bounds__(stage_threads<TY>(), MinBlocks<typename Pol::T, TY>::v)
 stage_kernel(const StageArgs A)
 {
     typedef typename Pol::T T;
@@ -277,7 +282,8 @@ stage_kernel(const StageArgs A)
         const int z0 = bz * A.dz;
         const int z1 = min(z0 + A.dz, D.nz);
         const int gx = x0 + tx, gy = y0 + ty;
-        const bool valid = (gx < D.nx) && (gy < D.ny);
+        const bool row = ty < TY;          // a column thread (not the helper)
+        const bool valid = row && (gx < D.nx) && (gy < D.ny);
         const int own = ty * kTX + tx;     // own column inside a ring slot
         // the tile's columns are all inside the domain: its ring holds the
         // exact primitives of every cur interior cell
@@ -286,7 +292,7 @@ stage_kernel(const StageArgs A)
         const bool inner = (x0 >= 4) && (x0 + kTX + 4 <= D.nx) && (y0 >= 3) && (y0 + TY + 3 <= D.ny);
 
         // ---- prologue: slabs z0-3 .. z0+1 of the own column into the ring
-        for (int sl = z0 - 3; sl <= z0 + 1; ++sl)
+        for (int sl = z0 - 3; row && sl <= z0 + 1; ++sl)
         {
             T q[7];
             load_prim<Pol>(D, U, gx, gy, sl, q);
@@ -317,6 +323,7 @@ stage_kernel(const StageArgs A)
         for (int k = z0; k <= z1; ++k)
         {
             // (A) leading slab k+2 of the own column
+            if (row)
             {
                 const int slot = (k + 2 + 6) % 6;
                 T q[7];
@@ -354,7 +361,7 @@ stage_kernel(const StageArgs A)
                     // box, mapping out-of-domain cells to their sources
                     if (!tma_late && !mbar_wait(barA, phA)) tma_late = true;
                     phA ^= 1;
-                    for (int i = threadIdx.x; i < (TY + 6) * L::kCurW; i += kTX * TY)
+                    for (int i = threadIdx.x; i < (TY + 6) * L::kCurW; i += stage_threads<TY>())
                     {
                         const int ly = i / L::kCurW - 3, lx = i % L::kCurW - 3;
                         bool fx, fy;
@@ -374,15 +381,18 @@ stage_kernel(const StageArgs A)
                 {
                     // interior from the ring, then the 6*32 + 6*TY halo cells
                     // the x/y stencils read (the corners are never read)
+                    if (row)
+                    {
 #pragma unroll
-                    for (int m = 0; m < 7; ++m)
-                        sm[m * L::kPP + L::kCurOff + (ty + 3) * L::kCurW + tx + 3] = sm[m * L::kPP + slot * L::kRing + own];
+                        for (int m = 0; m < 7; ++m)
+                            sm[m * L::kPP + L::kCurOff + (ty + 3) * L::kCurW + tx + 3] = sm[m * L::kPP + slot * L::kRing + own];
+                    }
                     if (use_tma)
                     {
                         if (!tma_late && !mbar_wait(barA, phA)) tma_late = true;
                         phA ^= 1;
                     }
-                    for (int i = threadIdx.x; i < 6 * kTX + 6 * TY; i += kTX * TY)
+                    for (int i = threadIdx.x; i < 6 * kTX + 6 * TY; i += stage_threads<TY>())
                     {
                         int lx, ly;
                         if (i < 6 * kTX)
@@ -440,10 +450,11 @@ stage_kernel(const StageArgs A)
                 }
             }
 
-            // (C) faces of slab k: job 0 = z face k-1/2 of the own column (kept
-            // in registers), job 1 = x face left of the own cell, job 2 = y face
-            // below it, job 3 = warp 0: y face above the tile (row TY),
-            // warp 1: x face right of the tile (column 32, one per row).
+            // (C) faces of slab k.  Column warps: job 0 = z face k-1/2 of the
+            // own column (kept in registers), job 1 = x face left of the own
+            // cell, job 2 = y face below it.  Helper warp: job 3 = y face above
+            // the tile (row TY, lane = column), job 4 = x face right of the
+            // tile (column 32, lane = row, lanes < TY).
             // One face instance serves every job (runtime direction and
             // stencil addresses).  R and U of cell k-1 are first prefetched
             // into L1, so that the finalisation after the faces finds them.
@@ -456,10 +467,11 @@ stage_kernel(const StageArgs A)
             }
             FaceOut<T> zf;
             {
-                const int njobs = (k < z1) ? ((ty == 0 || (ty == 1 && tx < TY)) ? 4 : 3) : 1;
+                const int jb = row ? 0 : 3;
+                const int je = row ? ((k < z1) ? 3 : 1) : ((k < z1) ? (tx < TY ? 5 : 4) : 3);
                 const int zs0 = (k + 3) % 6;          // ring slot of slab k-3
 #pragma unroll 1
-                for (int job = 0; job < njobs; ++job)
+                for (int job = jb; job < je; ++job)
                 {
                     int addr[6];
                     int dir, dst;
@@ -471,12 +483,12 @@ stage_kernel(const StageArgs A)
                     }
                     else
                     {
-                        const bool xdir = (job == 1) || (job == 3 && ty == 1);
+                        const bool xdir = (job == 1) || (job == 4);
                         dir = xdir ? 0 : 1;
                         int base;
                         if (job == 1)      { base = (ty + 3) * L::kCurW + tx;  dst = L::kFx + ty * (kTX + 1) + tx; }
                         else if (job == 2) { base = ty * L::kCurW + tx + 3;    dst = L::kFy + ty * kTX + tx; }
-                        else if (ty == 0)  { base = TY * L::kCurW + tx + 3;    dst = L::kFy + TY * kTX + tx; }
+                        else if (job == 3) { base = TY * L::kCurW + tx + 3;    dst = L::kFy + TY * kTX + tx; }
                         else               { base = (tx + 3) * L::kCurW + kTX; dst = L::kFx + tx * (kTX + 1) + kTX; }
                         const int step = xdir ? 1 : L::kCurW;
 #pragma unroll
@@ -530,7 +542,7 @@ stage_kernel(const StageArgs A)
             __syncthreads();
 
             // (F) x/y part of cell k, carried to the next slab
-            if (k < z1)
+            if (k < z1 && row)
             {
                 const T* fx = sm + L::kFx + ty * (kTX + 1) + tx;
                 const T* fy = sm + L::kFy + ty * kTX + tx;
@@ -558,7 +570,7 @@ stage_kernel(const StageArgs A)
                 double v = cs[m];
 #pragma unroll
                 for (int off = 16; off > 0; off >>= 1) v += __shfl_xor_sync(0xffffffffu, v, off);
-                if (tx == 0) red[ty * 5 + m] = v;
+                if (tx == 0 && row) red[ty * 5 + m] = v;
             }
             __syncthreads();
             if (threadIdx.x < 5)

@@ -8,7 +8,7 @@
 
 namespace mpcf {
 
-template <class Pol, bool kWithTY16>
+template <class Pol, bool kWithTY15>
 struct StageDispatch
 {
     typedef typename Pol::T T;
@@ -16,7 +16,7 @@ struct StageDispatch
     template <int TY, bool P, bool S, bool M>
     static cudaError_t go(const StageArgs& A, int grid, cudaStream_t st)
     {
-        stage_kernel<Pol, TY, P, S, M><<<grid, kTX * TY, stage_smem_bytes<T, TY, M>(), st>>>(A);
+        stage_kernel<Pol, TY, P, S, M><<<grid, stage_threads<TY>(), stage_smem_bytes<T, TY, M>(), st>>>(A);
         return cudaGetLastError();
     }
 
@@ -42,12 +42,12 @@ struct StageDispatch
     {
         switch (ty)
         {
-            case 4: return tma ? go_ty<4, true>(persist, A, grid, st) : go_ty<4, false>(persist, A, grid, st);
-            case 8: return tma ? go_ty<8, true>(persist, A, grid, st) : go_ty<8, false>(persist, A, grid, st);
-            case 16:
-                if (kWithTY16)
-                    return tma ? go_ty<kWithTY16 ? 16 : 8, true>(persist, A, grid, st)
-                               : go_ty<kWithTY16 ? 16 : 8, false>(persist, A, grid, st);
+            case 3: return tma ? go_ty<3, true>(persist, A, grid, st) : go_ty<3, false>(persist, A, grid, st);
+            case 7: return tma ? go_ty<7, true>(persist, A, grid, st) : go_ty<7, false>(persist, A, grid, st);
+            case 15:
+                if (kWithTY15)
+                    return tma ? go_ty<kWithTY15 ? 15 : 7, true>(persist, A, grid, st)
+                               : go_ty<kWithTY15 ? 15 : 7, false>(persist, A, grid, st);
                 return cudaErrorInvalidValue;
             default: return cudaErrorInvalidValue;
         }
@@ -57,11 +57,11 @@ struct StageDispatch
     {
         switch (ty)
         {
-            case 4: return tma ? info_ty<4, true>(persist, sums) : info_ty<4, false>(persist, sums);
-            case 8: return tma ? info_ty<8, true>(persist, sums) : info_ty<8, false>(persist, sums);
-            case 16:
-                if (kWithTY16)
-                    return tma ? info_ty<kWithTY16 ? 16 : 8, true>(persist, sums) : info_ty<kWithTY16 ? 16 : 8, false>(persist, sums);
+            case 3: return tma ? info_ty<3, true>(persist, sums) : info_ty<3, false>(persist, sums);
+            case 7: return tma ? info_ty<7, true>(persist, sums) : info_ty<7, false>(persist, sums);
+            case 15:
+                if (kWithTY15)
+                    return tma ? info_ty<kWithTY15 ? 15 : 7, true>(persist, sums) : info_ty<kWithTY15 ? 15 : 7, false>(persist, sums);
                 { StageKernelInfo I = {nullptr, 0}; return I; }
             default: { StageKernelInfo I = {nullptr, 0}; return I; }
         }

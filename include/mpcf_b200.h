@@ -191,7 +191,8 @@ int mpcf_bubbles(unsigned long long seed, int n, double rmin, double rmax,
                  const double* lo3, const double* hi3, double gap, int max_tries, double* out4);
 
 /* ---- launch configuration ------------------------------------------------- *
- * tile = 32 x ty columns x dz slabs (ty 4 or 8; 16 for MPCF_PREC_FP32_REF);
+ * tile = 32 x ty columns x dz slabs (ty 3 or 7; 15 for MPCF_PREC_FP32_REF),
+ * one CTA of 32*(ty+1) threads per tile;
  * flags = MPCF_TILE_PERSISTENT | MPCF_TILE_TMA.  With MPCF_TILE_TMA, domains
  * whose rows are multiples of 16 bytes stage their slabs with bulk tensor
  * copies (other domains keep ordinary loads).  mpcf_autotune times the

@@ -111,7 +111,7 @@ def test_ensemble_equals_separate_solvers(mpcf):
     cfg = mpcf.configs.config("c4_ensemble")
     dims = cfg["dims"]
     with mpcf.Solver(dims, precision="fp32_ref") as s:
-        s.set_tiling(4, 32, True)
+        s.set_tiling(3, 32, True)
         for d, bub in enumerate(cfg["bubbles"]):
             s.ic_cloud(cfg["params"], bub, dom=d)
         t_ens = s.run(3, cfl=0.3, graph=True)
