@@ -773,6 +773,73 @@ int mpcf_ic_cloud(mpcf_solver* s, int dom, const mpcf_ic_params* p, int nbubbles
     return MPCF_OK;
 }
 
+void mpcf_sic_default_params(mpcf_sic_params* p)
+{
+    if (!p) return;
+    *p = mpcf_sic_params();
+    p->rho0 = 1000; p->u0 = 0; p->p0 = 1;
+    p->rhoB = 1; p->uB = 0; p->pB = 0.0234;
+    p->pressure_ratio = 40;
+    p->shock_n[0] = 1; p->shock_n[1] = 0; p->shock_n[2] = 0;
+    p->shock_s[0] = 0.05; p->shock_s[1] = 0; p->shock_s[2] = 0;
+    p->g1 = 6.59; p->g2 = 1.4; p->pc1 = 4096.0; p->pc2 = 1.0;
+    p->eps = 0;
+}
+
+static int sic_check(const mpcf_sic_params* p)
+{
+    if (!p) return fail(MPCF_ERR_ARG, "null SIC parameters");
+    const double mag2 = p->shock_n[0] * p->shock_n[0] + p->shock_n[1] * p->shock_n[1] + p->shock_n[2] * p->shock_n[2];
+    if (!(mag2 > 0)) return fail(MPCF_ERR_ARG, "shock normal must be non-zero");
+    if (!(p->g1 > 1) || !(p->g2 > 1)) return fail(MPCF_ERR_ARG, "gamma must exceed 1");
+    if (!(p->rho0 > 0) || !(p->rhoB > 0)) return fail(MPCF_ERR_ARG, "densities must be positive");
+    if (!(p->eps >= 0)) return fail(MPCF_ERR_ARG, "eps must be >= 0");
+    return MPCF_OK;
+}
+
+int mpcf_sic_post_shock(const mpcf_sic_params* p, int precision, double* post4)
+{
+    int rc = sic_check(p);
+    if (rc) return rc;
+    if (!post4 || precision < 0 || precision > 3) return fail(MPCF_ERR_ARG, "bad arguments");
+    SicParams P;
+    static_assert(sizeof(SicParams) == sizeof(mpcf_sic_params), "SIC parameter layout");
+    memcpy(&P, p, sizeof(P));
+    sic_post_shock(precision == MPCF_PREC_FP64, P, post4);
+    return MPCF_OK;
+}
+
+int mpcf_ic_sic_cloud(mpcf_solver* s, int dom, const mpcf_sic_params* p, int nshapes, const double* shapes4)
+{
+    int rc = check_dom(s, dom);
+    if (rc) return rc;
+    if ((rc = sic_check(p))) return rc;
+    if (nshapes < 0 || (nshapes > 0 && !shapes4)) return fail(MPCF_ERR_ARG, "bad shape arguments");
+    for (int i = 0; i < nshapes; ++i)
+        if (!(shapes4[4 * i + 3] > 0)) return fail(MPCF_ERR_ARG, "shape %d has a non-positive radius", i);
+    DeviceGuard g(s->device);
+    if (nshapes > s->bubbles_cap)
+    {
+        if (s->bubbles)
+        {
+            CK(cudaStreamSynchronize(s->stream));
+            cudaFree(s->bubbles);
+            s->allocs.erase(std::remove(s->allocs.begin(), s->allocs.end(), (void*)s->bubbles), s->allocs.end());
+            s->bubbles = nullptr;
+        }
+        if ((rc = dev_alloc(s, (void**)&s->bubbles, sizeof(double) * 4 * (size_t)nshapes))) return rc;
+        s->bubbles_cap = nshapes;
+    }
+    if (nshapes > 0) CK(cudaMemcpyAsync(s->bubbles, shapes4, sizeof(double) * 4 * nshapes, cudaMemcpyHostToDevice, s->stream));
+    SicParams P;
+    memcpy(&P, p, sizeof(P));
+    const DomDev& D = s->hdoms[dom];
+    CK(launch_sic_cloud(s->esz == 8, s->ddoms + dom, D.nx, D.ny, D.nz, s->parity, P, s->bubbles, nshapes, s->stream));
+    s->sums_valid = false;
+    CK(cudaStreamSynchronize(s->stream));
+    return MPCF_OK;
+}
+
 int mpcf_ic_cloud_host(int nx, int ny, int nz, const mpcf_ic_params* p, int nbubbles,
                        const double* bubbles4, int elem_size, void* const* out7)
 {

@@ -3,6 +3,7 @@
 // bubble-cloud initial condition and an explicit ghost-buffer fill.
 #include <cuda_runtime.h>
 #include <math.h>
+#include <cmath>
 #include <mutex>
 #include "mpcf_math.cuh"
 #include "mpcf_stage.cuh"
@@ -199,6 +200,214 @@ cudaError_t launch_ic_cloud(int is_double, const DomDev* dom, int parity, const 
 {
     if (is_double) ic_cloud_kernel<double><<<148 * 16, 256, 0, st>>>(dom, parity, P, bubbles, nbubbles);
     else           ic_cloud_kernel<float><<<148 * 16, 256, 0, st>>>(dom, parity, P, bubbles, nbubbles);
+    return cudaGetLastError();
+}
+
+// ---------------------------------------------------------------------------
+// Shock-induced cloud-collapse initial condition: the reference's
+// Sim_SICCloudMPI case (Sim_SICCloudMPI.cpp:43-357, Sim_SICCloudMPI.h:27-301).
+// A planar shock (Johnsen's post-shock state) ahead of a cloud of spheres;
+// every cell holds the 3x3x3 Simpson average of the sampled mixture.  The
+// arithmetic follows the reference's types: Real is the state's type, and
+// the sub-expressions its double literals promote are evaluated in double
+// (this translation unit contracts no multiply-adds, so the FP32 fields are
+// bit-identical to the reference built with _FLOAT_PRECISION_).
+// ---------------------------------------------------------------------------
+template <class Real>
+struct SicState
+{
+    Real rho0, u0, p0, rhoB, uB, pB, psi;
+    Real n[3], S[3];
+    Real g1, g2, pc1, pc2;
+    Real rho1, u1, p1, mach;
+};
+
+// Host: parameters to Real, shock normal normalised, post-shock state
+// (Sim_SICCloudMPI.cpp:76-103; pow(Real, int) promotes to double).
+template <class Real>
+SicState<Real> sic_setup(const SicParams& P)
+{
+    SicState<Real> st;
+    st.rho0 = (Real)P.rho0; st.u0 = (Real)P.u0; st.p0 = (Real)P.p0;
+    st.rhoB = (Real)P.rhoB; st.uB = (Real)P.uB; st.pB = (Real)P.pB;
+    st.psi = (Real)P.pressure_ratio;
+    for (int i = 0; i < 3; ++i) { st.n[i] = (Real)P.shock_n[i]; st.S[i] = (Real)P.shock_s[i]; }
+    st.g1 = (Real)P.g1; st.g2 = (Real)P.g2; st.pc1 = (Real)P.pc1; st.pc2 = (Real)P.pc2;
+    const Real mag = (Real)std::sqrt((double)st.n[0] * (double)st.n[0] + (double)st.n[1] * (double)st.n[1]
+                                     + (double)st.n[2] * (double)st.n[2]);
+    for (int i = 0; i < 3; ++i) st.n[i] /= mag;
+    const Real gamma = st.g1, pc = st.pc1, p0 = st.p0, rho0 = st.rho0, u0 = st.u0, psi = st.psi;
+    const Real p1   = p0 * psi;
+    const Real tmp1 = (Real)(((double)gamma + 1.0) / ((double)gamma - 1.0));
+    const Real tmp2 = (p1 + pc) / (p0 + pc);
+    const Real c0   = std::sqrt(gamma * (p0 + pc) / rho0);           // sqrt of Real
+    const Real mach = (Real)std::sqrt(((double)gamma + 1.0) / (2.0 * (double)gamma) * ((double)psi - 1.0) * (double)p0
+                                      / (double)(p0 + pc) + 1.0);
+    st.mach = mach;
+    st.u1   = (Real)((double)u0 + (double)c0 * ((double)psi - 1.0) * (double)p0 / (double)(gamma * (p0 + pc) * mach));
+    st.rho1 = (Real)((double)rho0 * ((double)(tmp1 * tmp2) + 1.0) / (double)(tmp1 + tmp2));
+    st.p1   = p1;
+    return st;
+}
+
+void sic_post_shock(int is_double, const SicParams& P, double post4[4])
+{
+    if (is_double)
+    {
+        const SicState<double> st = sic_setup<double>(P);
+        post4[0] = st.rho1; post4[1] = st.u1; post4[2] = st.p1; post4[3] = st.mach;
+    }
+    else
+    {
+        const SicState<float> st = sic_setup<float>(P);
+        post4[0] = st.rho1; post4[1] = st.u1; post4[2] = st.p1; post4[3] = st.mach;
+    }
+}
+
+// |pos - c| - r: differences in Real, squares and sum in double
+// (Sim_SICCloudMPI.h:97-101)
+template <class Real>
+__device__ __forceinline__ Real sic_shape_eval(const Real* shp, const Real pos[3])
+{
+    const double dx = (double)(pos[0] - shp[0]), dy = (double)(pos[1] - shp[1]), dz = (double)(pos[2] - shp[2]);
+    return (Real)(sqrt(dx * dx + dy * dy + dz * dz) - (double)shp[3]);
+}
+
+// Cloud indicator: cosine ramp of half-width eps around the nearest sphere
+// surface; eps = 0 gives 1 inside or on a sphere, 0 outside
+// (Sim_SICCloudMPI.h:285-301, min/max with the comparisons of std::min/max).
+template <class Real>
+__device__ __forceinline__ Real sic_indicator(const Real* shp, int n, const Real pos[3], double eps)
+{
+    Real d = (Real)HUGE_VAL;
+    for (int i = 0; i < n; ++i)
+    {
+        const Real nd = sic_shape_eval<Real>(shp + 4 * i, pos);
+        d = (nd < d) ? nd : d;
+    }
+    const double x  = ((double)d + eps) / (2 * eps);
+    const double mx = (0. < x) ? x : 0.;
+    const double mn = (mx < 1.) ? mx : 1.;
+    return (Real)(0.5 + 0.5 * cos(3.14159265358979323846 * mn));
+}
+
+// Mixture of one sample (Sim_SICCloudMPI.cpp:247-276)
+template <class Real>
+__device__ __forceinline__ void sic_mix(const SicState<Real>& st, const Real shock, const Real bubble, Real out[7])
+{
+    const Real G1 = st.g1 - 1, G2 = st.g2 - 1;
+    const Real F1 = st.g1 * st.pc1, F2 = st.g2 * st.pc2;
+    const Real rho = shock * st.rho1 + (1 - shock) * (st.rhoB * bubble + st.rho0 * (1 - bubble));
+    const Real u   = (shock * st.u1 + (1 - shock) * (st.uB * bubble + st.u0 * (1 - bubble))) * rho;
+    const Real v = 0, w = 0;
+    const Real G = (Real)(1. / (double)G1 * (double)(1 - bubble) + 1. / (double)G2 * (double)bubble);
+    const Real P = F1 / G1 * (1 - bubble) + F2 / G2 * bubble;
+    const Real pressure = shock * st.p1 + (1 - shock) * (st.pB * bubble + st.p0 * (1 - bubble));
+    const Real ke = (Real)(0.5 * (double)(u * u + v * v + w * w) / (double)rho);
+    out[0] = rho; out[1] = u; out[2] = v; out[3] = w;
+    out[4] = pressure * G + P + ke;
+    out[5] = G; out[6] = P;
+}
+
+constexpr int kSicMaxShapes = 1024;   // shapes of one tile kept in shared memory
+
+// One thread per cell of an 8x8x4 tile.  The tile first gathers the shapes
+// within reach of its samples (centre within radius + eps + h of the tile's
+// sample box): any other shape lies farther than eps + h from every sample,
+// so it is neither inside nor within the ramp and cannot change the
+// indicator.  More than kSicMaxShapes shapes in reach: every shape is used.
+template <class Real>
+__global__ void __launch_bounds__(256) sic_cloud_kernel(const DomDev* dom, int parity, const SicState<Real> st,
+                                                        const double* __restrict__ shapes, int nshapes, double eps)
+{
+    __shared__ Real sh[4 * kSicMaxShapes];
+    __shared__ int cnt;
+    const DomDev& D = *dom;
+    const double hd = D.h;
+    const int ix = blockIdx.x * 8 + (threadIdx.x & 7);
+    const int iy = blockIdx.y * 8 + ((threadIdx.x >> 3) & 7);
+    const int iz = blockIdx.z * 4 + (threadIdx.x >> 6);
+    if (threadIdx.x == 0) cnt = 0;
+    __syncthreads();
+    const double lo[3] = {hd * (blockIdx.x * 8), hd * (blockIdx.y * 8), hd * (blockIdx.z * 4)};
+    const double hi[3] = {hd * (blockIdx.x * 8 + 8), hd * (blockIdx.y * 8 + 8), hd * (blockIdx.z * 4 + 4)};
+    for (int i = threadIdx.x; i < nshapes; i += blockDim.x)
+    {
+        const double* c = shapes + 4 * (size_t)i;
+        const double reach = c[3] + eps + hd;
+        bool hit = true;
+        for (int d = 0; d < 3; ++d) hit = hit && (c[d] >= lo[d] - reach) && (c[d] <= hi[d] + reach);
+        if (hit)
+        {
+            const int k = atomicAdd(&cnt, 1);
+            if (k < kSicMaxShapes)
+                for (int j = 0; j < 4; ++j) sh[4 * k + j] = (Real)c[j];
+        }
+    }
+    __syncthreads();
+    if (ix >= D.nx || iy >= D.ny || iz >= D.nz) return;
+    const int nc = cnt;
+    const bool overflow = nc > kSicMaxShapes;   // then every shape, converted per use
+    Real all[4];
+
+    const Real h  = (Real)hd / 2;          // sample spacing: half the grid spacing
+    const double p[3] = {hd * (ix + 0.5), hd * (iy + 0.5), hd * (iz + 0.5)};
+    const Real x0[3] = {(Real)(p[0] - (double)h), (Real)(p[1] - (double)h), (Real)(p[2] - (double)h)};
+    const Real w6 = (Real)(1 / 6.), w23 = (Real)(2. / 3);
+    Real acc[7];
+    for (int jx = 0; jx < 3; ++jx)
+    {
+        Real yacc[7];
+        for (int jy = 0; jy < 3; ++jy)
+        {
+            Real zs[3][7];
+            for (int jz = 0; jz < 3; ++jz)
+            {
+                const Real pos[3] = {x0[0] + (Real)jx * h, x0[1] + (Real)jy * h, x0[2] + (Real)jz * h};
+                const Real sd = -(st.n[0] * (st.S[0] - pos[0]) + st.n[1] * (st.S[1] - pos[1]) + st.n[2] * (st.S[2] - pos[2]));
+                const Real shock = sd > 0 ? (Real)0 : (Real)1;
+                Real bubble = 0;
+                if (nshapes > 0)
+                {
+                    if (!overflow) bubble = sic_indicator<Real>(sh, nc, pos, eps);
+                    else
+                    {
+                        Real d = (Real)HUGE_VAL;
+                        for (int i = 0; i < nshapes; ++i)
+                        {
+                            for (int j = 0; j < 4; ++j) all[j] = (Real)shapes[4 * (size_t)i + j];
+                            const Real nd = sic_shape_eval<Real>(all, pos);
+                            d = (nd < d) ? nd : d;
+                        }
+                        const double x  = ((double)d + eps) / (2 * eps);
+                        const double mx = (0. < x) ? x : 0.;
+                        const double mn = (mx < 1.) ? mx : 1.;
+                        bubble = (Real)(0.5 + 0.5 * cos(3.14159265358979323846 * mn));
+                    }
+                }
+                sic_mix<Real>(st, shock, bubble, zs[jz]);
+            }
+            // z integral of this (x, y) column, then accumulated in y
+            Real zi[7];
+            for (int m = 0; m < 7; ++m) zi[m] = (w6 * zs[0][m] + w23 * zs[1][m]) + w6 * zs[2][m];
+            for (int m = 0; m < 7; ++m)
+                yacc[m] = jy == 0 ? w6 * zi[m] : (jy == 1 ? yacc[m] + w23 * zi[m] : yacc[m] + w6 * zi[m]);
+        }
+        for (int m = 0; m < 7; ++m)
+            acc[m] = jx == 0 ? w6 * yacc[m] : (jx == 1 ? acc[m] + w23 * yacc[m] : acc[m] + w6 * yacc[m]);
+    }
+    Real* U = (Real*)D.U[parity];
+    Real* R = (Real*)D.R;
+    const long long c = ix + (long long)D.nx * (iy + (long long)D.ny * iz);
+    for (int m = 0; m < 7; ++m) { U[m * D.fs + c] = acc[m]; R[m * D.fs + c] = (Real)0; }
+}
+
+cudaError_t launch_sic_cloud(int is_double, const DomDev* dom, int nx, int ny, int nz, int parity,
+                             const SicParams& P, const double* shapes, int nshapes, cudaStream_t st)
+{
+    const dim3 grid((nx + 7) / 8, (ny + 7) / 8, (nz + 3) / 4);
+    if (is_double) sic_cloud_kernel<double><<<grid, 256, 0, st>>>(dom, parity, sic_setup<double>(P), shapes, nshapes, P.eps);
+    else           sic_cloud_kernel<float><<<grid, 256, 0, st>>>(dom, parity, sic_setup<float>(P), shapes, nshapes, P.eps);
     return cudaGetLastError();
 }
 

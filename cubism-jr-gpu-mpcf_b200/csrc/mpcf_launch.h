@@ -31,6 +31,12 @@ StageKernelInfo stage_info_fp64(int ty, bool persist, bool sums, bool tma);
 cudaError_t launch_sos(int pol, const SosArgs& A, cudaStream_t st);
 cudaError_t launch_dt(int pol, const DtArgs& A, cudaStream_t st);
 cudaError_t launch_sum_tiles(const DomDev* doms, int ndom, const double* tile_sums, double* out, cudaStream_t st);
+// Shock-induced cloud-collapse IC (mpcf_aux.cu); post4 receives the
+// post-shock rho1, u1, p1 and the shock Mach number in the state's precision.
+cudaError_t launch_sic_cloud(int is_double, const DomDev* dom, int nx, int ny, int nz, int parity,
+                             const SicParams& P, const double* shapes, int nshapes, cudaStream_t st);
+void sic_post_shock(int is_double, const SicParams& P, double post4[4]);
+
 cudaError_t launch_ic_cloud(int is_double, const DomDev* dom, int parity, const IcParams& P,
                             const double* bubbles, int nbubbles, cudaStream_t st);
 cudaError_t launch_fill_ghosts(int is_double, const DomDev* dom, int parity,

@@ -87,4 +87,17 @@ struct IcParams
     unsigned long long seed;
 };
 
+// Parameters of the reference's shock-induced cloud-collapse case
+// (Sim_SICCloudMPI.cpp:52-81), in the order of its command-line options.
+struct SicParams
+{
+    double rho0, u0, p0;        // pre-shock liquid
+    double rhoB, uB, pB;        // bubble gas
+    double pressure_ratio;      // p1/p0 across the shock
+    double shock_n[3];          // shock normal (normalised by the set-up)
+    double shock_s[3];          // a point on the shock plane
+    double g1, g2, pc1, pc2;    // liquid / gas gamma and pc
+    double eps;                 // interface half-width (SimTools::EPSILON; 0: sharp)
+};
+
 } // namespace mpcf

@@ -44,6 +44,13 @@ class IcParams(ctypes.Structure):
                 ("noise", _D), ("width", _D), ("seed", _c.c_ulonglong)]
 
 
+class SicParams(ctypes.Structure):
+    """mirror of mpcf_sic_params (the reference's SICCloud case options)"""
+    _fields_ = [("rho0", _D), ("u0", _D), ("p0", _D), ("rhoB", _D), ("uB", _D), ("pB", _D),
+                ("pressure_ratio", _D), ("shock_n", _D * 3), ("shock_s", _D * 3),
+                ("g1", _D), ("g2", _D), ("pc1", _D), ("pc2", _D), ("eps", _D)]
+
+
 SIGNATURES = {
     "mpcf_version": (_I, []),
     "mpcf_last_error": (_c.c_char_p, []),
@@ -71,6 +78,9 @@ SIGNATURES = {
     "mpcf_ic_cloud": (_I, [_P, _I, _c.POINTER(IcParams), _I, _PD]),
     "mpcf_ic_cloud_host": (_I, [_I, _I, _I, _c.POINTER(IcParams), _I, _PD, _I, _PP]),
     "mpcf_bubbles": (_I, [_c.c_ulonglong, _I, _D, _D, _PD, _PD, _D, _I, _PD]),
+    "mpcf_sic_default_params": (None, [_c.POINTER(SicParams)]),
+    "mpcf_sic_post_shock": (_I, [_c.POINTER(SicParams), _I, _PD]),
+    "mpcf_ic_sic_cloud": (_I, [_P, _I, _c.POINTER(SicParams), _I, _PD]),
     "mpcf_set_tiling": (_I, [_P, _I, _I, _I]),
     "mpcf_get_tiling": (_I, [_P, _PI, _PI, _PI]),
     "mpcf_autotune": (_I, [_P, _I, _PI, _PD]),

@@ -166,6 +166,15 @@ class Solver:
         check(lib().mpcf_ic_cloud(self._h, dom, ctypes.byref(params), nb,
                                   b.ctypes.data_as(ctypes.POINTER(ctypes.c_double)) if nb else None))
 
+    def ic_sic_cloud(self, params, shapes, dom=0):
+        """The reference's shock-induced cloud-collapse IC (Sim_SICCloudMPI::_ic,
+        Sim_SICCloudMPI.cpp:43-357) on domain `dom`: params is a SicParams
+        (see sic_params), shapes an (n, 4) array of (x, y, z, radius)."""
+        b = np.ascontiguousarray(shapes, dtype=np.float64).reshape(-1)
+        n = b.size // 4
+        check(lib().mpcf_ic_sic_cloud(self._h, dom, ctypes.byref(params), n,
+                                      b.ctypes.data_as(ctypes.POINTER(ctypes.c_double)) if n else None))
+
     # -- launch configuration ----------------------------------------------
     def set_tiling(self, ty, dz, persistent=False, tma=True):
         flags = (_lib.TILE_PERSISTENT if persistent else 0) | (_lib.TILE_TMA if tma else 0)
@@ -192,6 +201,30 @@ class Solver:
         ms = ctypes.c_double()
         check(lib().mpcf_time_stages(self._h, int(reps), float(dtinvh), ctypes.byref(ms)))
         return ms.value
+
+
+def sic_params(**kw):
+    """SicParams with the reference's option defaults (Sim_SICCloudMPI.cpp:52-76),
+    overridden by keyword: rho0, u0, p0, rhoB, uB, pB, pressure_ratio,
+    shock_n (3), shock_s (3), g1, g2, pc1, pc2, eps."""
+    p = _lib.SicParams()
+    lib().mpcf_sic_default_params(ctypes.byref(p))
+    for k, v in kw.items():
+        if k in ("shock_n", "shock_s"):
+            for i in range(3):
+                getattr(p, k)[i] = float(v[i])
+        elif hasattr(p, k):
+            setattr(p, k, float(v))
+        else:
+            raise KeyError(k)
+    return p
+
+
+def sic_post_shock(params, precision="fp32_ref"):
+    """(rho1, u1, p1, mach) behind the shock, as the given precision computes them."""
+    out = (ctypes.c_double * 4)()
+    check(lib().mpcf_sic_post_shock(ctypes.byref(params), _lib.PRECISIONS[precision], out))
+    return tuple(out)
 
 
 def ic_cloud_host(dims, params, bubbles, dtype=np.float32):

@@ -9,6 +9,7 @@
 #include <cstdlib>
 #include <vector>
 #include <algorithm>
+#include <cmath>
 
 #include "NodeBlock.h"
 
@@ -36,6 +37,22 @@ struct flesh2ghost
     static inline uint_t X_R(const int ix, const int iy, const int iz) { return ghostmap::X(ix - NodeBlock::sizeX + 3, iy, iz); }
     static inline uint_t Y_L(const int ix, const int iy, const int iz) { return ghostmap::Y(ix, iy, iz); }
     static inline uint_t Y_R(const int ix, const int iy, const int iz) { return ghostmap::Y(ix, iy - NodeBlock::sizeY + 3, iz); }
+};
+
+// Interface-smoothing helpers of the case set-ups (source/Types.h:84-100):
+// a sharp step (1 where phi <= 0) and a cosine ramp of half-width EPSILON.
+class SimTools
+{
+public:
+    static double EPSILON;
+
+    static Real heaviside(const Real phi) { return phi > 0 ? 0 : 1; }
+
+    static Real heaviside_smooth(const Real phi)
+    {
+        const Real alpha = M_PI * std::min(1., std::max(0., 0.5 * (phi + EPSILON) / EPSILON));
+        return 0.5 + 0.5 * std::cos(alpha);
+    }
 };
 
 class Simulation

@@ -38,3 +38,12 @@ static inline int MPI_Allreduce(const void* s, void* r, int count, MPI_Datatype 
     return 0;
 }
 static inline int MPI_Bcast(void*, int, MPI_Datatype, int, MPI_Comm) { return 0; }
+
+#ifdef __cplusplus
+/* the datatype names of the MPI-2 C++ bindings, which the reference's case
+ * set-up passes to MPI_Bcast (Sim_SICCloudMPI.cpp:162-169) */
+namespace MPI
+{
+static const MPI_Datatype CHAR = 1, INT = 4, FLOAT = 4, DOUBLE = 8;
+}
+#endif

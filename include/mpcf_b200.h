@@ -190,6 +190,36 @@ int mpcf_ic_cloud_host(int nx, int ny, int nz, const mpcf_ic_params* p, int nbub
 int mpcf_bubbles(unsigned long long seed, int n, double rmin, double rmax,
                  const double* lo3, const double* hi3, double gap, int max_tries, double* out4);
 
+/* ---- shock-induced cloud collapse ----------------------------------------- *
+ * The reference's Sim_SICCloudMPI initial condition (replaces
+ * Sim_SICCloudMPI::_ic, Sim_SICCloudMPI.cpp:43-132 and _ic_quad, :339-357):
+ * a planar shock with Johnsen's post-shock liquid state behind it (the side
+ * where n.(x - s) <= 0), a cloud of spheres of gas ahead of it, and every
+ * cell set to the 3x3x3 Simpson average of the sampled mixture (samples at
+ * the cell centre and its faces).  Fields use the state's precision with the
+ * reference's rounding (FP32 bit-identical to the reference's
+ * _FLOAT_PRECISION_ build); the register is cleared.  shapes4 holds
+ * nshapes (x, y, z, radius) spheres, the lines of the reference's cloud.dat,
+ * rounded once to the state's precision.  eps is SimTools::EPSILON: 0 (the
+ * reference's SICCloud setting) gives a sharp interface, eps > 0 a cosine
+ * ramp of half-width eps.  mpcf_sic_default_params gives the reference's
+ * option defaults (Sim_SICCloudMPI.cpp:52-76); mpcf_sic_post_shock returns
+ * rho1, u1, p1 and the shock Mach number as that precision computes them
+ * (precision = MPCF_PREC_*). */
+typedef struct
+{
+    double rho0, u0, p0;            /* pre-shock liquid        -rho0 -u0 -p0 */
+    double rhoB, uB, pB;            /* bubble gas              -rhoB -uB -pB */
+    double pressure_ratio;          /* p1/p0 across the shock  -pressureratio */
+    double shock_n[3];              /* shock normal            -shockNx -shockNy -shockNz */
+    double shock_s[3];              /* point on the shock      -shockSx -shockSy -shockSz */
+    double g1, g2, pc1, pc2;        /* liquid / gas            -g1 -g2 -pc1 -pc2 */
+    double eps;                     /* SimTools::EPSILON */
+} mpcf_sic_params;
+void mpcf_sic_default_params(mpcf_sic_params* p);
+int mpcf_sic_post_shock(const mpcf_sic_params* p, int precision, double* post4);
+int mpcf_ic_sic_cloud(mpcf_solver* s, int dom, const mpcf_sic_params* p, int nshapes, const double* shapes4);
+
 /* ---- launch configuration ------------------------------------------------- *
  * tile = 32 x ty columns x dz slabs (ty 3 or 7; 15 for MPCF_PREC_FP32_REF),
  * one CTA of 32*(ty+1) threads per tile;

@@ -26,6 +26,7 @@
 #define RSQRT sqrtf
 #define RABS fabsf
 #include "oracle_core.h"
+#include "oracle_ic.h"
 #undef REAL
 #undef SFX
 #undef RMIN
@@ -41,6 +42,7 @@
 #define RSQRT sqrt
 #define RABS fabs
 #include "oracle_core.h"
+#include "oracle_ic.h"
 #undef REAL
 #undef SFX
 #undef RMIN
@@ -141,3 +143,36 @@ void oracle_stencil_f32(int nx, int ny, int nz, float** U, const float* gx_all, 
         out6[j] = cell_f32(nx, ny, nz, U, gx, gy, gz, q, ix + (dir == 0 ? o : 0), iy + (dir == 1 ? o : 0), iz + (dir == 2 ? o : 0));
     }
 }
+
+/* --------------------------------------------------------------------- */
+/* Shock-induced cloud-collapse IC (oracle_ic.h) on an nx*ny*nz block of
+ * spacing 1/max(nx,ny,nz), cell centres (i+0.5)h (NodeBlock.h:71,90-96).
+ * shapes4: nshapes x (cx, cy, cz, r), rounded to Real as the reference's
+ * cloud.dat reader does.  post4 (optional): rho1, u1, p1, mach. */
+#define ORACLE_SIC(SUF, T)                                                               \
+void oracle_sic_cloud_##SUF(int nx, int ny, int nz, const double* prm, int nshapes,      \
+                            const double* shapes4, double eps, T** out7, double* post4) \
+{                                                                                         \
+    sic_state_##SUF st;                                                                   \
+    sic_setup_##SUF(prm, &st);                                                            \
+    if (post4) { post4[0] = st.rho1; post4[1] = st.u1; post4[2] = st.p1; post4[3] = st.mach; } \
+    T* shp = (T*)malloc(sizeof(T) * 4 * (nshapes > 0 ? nshapes : 1));                      \
+    for (int i = 0; i < 4 * nshapes; ++i) shp[i] = (T)shapes4[i];                          \
+    const int mx = nx > ny ? (nx > nz ? nx : nz) : (ny > nz ? ny : nz);                   \
+    const double hd = 1.0 / mx;                                                           \
+    const T h = (T)hd;                                                                    \
+    _Pragma("omp parallel for")                                                           \
+    for (int iz = 0; iz < nz; ++iz)                                                       \
+        for (int iy = 0; iy < ny; ++iy)                                                   \
+            for (int ix = 0; ix < nx; ++ix)                                               \
+            {                                                                             \
+                const double p[3] = {hd * (ix + 0.5), hd * (iy + 0.5), hd * (iz + 0.5)};  \
+                T v[7];                                                                   \
+                sic_integral_##SUF(&st, shp, nshapes, eps, p, h / 2, v);                  \
+                const long long c = ix + (long long)nx * (iy + (long long)ny * iz);       \
+                for (int m = 0; m < 7; ++m) out7[m][c] = v[m];                            \
+            }                                                                             \
+    free(shp);                                                                            \
+}
+ORACLE_SIC(f32, float)
+ORACLE_SIC(f64, double)

@@ -9,6 +9,8 @@ It calls the reference's own code compiled from its sources (oracle/_ref):
     Batten s*, HLLC rho/vel/pvel/e, extra-term velocity, stencil reads),
   * source/BoundaryConditions.h absorbing/reflecting ghost fills,
   * source/MaxSpeedOfSound.cpp (MaxSpeedOfSound_CPP::compute),
+  * source/Sim/Sim_SICCloudMPI.cpp (the shock-induced cloud-collapse IC,
+    Sim_SICCloudMPI::_ic run on a 24x20x16 block),
 on seeded inputs, and stores inputs and outputs as .npz fixtures next to
 this script.  The reference has no golden vectors or known-answer tests of
 its own; these fixtures are its outputs, recorded here.
@@ -137,6 +139,45 @@ def make_sos():
     np.savez_compressed(os.path.join(HERE, "ref_sos.npz"), **rec)
 
 
+def sic_cases(rng):
+    """Parameter sets and clouds of the SICCloud IC cases: shock along x with a
+    sharp interface; an oblique shock with a cosine ramp; the reference's
+    option defaults with spheres cut by the domain edges."""
+    cases = []
+    prm = list(O.SIC_DEFAULTS)
+    prm[2], prm[10] = 100.0, 0.2                          # p0, shock point x
+    sh = [(0.5, 0.4, 0.3, 0.12), (0.75, 0.3, 0.35, 0.07), (0.62, 0.62, 0.45, 0.09)]
+    cases.append((prm, sh, 0.0))
+    prm = list(O.SIC_DEFAULTS)
+    prm[2], prm[6] = 10.0, 25.0                           # p0, pressure ratio
+    prm[7], prm[8], prm[9] = 1.0, 0.35, 0.2               # oblique normal
+    prm[10], prm[11], prm[12] = 0.15, 0.1, 0.3
+    sh = [tuple(v) for v in np.column_stack([rng.uniform(0.35, 0.95, 12), rng.uniform(0.1, 0.75, 12),
+                                             rng.uniform(0.1, 0.6, 12), rng.uniform(0.02, 0.08, 12)])]
+    cases.append((prm, sh, 0.03))
+    prm = list(O.SIC_DEFAULTS)
+    sh = [(0.98, 0.05, 0.3, 0.1), (0.4, 0.8, 0.64, 0.15), (0.3, 0.3, 0.0, 0.2)]
+    cases.append((prm, sh, 0.0))
+    # shapes as float32 values (the reference reads cloud.dat into Real)
+    return [(p, [tuple(float(np.float32(x)) for x in c) for c in sh], e) for p, sh, e in cases]
+
+
+def make_sic(rng):
+    import tempfile
+    L = O.ref_lib("libref_sic_ic")
+    rec = {}
+    for i, (prm, sh, eps) in enumerate(sic_cases(rng)):
+        with tempfile.TemporaryDirectory() as w:
+            dims, out, post = O.ref_sic_cloud(L, prm, sh, eps, w)
+        rec[f"dims{i}"] = np.array(dims)
+        rec[f"prm{i}"] = np.array(prm, np.float64)
+        rec[f"shapes{i}"] = np.array(sh, np.float64)
+        rec[f"eps{i}"] = np.float64(eps)
+        rec[f"U{i}"] = np.array(out)
+        rec[f"post{i}"] = np.array(post, np.float64)
+    np.savez_compressed(os.path.join(HERE, "ref_sic_ic.npz"), **rec)
+
+
 def main():
     sys.path.insert(0, os.path.join(os.path.dirname(os.path.dirname(HERE)), "cubism-jr-gpu-mpcf_b200"))
     L = O.ref_lib("libref_devmath_8x7x6")
@@ -146,6 +187,7 @@ def main():
     make_devmath(L, rng)
     make_bc(rng)
     make_sos()
+    make_sic(np.random.default_rng(20261204))
     print("wrote", sorted(f for f in os.listdir(HERE) if f.endswith(".npz")))
 
 

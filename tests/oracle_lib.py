@@ -64,6 +64,8 @@ def oracle():
         L.oracle_extraterm_hllc_vel_f32.restype = _F
         L.oracle_extraterm_hllc_vel_f32.argtypes = [_F] * 9
         L.oracle_stencil_f32.argtypes = [_I, _I, _I, _PPF, _PF, _PF, _PF, _I, _I, _I, _I, _I, _PF]
+        L.oracle_sic_cloud_f32.argtypes = [_I, _I, _I, _PD, _I, _PD, _D, _PPF, _PD]
+        L.oracle_sic_cloud_f64.argtypes = [_I, _I, _I, _PD, _I, _PD, _D, _PPD, _PD]
         _oracle = L
     return _oracle
 
@@ -80,6 +82,9 @@ def ref_lib(name):
     if name.startswith("libref_bc"):
         L.ref_fill_ghosts.argtypes = [_PI, _PPF, _PF, _PF, _PF]
         L.ref_bc_dims.argtypes = [_PI]
+    if name == "libref_sic_ic":
+        L.ref_sic_dims.argtypes = [_PI]
+        L.ref_sic_ic.argtypes = [_c.c_char_p, _I, _c.POINTER(_c.c_char_p), _D, _PPF, _PD]
     if name.startswith("libref_devmath"):
         L.ref_devmath_dims.argtypes = [_PI]
         for n in ("ref_weno_pluss", "ref_weno_minus", "ref_weno_pluss_clipped", "ref_weno_minus_clipped"):
@@ -150,3 +155,56 @@ def fill_ghosts(dims, bc, U):
     oracle().oracle_fill_ghosts_f32(nx, ny, nz, bc_arr(bc), fptrs(U),
                                     gx.ctypes.data_as(_PF), gy.ctypes.data_as(_PF), gz.ctypes.data_as(_PF))
     return gx, gy, gz
+
+
+# --- shock-induced cloud-collapse IC ------------------------------------------
+# Parameter vector order of oracle_sic_cloud_* (and of mpcf_sic_params):
+SIC_KEYS = ("rho0", "u0", "p0", "rhoB", "uB", "pB", "pressure_ratio",
+            "nx", "ny", "nz", "Sx", "Sy", "Sz", "g1", "g2", "pc1", "pc2")
+# the reference's command-line option of each (Sim_SICCloudMPI.cpp:52-76)
+SIC_OPTS = ("-rho0", "-u0", "-p0", "-rhoB", "-uB", "-pB", "-pressureratio",
+            "-shockNx", "-shockNy", "-shockNz", "-shockSx", "-shockSy", "-shockSz",
+            "-g1", "-g2", "-pc1", "-pc2")
+SIC_DEFAULTS = (1000.0, 0.0, 1.0, 1.0, 0.0, 0.0234, 40.0, 1.0, 0.0, 0.0, 0.05, 0.0, 0.0, 6.59, 1.4, 4096.0, 1.0)
+
+
+def sic_cloud(dims, prm, shapes, eps, dtype=np.float32):
+    """Oracle restatement of the SICCloud IC: (7 fields, (rho1, u1, p1, mach))."""
+    nx, ny, nz = dims
+    out = [np.zeros(nx * ny * nz, dtype) for _ in range(7)]
+    p = np.ascontiguousarray(prm, np.float64)
+    sh = np.ascontiguousarray(shapes, np.float64).reshape(-1)
+    post = (_D * 4)()
+    f = oracle().oracle_sic_cloud_f64 if dtype == np.float64 else oracle().oracle_sic_cloud_f32
+    f(nx, ny, nz, p.ctypes.data_as(_PD), sh.size // 4, sh.ctypes.data_as(_PD) if sh.size else None,
+      float(eps), fptrs(out), post)
+    return out, tuple(post)
+
+
+def ref_sic_cloud(L, prm, shapes, eps, workdir):
+    """The reference's own Sim_SICCloudMPI::_ic() (oracle/_ref/libref_sic_ic.so)
+    on its compile-time block: writes cloud_config.dat and cloud.dat into
+    workdir (shapes as 9-significant-digit text, exact for float32 values)."""
+    if any(float(v) < 0 for v in prm):
+        # ArgumentParser.h:104-121 takes every token that starts with '-' as
+        # an option name, so "-shockNz -0.2" would set shockNz = 1: the
+        # reference's command line cannot carry negative values
+        raise ValueError("negative option values cannot reach the reference's parser")
+    d = (_c.c_int * 3)()
+    L.ref_sic_dims(d)
+    n = d[0] * d[1] * d[2]
+    with open(os.path.join(workdir, "cloud_config.dat"), "w") as f:
+        f.write(f"{len(shapes)} 0\n0.01 0.5\n0 0 0\n1 1 1\n")
+    with open(os.path.join(workdir, "cloud.dat"), "w") as f:
+        for i, c in enumerate(shapes):
+            f.write(f"{i} {c[0]:.9g} {c[1]:.9g} {c[2]:.9g} {c[3]:.9g}\n")
+    args = [b"sic"]
+    for opt, v in zip(SIC_OPTS, prm):
+        args += [opt.encode(), repr(float(v)).encode()]
+    argv = (_c.c_char_p * len(args))(*args)
+    out = [np.zeros(n, np.float32) for _ in range(7)]
+    post = (_D * 4)()
+    rc = L.ref_sic_ic(workdir.encode(), len(args), argv, float(eps), fptrs(out), post)
+    if rc != 0:
+        raise RuntimeError(f"ref_sic_ic failed: {rc}")
+    return (d[0], d[1], d[2]), out, tuple(post)
