@@ -42,10 +42,10 @@ METRIC = "cell-stage updates/s on 1 B200: mixed vs plain FP64 at stated L1 error
 UNIT = "cell-stage updates/s"
 BYTES_PER_CELL_STAGE = {"fp32_ref": 112, "fp32": 112, "mixed": 112, "fp64": 224}
 # DRAM bytes per cell-stage of the mixed stage kernel measured by ncu
-# (dram__bytes_read.sum + dram__bytes_write.sum = 1.863 GB for one launch
+# (dram__bytes_read.sum + dram__bytes_write.sum = 1.851 GB for one launch
 # over the 256^3 cloud, 16.78 M cells).  Traffic grows in proportion to the
 # cells, so the per-launch figure of a larger workload is this times its cells.
-MEASURED_DRAM_BYTES_PER_CELL_STAGE = {"mixed": 1.863e9 / 256 ** 3}
+MEASURED_DRAM_BYTES_PER_CELL_STAGE = {"mixed": 1.851e9 / 256 ** 3}
 
 
 # Algorithmic floating-point operations of one cell-stage, counted by
