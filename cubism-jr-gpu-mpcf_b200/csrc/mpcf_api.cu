@@ -15,6 +15,7 @@
 #include <cstdlib>
 #include <cstring>
 #include <cmath>
+#include <functional>
 #include <random>
 #include <string>
 #include <vector>
@@ -838,6 +839,209 @@ int mpcf_ic_sic_cloud(mpcf_solver* s, int dom, const mpcf_sic_params* p, int nsh
     s->sums_valid = false;
     CK(cudaStreamSynchronize(s->stream));
     return MPCF_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Output and restart (the reference's _dump / _save / _restart,
+// Sim_SteadyStateMPI.cpp:138-180, with the arrays of HDF5Dumper_MPI.h).
+// The interleaved array moves in z-chunks of at most kIoChunk bytes through
+// one device buffer and one pinned host buffer.
+// ---------------------------------------------------------------------------
+static const size_t kIoChunk = 64u << 20;
+
+// op(host chunk, bytes, byte offset of the chunk in the whole array)
+typedef std::function<int(void*, size_t, size_t)> IoOp;
+
+static int io_run(mpcf_solver* s, int dom, int kind, bool to_host, const IoOp& op)
+{
+    const DomDev& D = s->hdoms[dom];
+    const int nch = kind == MPCF_DUMP_TENSOR ? 9 : 7;
+    const size_t slab = (size_t)D.nx * D.ny * nch * s->esz;
+    const int zc = (int)std::max<size_t>(1, std::min<size_t>((size_t)D.nz, kIoChunk / slab));
+    void* dbuf = nullptr;
+    void* hbuf = nullptr;
+    int rc = MPCF_OK;
+    if (cudaMalloc(&dbuf, slab * zc) != cudaSuccess) { cudaGetLastError(); return fail(MPCF_ERR_NOMEM, "cannot allocate the %zu B I/O staging buffer", slab * zc); }
+    if (cudaMallocHost(&hbuf, slab * zc) != cudaSuccess) { cudaGetLastError(); cudaFree(dbuf); return fail(MPCF_ERR_NOMEM, "cannot allocate the pinned I/O buffer"); }
+    for (int z0 = 0; z0 < D.nz && !rc; z0 += zc)
+    {
+        const int z1 = std::min(D.nz, z0 + zc);
+        const size_t bytes = slab * (z1 - z0);
+        cudaError_t e = cudaSuccess;
+        if (to_host)
+        {
+            e = launch_pack(s->esz == 8, kind, s->ddoms + dom, s->parity, z0, z1, dbuf, s->stream);
+            if (e == cudaSuccess) e = cudaMemcpyAsync(hbuf, dbuf, bytes, cudaMemcpyDeviceToHost, s->stream);
+            if (e == cudaSuccess) e = cudaStreamSynchronize(s->stream);
+            if (e == cudaSuccess) rc = op(hbuf, bytes, slab * z0);
+        }
+        else
+        {
+            rc = op(hbuf, bytes, slab * z0);
+            if (!rc) e = cudaMemcpyAsync(dbuf, hbuf, bytes, cudaMemcpyHostToDevice, s->stream);
+            if (!rc && e == cudaSuccess) e = launch_unpack_save(s->esz == 8, s->ddoms + dom, s->parity, z0, z1, dbuf, s->stream);
+            if (!rc && e == cudaSuccess) e = cudaStreamSynchronize(s->stream);
+        }
+        if (e != cudaSuccess) rc = fail(MPCF_ERR_CUDA, "output transfer: %s", cudaGetErrorString(e));
+    }
+    cudaFreeHost(hbuf);
+    cudaFree(dbuf);
+    return rc;
+}
+
+static std::string join_path(const char* dir, const std::string& name)
+{
+    std::string d = (dir && dir[0]) ? dir : ".";
+    return d + "/" + name;
+}
+
+int mpcf_pack(mpcf_solver* s, int dom, int kind, void* host_out)
+{
+    int rc = check_dom(s, dom);
+    if (rc) return rc;
+    if (!host_out || (kind != MPCF_DUMP_TENSOR && kind != MPCF_DUMP_SAVE)) return fail(MPCF_ERR_ARG, "bad arguments");
+    DeviceGuard g(s->device);
+    return io_run(s, dom, kind, true, [&](void* h, size_t b, size_t off) {
+        memcpy((char*)host_out + off, h, b);
+        return MPCF_OK;
+    });
+}
+
+int mpcf_unpack_save(mpcf_solver* s, int dom, const void* host_in)
+{
+    int rc = check_dom(s, dom);
+    if (rc) return rc;
+    if (!host_in) return fail(MPCF_ERR_ARG, "null input");
+    DeviceGuard g(s->device);
+    rc = io_run(s, dom, MPCF_DUMP_SAVE, false, [&](void* h, size_t b, size_t off) {
+        memcpy(h, (const char*)host_in + off, b);
+        return MPCF_OK;
+    });
+    s->sums_valid = false;
+    return rc;
+}
+
+int mpcf_dump(mpcf_solver* s, int dom, int kind, const char* dir, const char* name, int step)
+{
+    int rc = check_dom(s, dom);
+    if (rc) return rc;
+    if (!name || !name[0] || (kind != MPCF_DUMP_TENSOR && kind != MPCF_DUMP_SAVE)) return fail(MPCF_ERR_ARG, "bad arguments");
+    DeviceGuard g(s->device);
+    const DomDev& D = s->hdoms[dom];
+    const std::string bin = join_path(dir, std::string(name) + ".bin");
+    FILE* f = fopen(bin.c_str(), "wb");
+    if (!f) return fail(MPCF_ERR_ARG, "cannot open %s for writing", bin.c_str());
+    rc = io_run(s, dom, kind, true, [&](void* h, size_t b, size_t) {
+        return fwrite(h, 1, b, f) == b ? MPCF_OK : fail(MPCF_ERR_ARG, "short write to %s", bin.c_str());
+    });
+    if (fclose(f) != 0 && !rc) rc = fail(MPCF_ERR_ARG, "cannot close %s", bin.c_str());
+    if (rc) return rc;
+    // XDMF wrapper describing the array: node-centred data on a uniform mesh of
+    // spacing h with the origin at 0 (the dimensions listed z, y, x, channels)
+    const std::string xmf = join_path(dir, std::string(name) + ".xmf");
+    FILE* x = fopen(xmf.c_str(), "w");
+    if (!x) return fail(MPCF_ERR_ARG, "cannot open %s for writing", xmf.c_str());
+    const int nch = kind == MPCF_DUMP_TENSOR ? 9 : 7;
+    const char* attr = kind == MPCF_DUMP_TENSOR ? "Tensor" : "Save Data";
+    fprintf(x,
+            "<?xml version=\"1.0\" ?>\n"
+            "<!DOCTYPE Xdmf SYSTEM \"Xdmf.dtd\" []>\n"
+            "<Xdmf Version=\"2.0\">\n"
+            " <Domain>\n"
+            "   <Grid GridType=\"Uniform\">\n"
+            "     <Time Value=\"%05d\"/>\n"
+            "     <Topology TopologyType=\"3DCORECTMesh\" Dimensions=\"%d %d %d\"/>\n"
+            "     <Geometry GeometryType=\"ORIGIN_DXDYDZ\">\n"
+            "       <DataItem Name=\"Origin\" Dimensions=\"3\" NumberType=\"Float\" Precision=\"4\" Format=\"XML\">\n"
+            "        %e %e %e\n"
+            "       </DataItem>\n"
+            "       <DataItem Name=\"Spacing\" Dimensions=\"3\" NumberType=\"Float\" Precision=\"4\" Format=\"XML\">\n"
+            "        %e %e %e\n"
+            "       </DataItem>\n"
+            "     </Geometry>\n"
+            "     <Attribute Name=\"data\" AttributeType=\"%s\" Center=\"Node\">\n"
+            "       <DataItem Dimensions=\"%d %d %d %d\" NumberType=\"Float\" Precision=\"%d\" Format=\"Binary\" Endian=\"Little\">\n"
+            "        %s.bin\n"
+            "       </DataItem>\n"
+            "     </Attribute>\n"
+            "   </Grid>\n"
+            " </Domain>\n"
+            "</Xdmf>\n",
+            step, D.nz, D.ny, D.nx, 0., 0., 0., D.h, D.h, D.h, attr, D.nz, D.ny, D.nx, nch, (int)s->esz, name);
+    if (fclose(x) != 0) return fail(MPCF_ERR_ARG, "cannot close %s", xmf.c_str());
+    return MPCF_OK;
+}
+
+int mpcf_set_time(mpcf_solver* s, int dom, double t)
+{
+    int rc = check_dom(s, dom);
+    if (rc) return rc;
+    DeviceGuard g(s->device);
+    CK(cudaMemcpyAsync(s->time + dom, &t, sizeof(double), cudaMemcpyHostToDevice, s->stream));
+    CK(cudaStreamSynchronize(s->stream));
+    return MPCF_OK;
+}
+
+int mpcf_get_time(mpcf_solver* s, int dom, double* t)
+{
+    int rc = check_dom(s, dom);
+    if (rc) return rc;
+    if (!t) return fail(MPCF_ERR_ARG, "null output");
+    DeviceGuard g(s->device);
+    CK(cudaMemcpyAsync(t, s->time + dom, sizeof(double), cudaMemcpyDeviceToHost, s->stream));
+    CK(cudaStreamSynchronize(s->stream));
+    return MPCF_OK;
+}
+
+int mpcf_save(mpcf_solver* s, int dom, const char* dir, double t, int step, int fcount)
+{
+    int rc = check_dom(s, dom);
+    if (rc) return rc;
+    const std::string info = join_path(dir, "save.info");
+    FILE* f = fopen(info.c_str(), "w");
+    if (!f) return fail(MPCF_ERR_ARG, "cannot open %s for writing", info.c_str());
+    fprintf(f, "%.15g\n%d\n%d\n", t, step, fcount);
+    if (fclose(f) != 0) return fail(MPCF_ERR_ARG, "cannot close %s", info.c_str());
+    return mpcf_dump(s, dom, MPCF_DUMP_SAVE, dir, "save.data", step);
+}
+
+int mpcf_restart(mpcf_solver* s, int dom, const char* dir, double* t, int* step, int* fcount)
+{
+    int rc = check_dom(s, dom);
+    if (rc) return rc;
+    const std::string info = join_path(dir, "save.info");
+    FILE* f = fopen(info.c_str(), "r");
+    if (!f) return 0;                                    // nothing to restart from
+    double tt = 0;
+    int st = 0, fc = 0;
+    const int got = fscanf(f, "%lf %d %d", &tt, &st, &fc);
+    fclose(f);
+    if (got != 3) return fail(MPCF_ERR_ARG, "%s is not a save record", info.c_str());
+    const DomDev& D = s->hdoms[dom];
+    const size_t want = (size_t)D.nx * D.ny * D.nz * 7 * s->esz;
+    const std::string bin = join_path(dir, "save.data.bin");
+    FILE* b = fopen(bin.c_str(), "rb");
+    if (!b) return fail(MPCF_ERR_ARG, "cannot open %s", bin.c_str());
+    fseek(b, 0, SEEK_END);
+    const long size = ftell(b);
+    fseek(b, 0, SEEK_SET);
+    if (size < 0 || (size_t)size != want)
+    {
+        fclose(b);
+        return fail(MPCF_ERR_ARG, "%s holds %ld bytes, the domain needs %zu", bin.c_str(), size, want);
+    }
+    DeviceGuard g(s->device);
+    rc = io_run(s, dom, MPCF_DUMP_SAVE, false, [&](void* h, size_t n, size_t) {
+        return fread(h, 1, n, b) == n ? MPCF_OK : fail(MPCF_ERR_ARG, "short read from %s", bin.c_str());
+    });
+    fclose(b);
+    s->sums_valid = false;
+    if (rc) return rc;
+    if ((rc = mpcf_set_time(s, dom, tt))) return rc;
+    if (t) *t = tt;
+    if (step) *step = st;
+    if (fcount) *fcount = fc;
+    return 1;
 }
 
 int mpcf_ic_cloud_host(int nx, int ny, int nz, const mpcf_ic_params* p, int nbubbles,

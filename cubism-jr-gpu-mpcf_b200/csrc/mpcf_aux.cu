@@ -412,6 +412,90 @@ cudaError_t launch_sic_cloud(int is_double, const DomDev* dom, int nx, int ny, i
 }
 
 // ---------------------------------------------------------------------------
+// Output packing of the reference's dump and save (source/Types.h:192-277,
+// source/IO/HDF5Dumper_MPI.h:104-121,243-253): cell (ix,iy,iz) of slabs
+// [z0, z1) to out[NCH*(ix + nx*(iy + ny*(iz - z0))) + ch], channels
+//   kind 0 (myTensorialStreamer): rho, u, v, w, p, G, P, 0, 0 with
+//          p = (E - 0.5*(ru^2+rv^2+rw^2)/rho - P)/G, the 0.5 literal making
+//          that part double (the momentum squares are summed in Real);
+//   kind 1 (mySaveStreamer): the 7 conserved fields.
+// unpack_save_kernel is the restart direction of kind 1.
+// ---------------------------------------------------------------------------
+template <class T, int KIND>
+__global__ void pack_kernel(const DomDev* dom, int parity, int z0, int z1, T* __restrict__ out)
+{
+    const DomDev& D = *dom;
+    const T* U = (const T*)D.U[parity];
+    const long long plane = (long long)D.nx * D.ny;
+    const long long n = plane * (z1 - z0);
+    const long long base = plane * z0;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+    {
+        const long long c = base + i;
+        const T r = U[c], mu = U[D.fs + c], mv = U[2 * D.fs + c], mw = U[3 * D.fs + c];
+        const T e = U[4 * D.fs + c], G = U[5 * D.fs + c], P = U[6 * D.fs + c];
+        if (KIND == 0)
+        {
+            T* o = out + 9 * i;
+            o[0] = r;
+            o[1] = mu / r;
+            o[2] = mv / r;
+            o[3] = mw / r;
+            o[4] = (T)(((double)e - 0.5 * (double)(mu * mu + mv * mv + mw * mw) / (double)r - (double)P) / (double)G);
+            o[5] = G;
+            o[6] = P;
+            o[7] = (T)0;
+            o[8] = (T)0;
+        }
+        else
+        {
+            T* o = out + 7 * i;
+            o[0] = r; o[1] = mu; o[2] = mv; o[3] = mw; o[4] = e; o[5] = G; o[6] = P;
+        }
+    }
+}
+
+template <class T>
+__global__ void unpack_save_kernel(const DomDev* dom, int parity, int z0, int z1, const T* __restrict__ in)
+{
+    const DomDev& D = *dom;
+    T* U = (T*)D.U[parity];
+    T* R = (T*)D.R;
+    const long long plane = (long long)D.nx * D.ny;
+    const long long n = plane * (z1 - z0);
+    const long long base = plane * z0;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+    {
+        const long long c = base + i;
+        for (int m = 0; m < 7; ++m) { U[m * D.fs + c] = in[7 * i + m]; R[m * D.fs + c] = (T)0; }
+    }
+}
+
+cudaError_t launch_pack(int is_double, int kind, const DomDev* dom, int parity, int z0, int z1, void* out, cudaStream_t st)
+{
+    const int grid = 148 * 8;
+    if (is_double)
+    {
+        if (kind == 0) pack_kernel<double, 0><<<grid, 256, 0, st>>>(dom, parity, z0, z1, (double*)out);
+        else           pack_kernel<double, 1><<<grid, 256, 0, st>>>(dom, parity, z0, z1, (double*)out);
+    }
+    else
+    {
+        if (kind == 0) pack_kernel<float, 0><<<grid, 256, 0, st>>>(dom, parity, z0, z1, (float*)out);
+        else           pack_kernel<float, 1><<<grid, 256, 0, st>>>(dom, parity, z0, z1, (float*)out);
+    }
+    return cudaGetLastError();
+}
+
+cudaError_t launch_unpack_save(int is_double, const DomDev* dom, int parity, int z0, int z1, const void* in, cudaStream_t st)
+{
+    const int grid = 148 * 8;
+    if (is_double) unpack_save_kernel<double><<<grid, 256, 0, st>>>(dom, parity, z0, z1, (const double*)in);
+    else           unpack_save_kernel<float><<<grid, 256, 0, st>>>(dom, parity, z0, z1, (const float*)in);
+    return cudaGetLastError();
+}
+
+// ---------------------------------------------------------------------------
 // Explicit ghost buffers in the reference layouts, from the same boundary
 // map the stage kernel applies on the fly:
 //   gx[side][q][GHOSTMAPX(ix,iy,iz)]  = ix + 3*(iy + NY*iz),     ix 0..2

@@ -31,6 +31,11 @@ StageKernelInfo stage_info_fp64(int ty, bool persist, bool sums, bool tma);
 cudaError_t launch_sos(int pol, const SosArgs& A, cudaStream_t st);
 cudaError_t launch_dt(int pol, const DtArgs& A, cudaStream_t st);
 cudaError_t launch_sum_tiles(const DomDev* doms, int ndom, const double* tile_sums, double* out, cudaStream_t st);
+// Interleaved output arrays of the reference's dump (kind 0, 9 channels) and
+// save (kind 1, 7 channels) for slabs [z0, z1), and the restart direction.
+cudaError_t launch_pack(int is_double, int kind, const DomDev* dom, int parity, int z0, int z1, void* out, cudaStream_t st);
+cudaError_t launch_unpack_save(int is_double, const DomDev* dom, int parity, int z0, int z1, const void* in, cudaStream_t st);
+
 // Shock-induced cloud-collapse IC (mpcf_aux.cu); post4 receives the
 // post-shock rho1, u1, p1 and the shock Mach number in the state's precision.
 cudaError_t launch_sic_cloud(int is_double, const DomDev* dom, int nx, int ny, int nz, int parity,

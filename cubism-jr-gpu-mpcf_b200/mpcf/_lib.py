@@ -21,6 +21,8 @@ BC_ABSORBING = 0
 BC_REFLECTING = 1
 
 ERR_ARG, ERR_CUDA, ERR_NOMEM, ERR_STATE, ERR_NUMERIC = -1, -2, -3, -4, -5
+DUMP_TENSOR = 0
+DUMP_SAVE = 1
 ERRBIT_NONPHYSICAL = 1
 ERRBIT_SOS = 2
 ERRBIT_TMA_TIMEOUT = 4
@@ -81,6 +83,13 @@ SIGNATURES = {
     "mpcf_sic_default_params": (None, [_c.POINTER(SicParams)]),
     "mpcf_sic_post_shock": (_I, [_c.POINTER(SicParams), _I, _PD]),
     "mpcf_ic_sic_cloud": (_I, [_P, _I, _c.POINTER(SicParams), _I, _PD]),
+    "mpcf_pack": (_I, [_P, _I, _I, _P]),
+    "mpcf_unpack_save": (_I, [_P, _I, _P]),
+    "mpcf_dump": (_I, [_P, _I, _I, _c.c_char_p, _c.c_char_p, _I]),
+    "mpcf_save": (_I, [_P, _I, _c.c_char_p, _D, _I, _I]),
+    "mpcf_restart": (_I, [_P, _I, _c.c_char_p, _PD, _PI, _PI]),
+    "mpcf_set_time": (_I, [_P, _I, _D]),
+    "mpcf_get_time": (_I, [_P, _I, _PD]),
     "mpcf_set_tiling": (_I, [_P, _I, _I, _I]),
     "mpcf_get_tiling": (_I, [_P, _PI, _PI, _PI]),
     "mpcf_autotune": (_I, [_P, _I, _PI, _PD]),

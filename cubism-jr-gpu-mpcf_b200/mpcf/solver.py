@@ -175,6 +175,48 @@ class Solver:
         check(lib().mpcf_ic_sic_cloud(self._h, dom, ctypes.byref(params), n,
                                       b.ctypes.data_as(ctypes.POINTER(ctypes.c_double)) if n else None))
 
+    # -- output and restart (Sim_SteadyStateMPI.cpp:138-180) ---------------
+    def pack(self, kind="tensor", dom=0):
+        """The reference's dump ("tensor": rho, u, v, w, p, G, P, 0, 0) or save
+        ("save": the conserved fields) array of a domain, shape (nz, ny, nx, ch)."""
+        k = _lib.DUMP_TENSOR if kind == "tensor" else _lib.DUMP_SAVE
+        nx, ny, nz = self.dims[dom]
+        out = np.empty((nz, ny, nx, 9 if k == _lib.DUMP_TENSOR else 7), dtype=self.dtype)
+        check(lib().mpcf_pack(self._h, dom, k, out.ctypes.data))
+        return out
+
+    def unpack_save(self, arr, dom=0):
+        a = np.ascontiguousarray(arr, dtype=self.dtype)
+        nx, ny, nz = self.dims[dom]
+        if a.size != nx * ny * nz * 7:
+            raise ValueError("save array has the wrong size")
+        check(lib().mpcf_unpack_save(self._h, dom, a.ctypes.data))
+
+    def dump(self, directory, name, step=0, kind="tensor", dom=0):
+        k = _lib.DUMP_TENSOR if kind == "tensor" else _lib.DUMP_SAVE
+        check(lib().mpcf_dump(self._h, dom, k, str(directory).encode(), name.encode(), int(step)))
+
+    def save(self, directory, t, step, fcount=0, dom=0):
+        check(lib().mpcf_save(self._h, dom, str(directory).encode(), float(t), int(step), int(fcount)))
+
+    def restart(self, directory, dom=0):
+        """(t, step, fcount) after loading <directory>/save.*, or None when
+        there is no save record (the reference's _restart returning false)."""
+        t, st, fc = ctypes.c_double(), ctypes.c_int(), ctypes.c_int()
+        rc = lib().mpcf_restart(self._h, dom, str(directory).encode(), ctypes.byref(t), ctypes.byref(st), ctypes.byref(fc))
+        if rc == 0:
+            return None
+        check(rc if rc < 0 else 0)
+        return t.value, st.value, fc.value
+
+    def set_time(self, t, dom=0):
+        check(lib().mpcf_set_time(self._h, dom, float(t)))
+
+    def get_time(self, dom=0):
+        t = ctypes.c_double()
+        check(lib().mpcf_get_time(self._h, dom, ctypes.byref(t)))
+        return t.value
+
     # -- launch configuration ----------------------------------------------
     def set_tiling(self, ty, dz, persistent=False, tma=True):
         flags = (_lib.TILE_PERSISTENT if persistent else 0) | (_lib.TILE_TMA if tma else 0)

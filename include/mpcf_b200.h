@@ -220,6 +220,39 @@ void mpcf_sic_default_params(mpcf_sic_params* p);
 int mpcf_sic_post_shock(const mpcf_sic_params* p, int precision, double* post4);
 int mpcf_ic_sic_cloud(mpcf_solver* s, int dom, const mpcf_sic_params* p, int nshapes, const double* shapes4);
 
+/* ---- output and restart --------------------------------------------------- *
+ * The arrays of the reference's dump and save (replaces
+ * Sim_SteadyStateMPI::_dump/_save/_restart, Sim_SteadyStateMPI.cpp:138-180,
+ * with DumpHDF5_MPI / ReadHDF5_MPI, IO/HDF5Dumper_MPI.h:30-260): one array of
+ * nz x ny x nx cells x channels (channels fastest, then x, y, z) in the
+ * state's precision, filled as the reference's streamers fill it
+ * (Types.h:192-277):
+ *   MPCF_DUMP_TENSOR  9 channels: rho, u, v, w, p, G, P, 0, 0 (_dump)
+ *   MPCF_DUMP_SAVE    7 channels: the conserved fields (_save, restart)
+ * mpcf_pack copies the array into host memory (for a caller's own writer,
+ * e.g. HDF5); mpcf_unpack_save loads a MPCF_DUMP_SAVE array back into the
+ * state (register cleared).
+ * mpcf_dump writes <dir>/<name>.bin (the array, little-endian, no header) and
+ * <dir>/<name>.xmf, the reference's XDMF description with the data item
+ * pointing at the raw file (Format="Binary") where the reference points at
+ * its HDF5 dataset; readers of XDMF (ParaView, VisIt) open it as is.
+ * mpcf_save writes <dir>/save.info (t with 15 significant digits, step,
+ * fcount: one per line, as _save does) and the MPCF_DUMP_SAVE array as
+ * <dir>/save.data.{bin,xmf}.  mpcf_restart reads them back into the state,
+ * sets the domain's time to t and returns 1, or returns 0 when there is no
+ * <dir>/save.info (as _restart returns false).  The reference keeps save.info
+ * in the working directory and the data under -fpath; here both are in dir.
+ * mpcf_set_time / mpcf_get_time: the domain's accumulated time. */
+#define MPCF_DUMP_TENSOR 0
+#define MPCF_DUMP_SAVE   1
+int mpcf_pack(mpcf_solver* s, int dom, int kind, void* host_out);
+int mpcf_unpack_save(mpcf_solver* s, int dom, const void* host_in);
+int mpcf_dump(mpcf_solver* s, int dom, int kind, const char* dir, const char* name, int step);
+int mpcf_save(mpcf_solver* s, int dom, const char* dir, double t, int step, int fcount);
+int mpcf_restart(mpcf_solver* s, int dom, const char* dir, double* t, int* step, int* fcount);
+int mpcf_set_time(mpcf_solver* s, int dom, double t);
+int mpcf_get_time(mpcf_solver* s, int dom, double* t);
+
 /* ---- launch configuration ------------------------------------------------- *
  * tile = 32 x ty columns x dz slabs (ty 3 or 7; 15 for MPCF_PREC_FP32_REF),
  * one CTA of 32*(ty+1) threads per tile;

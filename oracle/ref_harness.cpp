@@ -11,6 +11,10 @@
  *   REF_HARNESS_BC:  BoundaryConditions<NodeBlock>::applyBC_absorbing /
  *                    applyBC_reflecting (source/BoundaryConditions.h:60-109)
  *                    for the compile-time block size.
+ *   REF_HARNESS_DUMP: the output streamers myTensorialStreamer and
+ *                    mySaveStreamer (source/Types.h:192-277) filling the
+ *                    interleaved array DumpHDF5_MPI / ReadHDF5_MPI move
+ *                    (source/IO/HDF5Dumper_MPI.h:104-121, 243-253).
  */
 #include <vector>
 #include <cstring>
@@ -79,6 +83,57 @@ extern "C" int ref_fill_ghosts(const int* bc, float** U, float* gx_all, float* g
     if (bc[3]) b.applyBC_reflecting<1,1,ghostmap::Y>(hy[1]); else b.applyBC_absorbing<1,1,ghostmap::Y>(hy[1]);
     if (bc[4]) b.applyBC_reflecting<2,0,ghostmap::Z>(hz[0]); else b.applyBC_absorbing<2,0,ghostmap::Z>(hz[0]);
     if (bc[5]) b.applyBC_reflecting<2,1,ghostmap::Z>(hz[1]); else b.applyBC_absorbing<2,1,ghostmap::Z>(hz[1]);
+    return 0;
+}
+#endif
+
+#ifdef REF_HARNESS_DUMP
+#include "Types.h"
+
+extern "C" int ref_dump_dims(int* d) { d[0] = _BLOCKSIZEX_; d[1] = _BLOCKSIZEY_; d[2] = _BLOCKSIZEZ_; return 0; }
+
+/* out[NCH*(ix + NX*(iy + NY*iz)) + c] = channel c of the streamer at (ix,iy,iz):
+ * kind 0 = myTensorialStreamer (9 channels), 1 = mySaveStreamer (7) */
+extern "C" int ref_pack(int kind, float** U, float* out)
+{
+    std::vector<Real*> ptr(U, U + 7);
+    const int NX = _BLOCKSIZEX_, NY = _BLOCKSIZEY_, NZ = _BLOCKSIZEZ_;
+    for (int iz = 0; iz < NZ; ++iz)
+        for (int iy = 0; iy < NY; ++iy)
+            for (int ix = 0; ix < NX; ++ix)
+            {
+                if (kind == 0)
+                {
+                    myTensorialStreamer st(ptr);
+                    Real o[myTensorialStreamer::NCHANNELS];
+                    st.operate(ix, iy, iz, o);
+                    std::memcpy(out + myTensorialStreamer::NCHANNELS * (ix + NX * (iy + NY * iz)), o, sizeof(o));
+                }
+                else
+                {
+                    mySaveStreamer st(ptr);
+                    Real o[mySaveStreamer::NCHANNELS];
+                    st.operate(ix, iy, iz, o);
+                    std::memcpy(out + mySaveStreamer::NCHANNELS * (ix + NX * (iy + NY * iz)), o, sizeof(o));
+                }
+            }
+    return 0;
+}
+
+/* the restart direction: mySaveStreamer::operate(input, ix, iy, iz) */
+extern "C" int ref_unpack_save(const float* in, float** U)
+{
+    std::vector<Real*> ptr(U, U + 7);
+    mySaveStreamer st(ptr);
+    const int NX = _BLOCKSIZEX_, NY = _BLOCKSIZEY_, NZ = _BLOCKSIZEZ_;
+    for (int iz = 0; iz < NZ; ++iz)
+        for (int iy = 0; iy < NY; ++iy)
+            for (int ix = 0; ix < NX; ++ix)
+            {
+                Real v[mySaveStreamer::NCHANNELS];
+                std::memcpy(v, in + mySaveStreamer::NCHANNELS * (ix + NX * (iy + NY * iz)), sizeof(v));
+                st.operate(v, ix, iy, iz);
+            }
     return 0;
 }
 #endif

@@ -11,6 +11,7 @@ It calls the reference's own code compiled from its sources (oracle/_ref):
   * source/MaxSpeedOfSound.cpp (MaxSpeedOfSound_CPP::compute),
   * source/Sim/Sim_SICCloudMPI.cpp (the shock-induced cloud-collapse IC,
     Sim_SICCloudMPI::_ic run on a 24x20x16 block),
+  * source/Types.h output streamers (the arrays of the dump and the save),
 on seeded inputs, and stores inputs and outputs as .npz fixtures next to
 this script.  The reference has no golden vectors or known-answer tests of
 its own; these fixtures are its outputs, recorded here.
@@ -178,6 +179,18 @@ def make_sic(rng):
     np.savez_compressed(os.path.join(HERE, "ref_sic_ic.npz"), **rec)
 
 
+def make_dump():
+    """The reference's dump and save arrays (myTensorialStreamer,
+    mySaveStreamer) of a 12x10x8 cloud state with a velocity field."""
+    L = O.ref_lib("libref_dump_12x10x8")
+    U = cloud((12, 10, 8), 41)
+    rng = np.random.default_rng(41)
+    for q in (1, 2, 3):                          # momenta of |u| up to ~5
+        U[q] = (U[0] * rng.uniform(-5, 5, U[0].size)).astype(np.float32)
+    rec = {"U": np.array(U), "tensor": O.ref_pack(L, "tensor", U), "save": O.ref_pack(L, "save", U)}
+    np.savez_compressed(os.path.join(HERE, "ref_dump.npz"), **rec)
+
+
 def main():
     sys.path.insert(0, os.path.join(os.path.dirname(os.path.dirname(HERE)), "cubism-jr-gpu-mpcf_b200"))
     L = O.ref_lib("libref_devmath_8x7x6")
@@ -188,6 +201,7 @@ def main():
     make_bc(rng)
     make_sos()
     make_sic(np.random.default_rng(20261204))
+    make_dump()
     print("wrote", sorted(f for f in os.listdir(HERE) if f.endswith(".npz")))
 
 

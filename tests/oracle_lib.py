@@ -82,6 +82,10 @@ def ref_lib(name):
     if name.startswith("libref_bc"):
         L.ref_fill_ghosts.argtypes = [_PI, _PPF, _PF, _PF, _PF]
         L.ref_bc_dims.argtypes = [_PI]
+    if name.startswith("libref_dump"):
+        L.ref_dump_dims.argtypes = [_PI]
+        L.ref_pack.argtypes = [_I, _PPF, _PF]
+        L.ref_unpack_save.argtypes = [_PF, _PPF]
     if name == "libref_sic_ic":
         L.ref_sic_dims.argtypes = [_PI]
         L.ref_sic_ic.argtypes = [_c.c_char_p, _I, _c.POINTER(_c.c_char_p), _D, _PPF, _PD]
@@ -208,3 +212,32 @@ def ref_sic_cloud(L, prm, shapes, eps, workdir):
     if rc != 0:
         raise RuntimeError(f"ref_sic_ic failed: {rc}")
     return (d[0], d[1], d[2]), out, tuple(post)
+
+
+# --- dump / save arrays -------------------------------------------------------
+def pack(U, dims, kind):
+    """The interleaved (nz, ny, nx, channels) array the reference's streamers
+    fill (Types.h:192-277): kind "tensor" = rho, u, v, w, p, G, P, 0, 0 with
+    p = (E - 0.5*(ru^2+rv^2+rw^2)/rho - P)/G (the 0.5 literal makes that part
+    double; the squares are summed in the state's type); kind "save" = the
+    7 conserved fields."""
+    nx, ny, nz = dims
+    r, mu, mv, mw, e, G, P = [np.asarray(a).reshape(nz, ny, nx) for a in U]
+    if kind == "save":
+        return np.stack([r, mu, mv, mw, e, G, P], axis=-1)
+    T = r.dtype.type
+    sq = (mu * mu + mv * mv) + mw * mw
+    f = np.float64
+    p = ((e.astype(f) - 0.5 * sq.astype(f) / r.astype(f)) - P.astype(f)) / G.astype(f)
+    z = np.zeros_like(r)
+    return np.stack([r, mu / r, mv / r, mw / r, p.astype(T), G, P, z, z], axis=-1)
+
+
+def ref_pack(L, kind, U):
+    """The reference's own streamers (oracle/_ref/libref_dump_*.so)."""
+    d = (_c.c_int * 3)()
+    L.ref_dump_dims(d)
+    nch = 9 if kind == "tensor" else 7
+    out = np.zeros(d[0] * d[1] * d[2] * nch, np.float32)
+    L.ref_pack(0 if kind == "tensor" else 1, fptrs([np.ascontiguousarray(a, np.float32) for a in U]), out.ctypes.data_as(_PF))
+    return out.reshape(d[2], d[1], d[0], nch)
