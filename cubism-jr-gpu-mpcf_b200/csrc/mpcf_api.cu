@@ -841,6 +841,85 @@ int mpcf_ic_sic_cloud(mpcf_solver* s, int dom, const mpcf_sic_params* p, int nsh
     return MPCF_OK;
 }
 
+void mpcf_case_default_params(mpcf_steady_params* st, mpcf_sod_params* sod, mpcf_sbi_params* sbi)
+{
+    if (st) { *st = mpcf_steady_params(); st->rho = 1; st->p = 1; st->g = 1.4; }
+    if (sod)
+    {
+        *sod = mpcf_sod_params();
+        sod->x0 = 0.5; sod->rho1 = 1; sod->rho2 = 0.125; sod->p1 = 1; sod->p2 = 0.1; sod->g1 = 1.4; sod->g2 = 1.4;
+    }
+    if (sbi)
+    {
+        *sbi = mpcf_sbi_params();
+        sbi->x0 = 0.1; sbi->mach = 1.22; sbi->rho = 1; sbi->rhobubble = 0.138; sbi->p = 1; sbi->pbubble = 1;
+        sbi->g1 = 1.4; sbi->g2 = 1.67; sbi->mollfactor = 1; sbi->axis0 = 0; sbi->axis1 = 1;
+    }
+}
+
+int mpcf_ic_steady(mpcf_solver* s, int dom, const mpcf_steady_params* p)
+{
+    int rc = check_dom(s, dom);
+    if (rc) return rc;
+    if (!p || !(p->g > 1) || !(p->rho > 0)) return fail(MPCF_ERR_ARG, "bad SteadyState parameters");
+    DeviceGuard g(s->device);
+    SteadyParams P;
+    static_assert(sizeof(SteadyParams) == sizeof(mpcf_steady_params), "parameter layout");
+    memcpy(&P, p, sizeof(P));
+    CK(launch_ic_steady(s->esz == 8, s->ddoms + dom, s->parity, P, s->stream));
+    s->sums_valid = false;
+    CK(cudaStreamSynchronize(s->stream));
+    return MPCF_OK;
+}
+
+int mpcf_ic_sod(mpcf_solver* s, int dom, const mpcf_sod_params* p)
+{
+    int rc = check_dom(s, dom);
+    if (rc) return rc;
+    if (!p || p->axis < 0 || p->axis > 2 || !(p->g1 > 1) || !(p->g2 > 1) || !(p->rho1 > 0) || !(p->rho2 > 0))
+        return fail(MPCF_ERR_ARG, "bad Sod parameters");
+    DeviceGuard g(s->device);
+    SodParams P;
+    static_assert(sizeof(SodParams) == sizeof(mpcf_sod_params), "parameter layout");
+    memcpy(&P, p, sizeof(P));
+    CK(launch_ic_sod(s->esz == 8, s->ddoms + dom, s->parity, P, s->stream));
+    s->sums_valid = false;
+    CK(cudaStreamSynchronize(s->stream));
+    return MPCF_OK;
+}
+
+int mpcf_ic_sbi(mpcf_solver* s, int dom, const mpcf_sbi_params* p, int nbubbles, const double* bubbles4)
+{
+    int rc = check_dom(s, dom);
+    if (rc) return rc;
+    if (!p || p->axis0 < 0 || p->axis0 > 2 || p->axis1 < 0 || p->axis1 > 2 || p->axis0 == p->axis1 ||
+        !(p->g1 > 1) || !(p->g2 > 1) || !(p->mach >= 1) || p->mollfactor < 1)
+        return fail(MPCF_ERR_ARG, "bad 2DSBI parameters");
+    if (nbubbles < 0 || (nbubbles > 0 && !bubbles4)) return fail(MPCF_ERR_ARG, "bad bubble arguments");
+    DeviceGuard g(s->device);
+    if (nbubbles > s->bubbles_cap)
+    {
+        if (s->bubbles)
+        {
+            CK(cudaStreamSynchronize(s->stream));
+            cudaFree(s->bubbles);
+            s->allocs.erase(std::remove(s->allocs.begin(), s->allocs.end(), (void*)s->bubbles), s->allocs.end());
+            s->bubbles = nullptr;
+        }
+        if ((rc = dev_alloc(s, (void**)&s->bubbles, sizeof(double) * 4 * (size_t)nbubbles))) return rc;
+        s->bubbles_cap = nbubbles;
+    }
+    if (nbubbles > 0) CK(cudaMemcpyAsync(s->bubbles, bubbles4, sizeof(double) * 4 * nbubbles, cudaMemcpyHostToDevice, s->stream));
+    SbiParams P;
+    static_assert(sizeof(SbiParams) == sizeof(mpcf_sbi_params), "parameter layout");
+    memcpy(&P, p, sizeof(P));
+    const DomDev& D = s->hdoms[dom];
+    CK(launch_ic_sbi(s->esz == 8, s->ddoms + dom, D.nx, D.ny, D.nz, s->parity, P, s->bubbles, nbubbles, s->stream));
+    s->sums_valid = false;
+    CK(cudaStreamSynchronize(s->stream));
+    return MPCF_OK;
+}
+
 // ---------------------------------------------------------------------------
 // Output and restart (the reference's _dump / _save / _restart,
 // Sim_SteadyStateMPI.cpp:138-180, with the arrays of HDF5Dumper_MPI.h).

@@ -4,6 +4,7 @@
 #include <cuda_runtime.h>
 #include <math.h>
 #include <cmath>
+#include <algorithm>
 #include <mutex>
 #include "mpcf_math.cuh"
 #include "mpcf_stage.cuh"
@@ -408,6 +409,175 @@ cudaError_t launch_sic_cloud(int is_double, const DomDev* dom, int nx, int ny, i
     const dim3 grid((nx + 7) / 8, (ny + 7) / 8, (nz + 3) / 4);
     if (is_double) sic_cloud_kernel<double><<<grid, 256, 0, st>>>(dom, parity, sic_setup<double>(P), shapes, nshapes, P.eps);
     else           sic_cloud_kernel<float><<<grid, 256, 0, st>>>(dom, parity, sic_setup<float>(P), shapes, nshapes, P.eps);
+    return cudaGetLastError();
+}
+
+// ---------------------------------------------------------------------------
+// The reference's other case set-ups: SteadyState (Sim_SteadyStateMPI.cpp:
+// 95-135), Sod (Sim_SodMPI.cpp:20-95) and 2DSBI (Sim_2DSBIMPI.cpp:83-233).
+// Each evaluates in double where the reference's options are doubles and in
+// the state's type where it stores to Real; the register is cleared.
+// ---------------------------------------------------------------------------
+template <class T>
+__global__ void fill_state_kernel(const DomDev* dom, int parity, const T v0, const T v1, const T v2, const T v3,
+                                  const T v4, const T v5, const T v6)
+{
+    const DomDev& D = *dom;
+    T* U = (T*)D.U[parity];
+    T* R = (T*)D.R;
+    const long long n = (long long)D.nx * D.ny * D.nz;
+    const T v[7] = {v0, v1, v2, v3, v4, v5, v6};
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+        for (int m = 0; m < 7; ++m) { U[m * D.fs + i] = v[m]; R[m * D.fs + i] = (T)0; }
+}
+
+cudaError_t launch_ic_steady(int is_double, const DomDev* dom, int parity, const SteadyParams& P, cudaStream_t st)
+{
+    // the uniform state in double (Sim_SteadyStateMPI.cpp:111-117)
+    const double ru = P.rho * P.u, rv = P.rho * P.v, rw = P.rho * P.w;
+    const double G  = 1.0 / (P.g - 1.0);
+    const double Pc = P.g * P.pc * G;
+    const double e  = G * P.p + Pc + 0.5 * P.rho * (P.u * P.u + P.v * P.v + P.w * P.w);
+    if (is_double) fill_state_kernel<double><<<148 * 8, 256, 0, st>>>(dom, parity, P.rho, ru, rv, rw, e, G, Pc);
+    else           fill_state_kernel<float><<<148 * 8, 256, 0, st>>>(dom, parity, (float)P.rho, (float)ru, (float)rv,
+                                                                       (float)rw, (float)e, (float)G, (float)Pc);
+    return cudaGetLastError();
+}
+
+template <class T>
+__global__ void sod_kernel(const DomDev* dom, int parity, const SodParams P)
+{
+    const DomDev& D = *dom;
+    T* U = (T*)D.U[parity];
+    T* R = (T*)D.R;
+    const long long n = (long long)D.nx * D.ny * D.nz;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+    {
+        const int idx[3] = {(int)(i % D.nx), (int)((i / D.nx) % D.ny), (int)(i / ((long long)D.nx * D.ny))};
+        const double pos = D.h * (idx[P.axis] + 0.5);
+        const bool x = P.reverse ? pos > P.x0 : pos < P.x0;
+        const bool nx = !x;
+        // the reference's boolean-weighted mixture (Sim_SodMPI.cpp:69-75)
+        const double r = x * P.rho1 + nx * P.rho2;
+        const double p = x * P.p1 + nx * P.p2;
+        const double u = x * P.rho1 * P.u1 + nx * P.rho2 * P.u2;
+        const double G = x * 1. / (P.g1 - 1.) + nx * 1. / (P.g2 - 1.);
+        const double Pc = x * P.pc1 * P.g1 / (P.g1 - 1.) + nx * P.pc2 * P.g2 / (P.g2 - 1.);
+        const T v[7] = {(T)r, (T)(P.axis == 0 ? u : 0.), (T)(P.axis == 1 ? u : 0.), (T)(P.axis == 2 ? u : 0.),
+                        (T)(G * p + Pc + 0.5 * u * u / r), (T)G, (T)Pc};
+        for (int m = 0; m < 7; ++m) { U[m * D.fs + i] = v[m]; R[m * D.fs + i] = (T)0; }
+    }
+}
+
+cudaError_t launch_ic_sod(int is_double, const DomDev* dom, int parity, const SodParams& P, cudaStream_t st)
+{
+    if (is_double) sod_kernel<double><<<148 * 8, 256, 0, st>>>(dom, parity, P);
+    else           sod_kernel<float><<<148 * 8, 256, 0, st>>>(dom, parity, P);
+    return cudaGetLastError();
+}
+
+// 2DSBI: post-shock state of the planar shock in Real (SimTools::
+// getPostShockRatio, with pow of Real), mixture constants in double.
+template <class Real>
+struct SbiState
+{
+    double rho1, u1, p1;            // post-shock state (from Real)
+    double G1, G2, F1, F2, eps;     // mixture constants, SimTools::EPSILON
+};
+
+template <class Real>
+static SbiState<Real> sbi_setup(const SbiParams& P, double h)
+{
+    const Real pre[3] = {(Real)P.rho, (Real)P.u, (Real)P.p};
+    const Real mach = (Real)P.mach, gamma = (Real)P.g1, pc = (Real)P.pc1;
+    Real post[3];
+    const Real m2 = std::pow(mach, (Real)2.);
+    const double mpost = std::sqrt((m2 * (gamma - 1.) + 2.) / (2. * gamma * m2 - (gamma - 1.)));
+    post[0] = (gamma + 1.) * m2 / ((gamma - 1.) * m2 + 2.) * pre[0];
+    post[2] = 1. / (gamma + 1.) * (2. * gamma * m2 - (gamma - 1.)) * pre[2];
+    const double u_pre  = mach * std::sqrt(gamma * (pc + pre[2]) / pre[0]);
+    const double u_post = mpost * std::sqrt(gamma * (pc + post[2]) / post[0]);
+    post[1] = u_pre - u_post;
+    SbiState<Real> S;
+    S.rho1 = post[0]; S.u1 = post[1]; S.p1 = post[2];
+    S.G1 = P.g1 - 1; S.G2 = P.g2 - 1; S.F1 = P.g1 * P.pc1; S.F2 = P.g2 * P.pc2;
+    S.eps = (double)(Real)P.mollfactor * std::sqrt(3.) * h;
+    return S;
+}
+
+template <class Real>
+__device__ __forceinline__ void sbi_cell(const DomDev& D, const SbiParams& P, const SbiState<Real>& S,
+                                         const double* __restrict__ bub, int nb, const int idx[3], Real v[7])
+{
+    const double p[3] = {D.h * (idx[0] + 0.5), D.h * (idx[1] + 0.5), D.h * (idx[2] + 0.5)};
+    const int a0 = P.axis0, a1 = P.axis1;
+    const Real shock = (Real)(p[a0] - P.x0) > 0 ? (Real)0 : (Real)1;
+    Real bubble = 0;
+    for (int i = 0; i < nb; ++i)
+    {
+        const double dx = p[a0] - (double)(Real)bub[4 * i + a0], dy = p[a1] - (double)(Real)bub[4 * i + a1];
+        const Real r = (Real)sqrt(dx * dx + dy * dy);
+        const Real phi = r - (Real)bub[4 * i + 3];
+        // SimTools::heaviside_smooth: cosine ramp of half-width EPSILON
+        const double x  = 0.5 * ((double)phi + S.eps) / S.eps;
+        const double mx = (0. < x) ? x : 0.;
+        const double mn = (mx < 1.) ? mx : 1.;
+        const Real alpha = (Real)(3.14159265358979323846 * mn);
+        bubble = (Real)(0.5 + 0.5 * (double)cos(alpha));
+        if (bubble > 0) break;
+    }
+    const double b = (double)bubble, s = (double)shock;
+    const Real rho = (Real)(s * S.rho1 + (double)(1 - shock) * (P.rhobubble * b + P.rho * (double)(1 - bubble)));
+    const Real mom = (Real)((s * S.u1 + (double)(1 - shock) * P.u) * (double)rho);
+    const Real G = (Real)(1. / S.G1 * (double)(1 - bubble) + 1. / S.G2 * b);
+    const Real Pc = (Real)(S.F1 / S.G1 * (double)(1 - bubble) + S.F2 / S.G2 * b);
+    const Real pressure = (Real)(s * S.p1 + (double)(1 - shock) * (P.pbubble * b + P.p * (double)(1 - bubble)));
+    const double m = (double)mom;
+    const Real ke = (Real)(0.5 * (m * m + 0. + 0.) / (double)rho);
+    v[0] = rho;
+    v[1] = a0 == 0 ? mom : (Real)0;
+    v[2] = a0 == 1 ? mom : (Real)0;
+    v[3] = a0 == 2 ? mom : (Real)0;
+    v[4] = pressure * G + Pc + ke;
+    v[5] = G;
+    v[6] = Pc;
+}
+
+// With `reverse`, every cell takes the state of its mirror image through the
+// domain centre (all three axes) with the momentum negated, except the middle
+// plane of an odd extent along the shock axis, which the reference's swap
+// loop (Sim_2DSBIMPI.cpp:196-229) leaves as it is.
+template <class Real>
+__global__ void sbi_kernel(const DomDev* dom, int parity, const SbiParams P, const SbiState<Real> S,
+                           const double* __restrict__ bub, int nb)
+{
+    const DomDev& D = *dom;
+    Real* U = (Real*)D.U[parity];
+    Real* R = (Real*)D.R;
+    const int n3[3] = {D.nx, D.ny, D.nz};
+    const long long n = (long long)D.nx * D.ny * D.nz;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+    {
+        int idx[3] = {(int)(i % D.nx), (int)((i / D.nx) % D.ny), (int)(i / ((long long)D.nx * D.ny))};
+        bool flip = false;
+        if (P.reverse && !((n3[P.axis0] & 1) && idx[P.axis0] == n3[P.axis0] / 2))
+        {
+            for (int d = 0; d < 3; ++d) idx[d] = n3[d] - 1 - idx[d];
+            flip = true;
+        }
+        Real v[7];
+        sbi_cell<Real>(D, P, S, bub, nb, idx, v);
+        if (flip) { v[1] = -v[1]; v[2] = -v[2]; v[3] = -v[3]; }
+        for (int m = 0; m < 7; ++m) { U[m * D.fs + i] = v[m]; R[m * D.fs + i] = (Real)0; }
+    }
+}
+
+cudaError_t launch_ic_sbi(int is_double, const DomDev* dom, int nx, int ny, int nz, int parity, const SbiParams& P,
+                          const double* bubbles, int nbubbles, cudaStream_t st)
+{
+    const double h = 1.0 / (double)std::max(nx, std::max(ny, nz));
+    if (is_double) sbi_kernel<double><<<148 * 8, 256, 0, st>>>(dom, parity, P, sbi_setup<double>(P, h), bubbles, nbubbles);
+    else           sbi_kernel<float><<<148 * 8, 256, 0, st>>>(dom, parity, P, sbi_setup<float>(P, h), bubbles, nbubbles);
     return cudaGetLastError();
 }
 

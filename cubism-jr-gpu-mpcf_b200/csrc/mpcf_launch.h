@@ -36,6 +36,12 @@ cudaError_t launch_sum_tiles(const DomDev* doms, int ndom, const double* tile_su
 cudaError_t launch_pack(int is_double, int kind, const DomDev* dom, int parity, int z0, int z1, void* out, cudaStream_t st);
 cudaError_t launch_unpack_save(int is_double, const DomDev* dom, int parity, int z0, int z1, const void* in, cudaStream_t st);
 
+// SteadyState, Sod and 2DSBI initial conditions (mpcf_aux.cu).
+cudaError_t launch_ic_steady(int is_double, const DomDev* dom, int parity, const SteadyParams& P, cudaStream_t st);
+cudaError_t launch_ic_sod(int is_double, const DomDev* dom, int parity, const SodParams& P, cudaStream_t st);
+cudaError_t launch_ic_sbi(int is_double, const DomDev* dom, int nx, int ny, int nz, int parity, const SbiParams& P,
+                          const double* bubbles, int nbubbles, cudaStream_t st);
+
 // Shock-induced cloud-collapse IC (mpcf_aux.cu); post4 receives the
 // post-shock rho1, u1, p1 and the shock Mach number in the state's precision.
 cudaError_t launch_sic_cloud(int is_double, const DomDev* dom, int nx, int ny, int nz, int parity,

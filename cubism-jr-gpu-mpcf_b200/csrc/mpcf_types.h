@@ -100,4 +100,19 @@ struct SicParams
     double eps;                 // interface half-width (SimTools::EPSILON; 0: sharp)
 };
 
+// Options of the reference's SteadyState, Sod and 2DSBI cases
+// (Sim_SteadyStateMPI.cpp:103-109, Sim_SodMPI.cpp:27-57, Sim_2DSBIMPI.cpp:
+// 15-58,83-96); axes are 0 = x, 1 = y, 2 = z.
+struct SteadyParams { double rho, u, v, w, p, g, pc; };
+struct SodParams
+{
+    double x0, rho1, rho2, u1, u2, p1, p2, g1, g2, pc1, pc2;
+    int reverse, axis;
+};
+struct SbiParams
+{
+    double x0, mach, rho, rhobubble, u, p, pbubble, g1, g2, pc1, pc2;
+    int reverse, mollfactor, axis0, axis1;
+};
+
 } // namespace mpcf

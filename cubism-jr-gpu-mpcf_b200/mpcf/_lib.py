@@ -53,6 +53,24 @@ class SicParams(ctypes.Structure):
                 ("g1", _D), ("g2", _D), ("pc1", _D), ("pc2", _D), ("eps", _D)]
 
 
+
+class SteadyParams(ctypes.Structure):
+    """mirror of mpcf_steady_params (Sim_SteadyStateMPI options)"""
+    _fields_ = [(k, _D) for k in ("rho", "u", "v", "w", "p", "g", "pc")]
+
+
+class SodParams(ctypes.Structure):
+    """mirror of mpcf_sod_params (Sim_SodMPI options)"""
+    _fields_ = [(k, _D) for k in ("x0", "rho1", "rho2", "u1", "u2", "p1", "p2", "g1", "g2", "pc1", "pc2")] + \
+               [("reverse", _I), ("axis", _I)]
+
+
+class SbiParams(ctypes.Structure):
+    """mirror of mpcf_sbi_params (Sim_2DSBIMPI options)"""
+    _fields_ = [(k, _D) for k in ("x0", "mach", "rho", "rhobubble", "u", "p", "pbubble", "g1", "g2", "pc1", "pc2")] + \
+               [("reverse", _I), ("mollfactor", _I), ("axis0", _I), ("axis1", _I)]
+
+
 SIGNATURES = {
     "mpcf_version": (_I, []),
     "mpcf_last_error": (_c.c_char_p, []),
@@ -83,6 +101,10 @@ SIGNATURES = {
     "mpcf_sic_default_params": (None, [_c.POINTER(SicParams)]),
     "mpcf_sic_post_shock": (_I, [_c.POINTER(SicParams), _I, _PD]),
     "mpcf_ic_sic_cloud": (_I, [_P, _I, _c.POINTER(SicParams), _I, _PD]),
+    "mpcf_case_default_params": (None, [_c.POINTER(SteadyParams), _c.POINTER(SodParams), _c.POINTER(SbiParams)]),
+    "mpcf_ic_steady": (_I, [_P, _I, _c.POINTER(SteadyParams)]),
+    "mpcf_ic_sod": (_I, [_P, _I, _c.POINTER(SodParams)]),
+    "mpcf_ic_sbi": (_I, [_P, _I, _c.POINTER(SbiParams), _I, _PD]),
     "mpcf_pack": (_I, [_P, _I, _I, _P]),
     "mpcf_unpack_save": (_I, [_P, _I, _P]),
     "mpcf_dump": (_I, [_P, _I, _I, _c.c_char_p, _c.c_char_p, _I]),

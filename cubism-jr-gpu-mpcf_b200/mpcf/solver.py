@@ -175,6 +175,21 @@ class Solver:
         check(lib().mpcf_ic_sic_cloud(self._h, dom, ctypes.byref(params), n,
                                       b.ctypes.data_as(ctypes.POINTER(ctypes.c_double)) if n else None))
 
+    def ic_steady(self, dom=0, **kw):
+        """Sim_SteadyStateMPI's uniform state (options as keywords, see case_params)."""
+        check(lib().mpcf_ic_steady(self._h, dom, ctypes.byref(case_params("steady", **kw))))
+
+    def ic_sod(self, dom=0, **kw):
+        """Sim_SodMPI's shock tube along axis (0 x, 1 y, 2 z)."""
+        check(lib().mpcf_ic_sod(self._h, dom, ctypes.byref(case_params("sod", **kw))))
+
+    def ic_sbi(self, bubbles, dom=0, **kw):
+        """Sim_2DSBIMPI's shock-bubble interaction; bubbles (n, 4) = x, y, z, r."""
+        b = np.ascontiguousarray(bubbles, dtype=np.float64).reshape(-1)
+        n = b.size // 4
+        check(lib().mpcf_ic_sbi(self._h, dom, ctypes.byref(case_params("sbi", **kw)), n,
+                                b.ctypes.data_as(ctypes.POINTER(ctypes.c_double)) if n else None))
+
     # -- output and restart (Sim_SteadyStateMPI.cpp:138-180) ---------------
     def pack(self, kind="tensor", dom=0):
         """The reference's dump ("tensor": rho, u, v, w, p, G, P, 0, 0) or save
@@ -243,6 +258,42 @@ class Solver:
         ms = ctypes.c_double()
         check(lib().mpcf_time_stages(self._h, int(reps), float(dtinvh), ctypes.byref(ms)))
         return ms.value
+
+
+CONFIG_AXES = {"xy": (0, 1), "xz": (0, 2), "yx": (1, 0), "yz": (1, 2), "zx": (2, 0), "zy": (2, 1)}
+
+
+def case_params(case, **kw):
+    """Option structure of case "steady", "sod" or "sbi" with the reference's
+    defaults, overridden by keyword (names of the reference's options; for
+    "sod" `config` = "x"|"y"|"z", for "sbi" `config` = "xy", "xz", ...)."""
+    st, so, sb = _lib.SteadyParams(), _lib.SodParams(), _lib.SbiParams()
+    lib().mpcf_case_default_params(ctypes.byref(st), ctypes.byref(so), ctypes.byref(sb))
+    p = {"steady": st, "sod": so, "sbi": sb}[case]
+    for k, v in kw.items():
+        if k == "config" and case == "sod":
+            p.axis = "xyz".index(v)
+        elif k == "config" and case == "sbi":
+            p.axis0, p.axis1 = CONFIG_AXES[v]
+        elif any(k == f[0] for f in p._fields_):
+            setattr(p, k, int(v) if k in ("reverse", "axis", "axis0", "axis1", "mollfactor") else float(v))
+        else:
+            raise KeyError(k)
+    return p
+
+
+def case_bc(case, config="xy"):
+    """Boundary conditions of the reference's lab of a case (the GPUlab*
+    _apply_bc overrides): SteadyState reflecting everywhere, Sod and the
+    cloud collapse absorbing, 2DSBI reflecting on the faces normal to the
+    second axis of its config."""
+    R, A = _lib.BC_REFLECTING, _lib.BC_ABSORBING
+    if case == "steady":
+        return (R,) * 6
+    if case in ("sod", "sic"):
+        return (A,) * 6
+    a1 = CONFIG_AXES[config][1]
+    return tuple(R if d // 2 == a1 else A for d in range(6))
 
 
 def sic_params(**kw):

@@ -220,6 +220,40 @@ void mpcf_sic_default_params(mpcf_sic_params* p);
 int mpcf_sic_post_shock(const mpcf_sic_params* p, int precision, double* post4);
 int mpcf_ic_sic_cloud(mpcf_solver* s, int dom, const mpcf_sic_params* p, int nshapes, const double* shapes4);
 
+/* ---- the reference's other cases ----------------------------------------- *
+ * Initial conditions of Sim_SteadyStateMPI (a uniform state;
+ * Sim_SteadyStateMPI.cpp:95-135), Sim_SodMPI (a two-state tube along `axis`;
+ * Sim_SodMPI.cpp:20-95) and Sim_2DSBIMPI (a planar shock of Mach number
+ * `mach` along axis0 hitting cylinders of gas with axes along the third
+ * direction, positions in the axis0/axis1 plane, interface mollified over
+ * mollfactor*sqrt(3)*h; Sim_2DSBIMPI.cpp:15-233), with the reference's
+ * rounding (FP32 bit-identical to its _FLOAT_PRECISION_ build, except the
+ * mollified 2DSBI interface, where CUDA's cosf may differ from the C
+ * library's by one unit in the last place).  Axes: 0 = x, 1 = y, 2 = z; the
+ * reference's -config strings map to (axis0, axis1) = "xy" (0,1), "xz" (0,2),
+ * "yx" (1,0), "yz" (1,2), "zx" (2,0), "zy" (2,1).  bubbles4: (x, y, z, r) per
+ * cylinder, the lines of the reference's <config>bubbles.dat.  The register is
+ * cleared.  The boundary conditions of the cases' labs are: SteadyState
+ * reflecting on all faces, Sod absorbing, 2DSBI reflecting on the axis1 faces
+ * and absorbing on the others (GPUlab2DSBI_*reflect); set them with
+ * mpcf_set_bc.  mpcf_case_default_params fills any non-NULL argument with the
+ * reference's option defaults. */
+typedef struct { double rho, u, v, w, p, g, pc; } mpcf_steady_params;      /* -rho -u -v -w -p -g -pc */
+typedef struct
+{
+    double x0, rho1, rho2, u1, u2, p1, p2, g1, g2, pc1, pc2;   /* -x0 -rho1 -rho2 -u1 -u2 -p1 -p2 -g1 -g2 -pc1 -pc2 */
+    int reverse, axis;                                          /* -reverse, -config x|y|z */
+} mpcf_sod_params;
+typedef struct
+{
+    double x0, mach, rho, rhobubble, u, p, pbubble, g1, g2, pc1, pc2;  /* -x0 -mach -rho -rhobubble -u -p -pbubble -g1 -g2 -pc1 -pc2 */
+    int reverse, mollfactor, axis0, axis1;                             /* -reverse -mollfactor -config */
+} mpcf_sbi_params;
+void mpcf_case_default_params(mpcf_steady_params* steady, mpcf_sod_params* sod, mpcf_sbi_params* sbi);
+int mpcf_ic_steady(mpcf_solver* s, int dom, const mpcf_steady_params* p);
+int mpcf_ic_sod(mpcf_solver* s, int dom, const mpcf_sod_params* p);
+int mpcf_ic_sbi(mpcf_solver* s, int dom, const mpcf_sbi_params* p, int nbubbles, const double* bubbles4);
+
 /* ---- output and restart --------------------------------------------------- *
  * The arrays of the reference's dump and save (replaces
  * Sim_SteadyStateMPI::_dump/_save/_restart, Sim_SteadyStateMPI.cpp:138-180,

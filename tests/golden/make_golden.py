@@ -12,6 +12,8 @@ It calls the reference's own code compiled from its sources (oracle/_ref):
   * source/Sim/Sim_SICCloudMPI.cpp (the shock-induced cloud-collapse IC,
     Sim_SICCloudMPI::_ic run on a 24x20x16 block),
   * source/Types.h output streamers (the arrays of the dump and the save),
+  * source/Sim/Sim_SteadyStateMPI.cpp, Sim_SodMPI.cpp, Sim_2DSBIMPI.cpp (the
+    other cases' initial conditions, run on a 24x20x16 block),
 on seeded inputs, and stores inputs and outputs as .npz fixtures next to
 this script.  The reference has no golden vectors or known-answer tests of
 its own; these fixtures are its outputs, recorded here.
@@ -191,6 +193,42 @@ def make_dump():
     np.savez_compressed(os.path.join(HERE, "ref_dump.npz"), **rec)
 
 
+CASE_SETS = [
+    ("steady", [], None, "xy"),
+    ("steady", [("-rho", 2.0), ("-u", 0.5), ("-v", 0.25), ("-w", 0.125), ("-p", 3.0), ("-g", 6.59), ("-pc", 4096.0)], None, "xy"),
+    ("steady", [("-rho", 1000.0), ("-u", 7.0), ("-p", 100.0), ("-g", 1.4), ("-pc", 0.5)], None, "xy"),
+    ("sod", [], None, "x"),
+    ("sod", [("-config", "y"), ("-reverse", 1), ("-x0", 0.3)], None, "y"),
+    ("sod", [("-config", "z"), ("-rho1", 1000.0), ("-p1", 1000.0), ("-g1", 6.59), ("-pc1", 4096.0), ("-u2", 3.0),
+             ("-rho2", 1.0), ("-p2", 1.0), ("-g2", 1.4), ("-pc2", 0.0)], None, "z"),
+    ("sbi", [("-config", "xy")], [(0.5, 0.45, 0.3, 0.15), (0.8, 0.2, 0.3, 0.08), (0.3, 0.7, 0.3, 0.1)], "xy"),
+    ("sbi", [("-config", "zx"), ("-reverse", 1), ("-mollfactor", 2), ("-x0", 0.2)],
+     [(0.4, 0.3, 0.35, 0.12), (0.7, 0.5, 0.5, 0.09)], "zx"),
+    ("sbi", [("-config", "yz"), ("-mach", 1.5), ("-rhobubble", 5.0), ("-pbubble", 1.0), ("-g2", 1.1)],
+     [(0.4, 0.45, 0.3, 0.13), (0.2, 0.6, 0.5, 0.11)], "yz"),
+]
+
+
+def make_cases():
+    """The reference's SteadyState, Sod and 2DSBI initial conditions
+    (Sim_*MPI::_ic run by oracle/ref_cases_harness.cpp on a 24x20x16 block)."""
+    import tempfile
+    L = O.ref_lib("libref_cases")
+    rec = {}
+    for i, (case, opts, bub, config) in enumerate(CASE_SETS):
+        if bub is not None:
+            bub = [tuple(float(np.float32(v)) for v in b) for b in bub]
+        with tempfile.TemporaryDirectory() as w:
+            dims, out = O.ref_case(L, case, opts, w, bubbles=bub, config=config)
+        rec[f"case{i}"] = np.array(case)
+        rec[f"opts{i}"] = np.array([f"{k}={v}" for k, v in opts])
+        rec[f"bubbles{i}"] = np.array(bub if bub is not None else np.zeros((0, 4)), np.float64)
+        rec[f"config{i}"] = np.array(config)
+        rec[f"dims{i}"] = np.array(dims)
+        rec[f"U{i}"] = np.array(out)
+    np.savez_compressed(os.path.join(HERE, "ref_cases.npz"), **rec)
+
+
 def main():
     sys.path.insert(0, os.path.join(os.path.dirname(os.path.dirname(HERE)), "cubism-jr-gpu-mpcf_b200"))
     L = O.ref_lib("libref_devmath_8x7x6")
@@ -202,6 +240,7 @@ def main():
     make_sos()
     make_sic(np.random.default_rng(20261204))
     make_dump()
+    make_cases()
     print("wrote", sorted(f for f in os.listdir(HERE) if f.endswith(".npz")))
 
 

@@ -86,6 +86,9 @@ def ref_lib(name):
         L.ref_dump_dims.argtypes = [_PI]
         L.ref_pack.argtypes = [_I, _PPF, _PF]
         L.ref_unpack_save.argtypes = [_PF, _PPF]
+    if name == "libref_cases":
+        L.ref_cases_dims.argtypes = [_PI]
+        L.ref_case_ic.argtypes = [_I, _c.c_char_p, _I, _c.POINTER(_c.c_char_p), _PPF]
     if name == "libref_sic_ic":
         L.ref_sic_dims.argtypes = [_PI]
         L.ref_sic_ic.argtypes = [_c.c_char_p, _I, _c.POINTER(_c.c_char_p), _D, _PPF, _PD]
@@ -241,3 +244,164 @@ def ref_pack(L, kind, U):
     out = np.zeros(d[0] * d[1] * d[2] * nch, np.float32)
     L.ref_pack(0 if kind == "tensor" else 1, fptrs([np.ascontiguousarray(a, np.float32) for a in U]), out.ctypes.data_as(_PF))
     return out.reshape(d[2], d[1], d[0], nch)
+
+
+# --- SteadyState / Sod / 2DSBI cases ----------------------------------------------
+CASES = {"steady": 0, "sod": 1, "sbi": 2}
+
+
+def ref_case(L, case, opts, workdir, bubbles=None, config="xy"):
+    """The reference's own case set-up (oracle/_ref/libref_cases.so) on its
+    compile-time block: opts is a list of (option, value) pairs; for "sbi"
+    the bubbles are written to <config>bubbles.dat in workdir."""
+    d = (_c.c_int * 3)()
+    L.ref_cases_dims(d)
+    n = d[0] * d[1] * d[2]
+    if bubbles is not None:
+        with open(os.path.join(workdir, f"{config}bubbles.dat"), "w") as f:
+            f.write(f"{len(bubbles)}\n")
+            for b in bubbles:
+                f.write(f"{b[0]:.9g} {b[1]:.9g} {b[2]:.9g} {b[3]:.9g}\n")
+    args = [b"case", b"-dryrun", b"1", b"-verb", b"0"]
+    for k, v in opts:
+        if isinstance(v, (int, float)) and float(v) < 0:
+            raise ValueError("negative option values cannot reach the reference's parser")
+        args += [k.encode(), str(v).encode()]
+    argv = (_c.c_char_p * len(args))(*args)
+    out = [np.zeros(n, np.float32) for _ in range(7)]
+    rc = L.ref_case_ic(CASES[case], workdir.encode(), len(args), argv, fptrs(out))
+    if rc != 0:
+        raise RuntimeError(f"ref_case_ic failed: {rc}")
+    return (d[0], d[1], d[2]), out
+
+
+_libm = None
+
+
+def _m():
+    global _libm
+    if _libm is None:
+        _libm = _c.CDLL("libm.so.6")
+        _libm.powf.restype = _F
+        _libm.powf.argtypes = [_F, _F]
+        _libm.cosf.restype = _F
+        _libm.cosf.argtypes = [_F]
+    return _libm
+
+
+def _cell_positions(dims):
+    nx, ny, nz = dims
+    h = 1.0 / max(dims)
+    iz, iy, ix = np.meshgrid(np.arange(nz), np.arange(ny), np.arange(nx), indexing="ij")
+    return h, [h * (ix.ravel() + 0.5), h * (iy.ravel() + 0.5), h * (iz.ravel() + 0.5)], [ix.ravel(), iy.ravel(), iz.ravel()]
+
+
+def case_ic(case, dims, prm, bubbles=None, dtype=np.float32):
+    """Restatement of the reference's case initial conditions:
+      "steady": Sim_SteadyStateMPI::_ic (Sim_SteadyStateMPI.cpp:103-134)
+      "sod":    Sim_SodMPI::_ic (Sim_SodMPI.cpp:27-91)
+      "sbi":    Sim_2DSBIMPI::_ic (Sim_2DSBIMPI.cpp:83-229; Real = dtype)
+    prm: dict of the mpcf_*_params fields.  Returns 7 flat fields."""
+    n = dims[0] * dims[1] * dims[2]
+    f = np.float64
+    if case == "steady":
+        r, u, v, w, p, g, pc = (prm[k] for k in ("rho", "u", "v", "w", "p", "g", "pc"))
+        G = 1.0 / (g - 1.0)
+        P = g * pc * G
+        e = G * p + P + 0.5 * r * (u * u + v * v + w * w)
+        return [np.full(n, val, dtype) for val in (r, r * u, r * v, r * w, e, G, P)]
+    h, pos, idx = _cell_positions(dims)
+    if case == "sod":
+        a = prm["axis"]
+        x = pos[a] > prm["x0"] if prm["reverse"] else pos[a] < prm["x0"]
+        xf, nf = x.astype(f), (~x).astype(f)
+        g1, g2 = prm["g1"], prm["g2"]
+        r = xf * prm["rho1"] + nf * prm["rho2"]
+        p = xf * prm["p1"] + nf * prm["p2"]
+        u = xf * prm["rho1"] * prm["u1"] + nf * prm["rho2"] * prm["u2"]
+        G = xf * 1. / (g1 - 1.) + nf * 1. / (g2 - 1.)
+        P = xf * prm["pc1"] * g1 / (g1 - 1.) + nf * prm["pc2"] * g2 / (g2 - 1.)
+        mom = [u if a == d else np.zeros(n) for d in range(3)]
+        return [a_.astype(dtype) for a_ in (r, mom[0], mom[1], mom[2], G * p + P + 0.5 * u * u / r, G, P)]
+    # 2DSBI, Real = dtype
+    T = np.dtype(dtype).type
+    L = _m()
+    pre = [T(prm["rho"]), T(prm["u"]), T(prm["p"])]
+    mach, gamma, pc = T(prm["mach"]), T(prm["g1"]), T(prm["pc1"])
+    m2 = T(L.powf(mach, T(2.))) if T is np.float32 else T(mach ** 2.0)
+    mpost = np.sqrt((f(m2) * (f(gamma) - 1.) + 2.) / (2. * f(gamma) * f(m2) - (f(gamma) - 1.)))
+    post0 = T((f(gamma) + 1.) * f(m2) / ((f(gamma) - 1.) * f(m2) + 2.) * f(pre[0]))
+    post2 = T(1. / (f(gamma) + 1.) * (2. * f(gamma) * f(m2) - (f(gamma) - 1.)) * f(pre[2]))
+    u_pre = f(mach * np.sqrt(gamma * (pc + pre[2]) / pre[0]))
+    u_post = mpost * f(np.sqrt(gamma * (pc + post2) / post0))
+    post1 = T(u_pre - u_post)
+    rho1, u1, p1 = f(post0), f(post1), f(post2)
+    G1, G2 = prm["g1"] - 1, prm["g2"] - 1
+    F1, F2 = prm["g1"] * prm["pc1"], prm["g2"] * prm["pc2"]
+    eps = f(T(prm["mollfactor"])) * np.sqrt(3.) * h
+    a0, a1 = prm["axis0"], prm["axis1"]
+    n3 = list(dims)
+    src = [i.copy() for i in idx]
+    flip = np.zeros(n, bool)
+    if prm["reverse"]:
+        mid = (idx[a0] == n3[a0] // 2) if n3[a0] % 2 else np.zeros(n, bool)
+        flip = ~mid
+        for d in range(3):
+            src[d] = np.where(flip, n3[d] - 1 - idx[d], idx[d])
+    P_ = [h * (src[d] + 0.5) for d in range(3)]
+    shock = np.where((P_[a0] - prm["x0"]).astype(T) > 0, T(0), T(1)).astype(T)
+    bubble = np.zeros(n, T)
+    done = np.zeros(n, bool)
+    cosf = np.vectorize(lambda x: L.cosf(x) if T is np.float32 else np.cos(x))
+    for b in (bubbles if bubbles is not None else []):
+        dx = P_[a0] - f(T(b[a0]))
+        dy = P_[a1] - f(T(b[a1]))
+        r = np.sqrt(dx * dx + dy * dy).astype(T)
+        phi = (r - T(b[3])).astype(T)
+        x = 0.5 * (phi.astype(f) + eps) / eps
+        mx = np.where(0. < x, x, 0.)
+        mn = np.where(mx < 1., mx, 1.)
+        alpha = (np.pi * mn).astype(T)
+        c = np.array(cosf(alpha), dtype=T) if alpha.size else alpha
+        bi = (0.5 + 0.5 * c.astype(f)).astype(T)
+        take = ~done
+        bubble = np.where(take, bi, bubble).astype(T)
+        done = done | (take & (bi > 0))
+    s, bb = shock.astype(f), bubble.astype(f)
+    one_s, one_b = (T(1) - shock).astype(f), (T(1) - bubble).astype(f)
+    rho = (s * rho1 + one_s * (prm["rhobubble"] * bb + prm["rho"] * one_b)).astype(T)
+    mom = ((s * u1 + one_s * prm["u"]) * rho.astype(f)).astype(T)
+    G = (1. / G1 * one_b + 1. / G2 * bb).astype(T)
+    P = (F1 / G1 * one_b + F2 / G2 * bb).astype(T)
+    pressure = (s * p1 + one_s * (prm["pbubble"] * bb + prm["p"] * one_b)).astype(T)
+    m = mom.astype(f)
+    ke = (0.5 * (m * m + 0. + 0.) / rho.astype(f)).astype(T)
+    E = (pressure * G + P + ke).astype(T)
+    mom = np.where(flip, -mom, mom).astype(T)
+    zero = np.zeros(n, T)
+    moms = [mom if a0 == d else zero for d in range(3)]
+    return [rho, moms[0], moms[1], moms[2], E, G, P]
+
+
+def case_prm(case, opts, config=None):
+    """mpcf_*_params fields (reference defaults) from a list of the
+    reference's (option, value) pairs."""
+    defaults = {
+        "steady": dict(rho=1.0, u=0.0, v=0.0, w=0.0, p=1.0, g=1.4, pc=0.0),
+        "sod": dict(x0=0.5, rho1=1.0, rho2=0.125, u1=0.0, u2=0.0, p1=1.0, p2=0.1, g1=1.4, g2=1.4, pc1=0.0,
+                    pc2=0.0, reverse=0, axis=0),
+        "sbi": dict(x0=0.1, mach=1.22, rho=1.0, rhobubble=0.138, u=0.0, p=1.0, pbubble=1.0, g1=1.4, g2=1.67,
+                    pc1=0.0, pc2=0.0, reverse=0, mollfactor=1, axis0=0, axis1=1),
+    }
+    prm = dict(defaults[case])
+    axes = {"xy": (0, 1), "xz": (0, 2), "yx": (1, 0), "yz": (1, 2), "zx": (2, 0), "zy": (2, 1)}
+    for k, v in opts:
+        k = k.lstrip("-")
+        if k == "config":
+            if case == "sod":
+                prm["axis"] = "xyz".index(v)
+            else:
+                prm["axis0"], prm["axis1"] = axes[v]
+        else:
+            prm[k] = type(prm[k])(v)
+    return prm
