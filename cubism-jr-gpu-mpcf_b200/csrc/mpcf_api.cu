@@ -108,6 +108,10 @@ struct mpcf_solver
     int sos_chunk = 32768, nchunks = 0;
     bool track_cons = false;
     bool sums_valid = false;
+    // the sound-speed accumulator holds the maximum of the current state,
+    // fused into the last stage of the previous step; any other change of
+    // the state clears this and the next step runs the stand-alone reduction
+    bool sos_fresh = false;
 
     // graphs of one step for the two parities
     cudaGraphExec_t graph[2] = {nullptr, nullptr};
@@ -291,13 +295,15 @@ StageArgs stage_args(mpcf_solver* s, double a, double b, bool sums)
     A.err = s->err;
     A.tile_sums = sums ? s->tile_sums : nullptr;
     A.tmaps = s->tmaps;
+    A.sos_bits = nullptr;
     return A;
 }
 
 // Enqueue one stage on the solver's stream (device dt/h) and flip parity.
-int enqueue_stage(mpcf_solver* s, double a, double b, bool sums)
+int enqueue_stage(mpcf_solver* s, double a, double b, bool sums, bool sos = false)
 {
     StageArgs A = stage_args(s, a, b, sums);
+    if (sos) A.sos_bits = s->sos_bits;
     int grid = s->ntiles;
     if (s->persist)
     {
@@ -346,14 +352,17 @@ int enqueue_dt(mpcf_solver* s, double cfl, double dt_max)
     return MPCF_OK;
 }
 
-// The whole LSRK3 step on the stream: sound speed, dt, three stages.
-int enqueue_step(mpcf_solver* s, double cfl, double dt_max)
+// The whole LSRK3 step on the stream: sound speed (the stand-alone reduction
+// when the accumulator does not hold the current state's), dt (which clears
+// the accumulator), three stages; the last stage accumulates the sound speed
+// of the state it writes, the next step's.
+int enqueue_step(mpcf_solver* s, double cfl, double dt_max, bool standalone_sos)
 {
     int rc;
-    if ((rc = enqueue_sos(s))) return rc;
+    if (standalone_sos && (rc = enqueue_sos(s))) return rc;
     if ((rc = enqueue_dt(s, cfl, dt_max))) return rc;
     for (int k = 0; k < 3; ++k)
-        if ((rc = enqueue_stage(s, kLSRK3[k][0], kLSRK3[k][1], s->track_cons && k == 2))) return rc;
+        if ((rc = enqueue_stage(s, kLSRK3[k][0], kLSRK3[k][1], s->track_cons && k == 2, k == 2))) return rc;
     return MPCF_OK;
 }
 
@@ -513,6 +522,7 @@ int mpcf_set_state(mpcf_solver* s, int dom, const void* const* state7, const voi
     if (rc) return rc;
     if (!state7) return fail(MPCF_ERR_ARG, "null state pointers");
     DeviceGuard g(s->device);
+    s->sos_fresh = false;                   // the state (or the accumulator) changes
     DomDev& D = s->hdoms[dom];
     const long long N = (long long)D.nx * D.ny * D.nz;
     if ((rc = copy_fields(s, D.U[s->parity], D.fs, N, state7, nullptr, true, src_is_device != 0))) return rc;
@@ -541,6 +551,7 @@ int mpcf_device_pointers(mpcf_solver* s, int dom, void** state7, void** reg7)
     int rc = check_dom(s, dom);
     if (rc) return rc;
     DomDev& D = s->hdoms[dom];
+    s->sos_fresh = false;   // the caller may write the state through these
     for (int q = 0; q < 7; ++q)
     {
         if (state7) state7[q] = (char*)D.U[s->parity] + (size_t)q * D.fs * s->esz;
@@ -553,6 +564,7 @@ int mpcf_max_sos(mpcf_solver* s, double* sos)
 {
     if (!s) return fail(MPCF_ERR_ARG, "null solver");
     DeviceGuard g(s->device);
+    s->sos_fresh = false;                   // the state (or the accumulator) changes
     int rc = enqueue_sos(s);
     if (rc) return rc;
     std::vector<char> buf(s->esz * s->ndom);
@@ -569,6 +581,7 @@ int mpcf_stage(mpcf_solver* s, double a, double b, const double* dtinvh)
 {
     if (!s) return fail(MPCF_ERR_ARG, "null solver");
     DeviceGuard g(s->device);
+    s->sos_fresh = false;                   // the state (or the accumulator) changes
     if (dtinvh)
     {
         CK(cudaStreamSynchronize(s->stream));   // host staging buffer reuse
@@ -590,6 +603,7 @@ int mpcf_compute_dt(mpcf_solver* s, double cfl, double dt_max, double* dt_out)
     if (!s) return fail(MPCF_ERR_ARG, "null solver");
     if (!(cfl > 0) || !(dt_max > 0)) return fail(MPCF_ERR_ARG, "cfl and dt_max must be positive");
     DeviceGuard g(s->device);
+    s->sos_fresh = false;                   // the state (or the accumulator) changes
     int rc;
     if ((rc = enqueue_sos(s))) return rc;
     if ((rc = enqueue_dt(s, cfl, dt_max))) return rc;
@@ -603,8 +617,9 @@ int mpcf_step(mpcf_solver* s, double cfl, double dt_max, double* dt_out)
     if (!s) return fail(MPCF_ERR_ARG, "null solver");
     if (!(cfl > 0) || !(dt_max > 0)) return fail(MPCF_ERR_ARG, "cfl and dt_max must be positive");
     DeviceGuard g(s->device);
-    int rc = enqueue_step(s, cfl, dt_max);
+    int rc = enqueue_step(s, cfl, dt_max, !s->sos_fresh);
     if (rc) return rc;
+    s->sos_fresh = true;
     if (dt_out)
     {
         CK(cudaMemcpyAsync(dt_out, s->dt, sizeof(double) * s->ndom, cudaMemcpyDeviceToHost, s->stream));
@@ -630,7 +645,7 @@ int mpcf_run(mpcf_solver* s, int nsteps, double cfl, double dt_max, int use_grap
             s->parity = p;
             cudaGraph_t gr = nullptr;
             CK(cudaStreamBeginCapture(s->stream, cudaStreamCaptureModeThreadLocal));
-            rc = enqueue_step(s, cfl, dt_max);
+            rc = enqueue_step(s, cfl, dt_max, false);
             cudaError_t ec = cudaStreamEndCapture(s->stream, &gr);
             s->parity = saved;
             if (rc) { if (gr) cudaGraphDestroy(gr); return rc; }
@@ -644,15 +659,20 @@ int mpcf_run(mpcf_solver* s, int nsteps, double cfl, double dt_max, int use_grap
         s->graph_cons = s->track_cons;
         for (int n = 0; n < nsteps; ++n)
         {
+            if (!s->sos_fresh && (rc = enqueue_sos(s))) return rc;
             CK(cudaGraphLaunch(s->graph[s->parity], s->stream));
             s->parity ^= 1;   // three stages: odd number of buffer swaps
+            s->sos_fresh = true;
         }
         if (nsteps > 0) s->sums_valid = s->track_cons;
     }
     else
     {
         for (int n = 0; n < nsteps; ++n)
-            if ((rc = enqueue_step(s, cfl, dt_max))) return rc;
+        {
+            if ((rc = enqueue_step(s, cfl, dt_max, !s->sos_fresh))) return rc;
+            s->sos_fresh = true;
+        }
     }
     if (time_out) CK(cudaMemcpyAsync(time_out, s->time, sizeof(double) * s->ndom, cudaMemcpyDeviceToHost, s->stream));
     CK(cudaStreamSynchronize(s->stream));
@@ -753,6 +773,7 @@ int mpcf_ic_cloud(mpcf_solver* s, int dom, const mpcf_ic_params* p, int nbubbles
     if (rc) return rc;
     if (!p || nbubbles < 0 || (nbubbles > 0 && !bubbles4)) return fail(MPCF_ERR_ARG, "bad IC arguments");
     DeviceGuard g(s->device);
+    s->sos_fresh = false;                   // the state (or the accumulator) changes
     if (nbubbles > s->bubbles_cap)
     {
         if (s->bubbles)
@@ -819,6 +840,7 @@ int mpcf_ic_sic_cloud(mpcf_solver* s, int dom, const mpcf_sic_params* p, int nsh
     for (int i = 0; i < nshapes; ++i)
         if (!(shapes4[4 * i + 3] > 0)) return fail(MPCF_ERR_ARG, "shape %d has a non-positive radius", i);
     DeviceGuard g(s->device);
+    s->sos_fresh = false;                   // the state (or the accumulator) changes
     if (nshapes > s->bubbles_cap)
     {
         if (s->bubbles)
@@ -863,6 +885,7 @@ int mpcf_ic_steady(mpcf_solver* s, int dom, const mpcf_steady_params* p)
     if (rc) return rc;
     if (!p || !(p->g > 1) || !(p->rho > 0)) return fail(MPCF_ERR_ARG, "bad SteadyState parameters");
     DeviceGuard g(s->device);
+    s->sos_fresh = false;                   // the state (or the accumulator) changes
     SteadyParams P;
     static_assert(sizeof(SteadyParams) == sizeof(mpcf_steady_params), "parameter layout");
     memcpy(&P, p, sizeof(P));
@@ -879,6 +902,7 @@ int mpcf_ic_sod(mpcf_solver* s, int dom, const mpcf_sod_params* p)
     if (!p || p->axis < 0 || p->axis > 2 || !(p->g1 > 1) || !(p->g2 > 1) || !(p->rho1 > 0) || !(p->rho2 > 0))
         return fail(MPCF_ERR_ARG, "bad Sod parameters");
     DeviceGuard g(s->device);
+    s->sos_fresh = false;                   // the state (or the accumulator) changes
     SodParams P;
     static_assert(sizeof(SodParams) == sizeof(mpcf_sod_params), "parameter layout");
     memcpy(&P, p, sizeof(P));
@@ -897,6 +921,7 @@ int mpcf_ic_sbi(mpcf_solver* s, int dom, const mpcf_sbi_params* p, int nbubbles,
         return fail(MPCF_ERR_ARG, "bad 2DSBI parameters");
     if (nbubbles < 0 || (nbubbles > 0 && !bubbles4)) return fail(MPCF_ERR_ARG, "bad bubble arguments");
     DeviceGuard g(s->device);
+    s->sos_fresh = false;                   // the state (or the accumulator) changes
     if (nbubbles > s->bubbles_cap)
     {
         if (s->bubbles)
@@ -992,6 +1017,7 @@ int mpcf_unpack_save(mpcf_solver* s, int dom, const void* host_in)
     if (rc) return rc;
     if (!host_in) return fail(MPCF_ERR_ARG, "null input");
     DeviceGuard g(s->device);
+    s->sos_fresh = false;                   // the state (or the accumulator) changes
     rc = io_run(s, dom, MPCF_DUMP_SAVE, false, [&](void* h, size_t b, size_t off) {
         memcpy(h, (const char*)host_in + off, b);
         return MPCF_OK;
@@ -1110,6 +1136,7 @@ int mpcf_restart(mpcf_solver* s, int dom, const char* dir, double* t, int* step,
         return fail(MPCF_ERR_ARG, "%s holds %ld bytes, the domain needs %zu", bin.c_str(), size, want);
     }
     DeviceGuard g(s->device);
+    s->sos_fresh = false;                   // the state (or the accumulator) changes
     rc = io_run(s, dom, MPCF_DUMP_SAVE, false, [&](void* h, size_t n, size_t) {
         return fread(h, 1, n, b) == n ? MPCF_OK : fail(MPCF_ERR_ARG, "short read from %s", bin.c_str());
     });
@@ -1212,6 +1239,7 @@ int mpcf_time_stages(mpcf_solver* s, int reps, double dtinvh, double* ms_per_sta
 {
     if (!s || reps < 1) return fail(MPCF_ERR_ARG, "bad arguments");
     DeviceGuard g(s->device);
+    s->sos_fresh = false;                   // the state (or the accumulator) changes
     std::vector<double> dv(s->ndom, dtinvh);
     CK(cudaStreamSynchronize(s->stream));
     for (int d = 0; d < s->ndom; ++d)
@@ -1242,6 +1270,7 @@ int mpcf_autotune(mpcf_solver* s, int reps, int* best3, double* best_ms)
     if (!s) return fail(MPCF_ERR_ARG, "null solver");
     if (reps < 1) reps = 3;
     DeviceGuard g(s->device);
+    s->sos_fresh = false;                   // the state (or the accumulator) changes
     CK(cudaStreamSynchronize(s->stream));
     // Trials read the current state and write the other state buffer; the
     // register is redirected to a scratch copy so the solver's state is
@@ -1359,6 +1388,7 @@ int mpcf_time_run(mpcf_solver* s, int nsteps, double cfl, double dt_max, double*
     DeviceGuard g(s->device);
     int rc = mpcf_run(s, 0, cfl, dt_max, 1, nullptr);   // builds the graphs
     if (rc) return rc;
+    if (!s->sos_fresh && (rc = enqueue_sos(s))) return rc;
     cudaEvent_t e0, e1;
     CK(cudaEventCreate(&e0));
     CK(cudaEventCreate(&e1));
@@ -1368,6 +1398,7 @@ int mpcf_time_run(mpcf_solver* s, int nsteps, double cfl, double dt_max, double*
         CK(cudaGraphLaunch(s->graph[s->parity], s->stream));
         s->parity ^= 1;
     }
+    s->sos_fresh = true;
     CK(cudaEventRecord(e1, s->stream));
     CK(cudaEventSynchronize(e1));
     float t = 0;
@@ -1383,6 +1414,7 @@ int mpcf_update(mpcf_solver* s, double b)
 {
     if (!s) return fail(MPCF_ERR_ARG, "null solver");
     DeviceGuard g(s->device);
+    s->sos_fresh = false;                   // the state (or the accumulator) changes
     CK(launch_update(s->esz == 8, s->ddoms, s->ndom, s->parity, b, s->stream));
     s->parity ^= 1;
     s->sums_valid = false;

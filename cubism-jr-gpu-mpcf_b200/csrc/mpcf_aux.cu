@@ -28,26 +28,9 @@ __device__ __forceinline__ typename Pol::T cell_sos(const typename Pol::T r, con
         const typename Pol::T v, const typename Pol::T w, const typename Pol::T e,
         const typename Pol::T G, const typename Pol::T P)
 {
-    typedef typename Pol::T T;
-    T p;
-    if (Pol::kP64)
-        p = (T)(((double)e - ((double)u*(double)u + (double)v*(double)v + (double)w*(double)w)*(0.5/(double)r) - (double)P) / (double)G);
-    else
-        p = (e - (u*u + v*v + w*w)*((T)0.5f/r) - P) / G;
-    const T c = dsqrt(((p + P) / G + p) / r);
-    return c + dmax(dmax(fabs(u), fabs(v)), fabs(w)) / r;
+    return cell_sos_rn<Pol>(r, u, v, w, e, G, P);
 }
 
-__device__ __forceinline__ void atomic_max_bits(void* p, float v)
-{
-    atomicMax((unsigned*)p, __float_as_uint(v));
-}
-__device__ __forceinline__ void atomic_max_bits(void* p, double v)
-{
-    atomicMax((unsigned long long*)p, (unsigned long long)__double_as_longlong(v));
-}
-__device__ __forceinline__ float  shfl_max(float v)  { for (int o = 16; o > 0; o >>= 1) v = fmaxf(v, __shfl_xor_sync(0xffffffffu, v, o)); return v; }
-__device__ __forceinline__ double shfl_max(double v) { for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o)); return v; }
 
 template <class Pol>
 __global__ void __launch_bounds__(256) sos_kernel(const SosArgs A)

@@ -563,4 +563,56 @@ __device__ __forceinline__ void to_primitive(const typename Pol::T c[7], typenam
     q[6] = c[6];
 }
 
+// Maximum of non-negative values through the order of their bit patterns
+// (a NaN's pattern orders above every finite value, so it surfaces).
+__device__ __forceinline__ void atomic_max_bits(void* p, float v)
+{
+    atomicMax((unsigned*)p, __float_as_uint(v));
+}
+__device__ __forceinline__ void atomic_max_bits(void* p, double v)
+{
+    atomicMax((unsigned long long*)p, (unsigned long long)__double_as_longlong(v));
+}
+__device__ __forceinline__ float  shfl_max(float v)  { for (int o = 16; o > 0; o >>= 1) v = fmaxf(v, __shfl_xor_sync(0xffffffffu, v, o)); return v; }
+__device__ __forceinline__ double shfl_max(double v) { for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o)); return v; }
+
+// Maximum characteristic speed of one cell, |u|max + c with
+//   p = (E - (ru^2+rv^2+rw^2)*(0.5/rho) - P)/G,  c = sqrt(((p+P)/G + p)/rho)
+// (GPUkernels.cu:1182-1222; the mixed policy recovers p in FP64).  Every
+// operation is an explicit round-to-nearest intrinsic, so the result is the
+// same whatever the translation unit's contraction and division flags: the
+// stand-alone reduction and the one fused into the stage kernel agree bit
+// for bit.
+template <class Pol>
+__device__ __forceinline__ typename Pol::T cell_sos_rn(const typename Pol::T r, const typename Pol::T u,
+        const typename Pol::T v, const typename Pol::T w, const typename Pol::T e,
+        const typename Pol::T G, const typename Pol::T P)
+{
+    typedef typename Pol::T T;
+    if constexpr (sizeof(T) == 8)
+    {
+        const double sq = __dadd_rn(__dadd_rn(__dmul_rn(u, u), __dmul_rn(v, v)), __dmul_rn(w, w));
+        const double p = __ddiv_rn(__dsub_rn(__dsub_rn(e, __dmul_rn(sq, __ddiv_rn(0.5, r))), P), G);
+        const double c = __dsqrt_rn(__ddiv_rn(__dadd_rn(__ddiv_rn(__dadd_rn(p, P), G), p), r));
+        return __dadd_rn(c, __ddiv_rn(fmax(fmax(fabs(u), fabs(v)), fabs(w)), r));
+    }
+    else
+    {
+        float p;
+        if constexpr (Pol::kP64)
+        {
+            const double du = u, dv = v, dw = w;
+            const double sq = __dadd_rn(__dadd_rn(__dmul_rn(du, du), __dmul_rn(dv, dv)), __dmul_rn(dw, dw));
+            p = (float)__ddiv_rn(__dsub_rn(__dsub_rn((double)e, __dmul_rn(sq, __ddiv_rn(0.5, (double)r))), (double)P), (double)G);
+        }
+        else
+        {
+            const float sq = __fadd_rn(__fadd_rn(__fmul_rn(u, u), __fmul_rn(v, v)), __fmul_rn(w, w));
+            p = __fdiv_rn(__fsub_rn(__fsub_rn(e, __fmul_rn(sq, __fdiv_rn(0.5f, r))), P), G);
+        }
+        const float c = __fsqrt_rn(__fdiv_rn(__fadd_rn(__fdiv_rn(__fadd_rn(p, P), G), p), r));
+        return __fadd_rn(c, __fdiv_rn(fmaxf(fmaxf(fabsf(u), fabsf(v)), fabsf(w)), r));
+    }
+}
+
 } // namespace mpcf

@@ -238,6 +238,7 @@ stage_kernel(const StageArgs A)
     const T factor6 = (T)1.0f / (T)6.0f;   // GPUkernels.cu:1103
     bool ok = true;
     uint32_t phA = 0, phB = 0;             // mbarrier phase parities
+    __shared__ T sos_w[TY + 1];            // per-warp maxima of the fused sound speed
     bool tma_late = false;
 
     if (TMA)
@@ -319,6 +320,8 @@ stage_kernel(const StageArgs A)
 #pragma unroll
         for (int m = 0; m < 12; ++m) zfp[m] = 0;
         double cs[5] = {0, 0, 0, 0, 0};
+        T smax = 0;              // fused sound speed of the new state (last stage)
+        bool sbad = false;
 
         for (int k = z0; k <= z1; ++k)
         {
@@ -532,6 +535,12 @@ stage_kernel(const StageArgs A)
                     Un[m * D.fs + idx] = un[m];
                 }
                 ok = ok && physical<T>(un[0], un[4], un[5], un[6]);
+                if (A.sos_bits)
+                {
+                    const T v = cell_sos_rn<Pol>(un[0], un[1], un[2], un[3], un[4], un[5], un[6]);
+                    sbad = sbad || !(v >= (T)0);   // NaN (the maximum would drop it) or negative
+                    smax = dmax(smax, v);
+                }
                 if (SUMS)
                 {
 #pragma unroll
@@ -559,6 +568,22 @@ stage_kernel(const StageArgs A)
 #pragma unroll
             for (int m = 0; m < 7; ++m) zfp[m] = zf.f[m];
             zfp[7] = zf.Gm; zfp[8] = zf.Gp; zfp[9] = zf.Pm; zfp[10] = zf.Pp; zfp[11] = zf.vel;
+        }
+
+        // ---- fused sound-speed maximum of the tile into its domain's
+        // accumulator (the stand-alone reduction's order of the bits)
+        if (A.sos_bits)
+        {
+            const bool bad = __syncthreads_or(sbad);
+            const T m = shfl_max(smax);
+            if (tx == 0) sos_w[ty] = m;
+            __syncthreads();
+            if (threadIdx.x < 32)
+            {
+                T mm = threadIdx.x < TY + 1 ? sos_w[threadIdx.x] : (T)0;
+                mm = shfl_max(mm);
+                if (threadIdx.x == 0) atomic_max_bits((char*)A.sos_bits + (size_t)d * sizeof(T), bad ? (T)NAN : mm);
+            }
         }
 
         // ---- per-tile FP64 conservation sums (deterministic: fixed order)

@@ -51,6 +51,7 @@ struct StageArgs
     unsigned* err;      // device error word
     double* tile_sums;  // [ntiles][5] FP64 partial conservation sums, or null
     const void* tmaps;  // per domain 4 CUtensorMap (128 B each): [buffer 0, 1] x [halo box, interior box]
+    void* sos_bits;     // per domain maximum sound speed of the new state (bits), or null
 };
 
 struct SosArgs

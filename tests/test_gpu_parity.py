@@ -282,3 +282,28 @@ def test_error_word_flags_nonphysical(mpcf):
         w = s.error_word(clear=True)
         assert w & mpcf._lib.ERRBIT_NONPHYSICAL
         assert s.error_word() == 0
+
+
+def test_fused_sound_speed_follows_state_changes(mpcf):
+    """The last stage of a step accumulates the next step's sound speed; a
+    state replaced between steps must be re-measured (the stand-alone
+    reduction), in graph and plain runs alike."""
+    dims = (40, 24, 16)
+    U = cloud_state(dims, nb=3)
+    U2 = cloud_state(dims, nb=1, seed=99, p_liquid=1000.0)
+    for graph in (True, False):
+        with mpcf.Solver([dims], precision="fp32_ref") as s:
+            s.set_state(U)
+            s.run(2, cfl=0.3, graph=graph)
+            s.set_state(U2)
+            s.run(2, cfl=0.3, graph=graph)
+            Ug = s.get_state(with_reg=False)
+        with mpcf.Solver([dims], precision="fp32_ref") as s1:
+            s1.set_state(U2)
+            s1.run(2, cfl=0.3, graph=not graph)
+            U1 = s1.get_state(with_reg=False)
+        Uo, Ro = [a.copy() for a in U2], [np.zeros_like(a) for a in U2]
+        for _ in range(2):
+            O.step(dims, (ABS,) * 6, Uo, Ro, cfl=0.3)
+        assert_bitwise(Ug, U1, f"graph={graph} vs fresh solver")
+        assert_bitwise(Ug, Uo, f"graph={graph} vs oracle")
