@@ -197,17 +197,26 @@ def cpu_sample(cfg_params, bub, dims, threads, U0=None):
     return 3.0 * n / dt, dt
 
 
+def sample_dims(dims, target=4 << 20):
+    """A z-slab of `dims` with about `target` cells (the whole domain when it
+    is smaller): same cell spacing, bubbles and material data."""
+    nx, ny, nz = dims
+    return (nx, ny, max(1, min(nz, -(-target // (nx * ny)))))
+
+
 def reference_arm(args):
     rank, world, _ = env_rank()
     if rank != 0:
         return 0
     import mpcf
+    sys.path.insert(0, os.path.join(REPO, "tests"))
+    import oracle_lib as O
     cores = os.cpu_count() or 1
     os.environ["OMP_NUM_THREADS"] = str(cores)
-    cfg = mpcf.configs.config(WORKLOAD)
-    # bounded sample: a 512 x 512 x 16 slab of the 512^3 cloud (same cell
-    # spacing, bubbles and material data), one full LSRK3 step per timed step
-    sub = (512, 512, 16)
+    cfg = mpcf.configs.config(args.workload)
+    # bounded sample of the workload: a z-slab of its first domain, one full
+    # LSRK3 step per timed step
+    sub = sample_dims(cfg["dims"][0])
     U0 = mpcf.ic_cloud_host(sub, cfg["params"], cfg["bubbles"][0], np.float32)
     vals = []
     for i in range(args.warmup + args.steps):
@@ -215,14 +224,28 @@ def reference_arm(args):
         if i >= args.warmup:
             vals.append(v)
     value = statistics.median(vals)
+    n_sub = sub[0] * sub[1] * sub[2]
+    ncell = sum(d[0] * d[1] * d[2] for d in cfg["dims"])
+    sample = (f"C restatement of the reference kernels (oracle/), FP32 reference rounding, one LSRK3 step of "
+              f"a {sub[0]}x{sub[1]}x{sub[2]} slab of the workload")
+    # the reference's own CPU sound speed (source/MaxSpeedOfSound.cpp, compiled
+    # from its sources into oracle/_ref, serial as written) on the same sample
+    sos = None
+    L = O.ref_lib("libref_sos")
+    if L is not None:
+        t0 = time.perf_counter()
+        reps = 3
+        for _ in range(reps):
+            L.ref_max_sos_cpp(n_sub, O.fptrs(U0))
+        sec = (time.perf_counter() - t0) / reps
+        sos = {"value": n_sub / sec, "unit": "cells/s", "cores": 1, "kind": "reference",
+               "sample": f"MaxSpeedOfSound_CPP::compute over the {sub[0]}x{sub[1]}x{sub[2]} sample"}
     line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
-            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 3.0 * 512 ** 3 / value * 1e3,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 3.0 * ncell / value * 1e3,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
-            "data": "synthetic", "config": {"workload": WORKLOAD + ": 512^3, 200-bubble cloud, liquid p=1000, "
-                                            "absorbing, CFL 0.3", "sample": "512x512x16 slab, 1 LSRK3 step"},
-            "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "port",
-                             "sample": "C restatement of the reference kernels (oracle/), FP32 reference "
-                                       "rounding, one LSRK3 step of a 512x512x16 slab of the workload"},
+            "data": "synthetic", "config": {"workload": args.workload, "sample": f"{sub[0]}x{sub[1]}x{sub[2]} slab, 1 LSRK3 step"},
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "port", "sample": sample},
+            "reference_sos_cpu": sos,
             "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
     return 0
