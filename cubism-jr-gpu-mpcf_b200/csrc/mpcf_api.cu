@@ -122,11 +122,15 @@ struct mpcf_solver
 namespace {
 
 // Tile heights with stage-kernel instances: 3 and 7 rows (CTAs of 4 and 8
-// warps: one warp per row plus the helper warp), and 15 rows (16 warps) for
-// the FP32 reference-rounding form.
+// warps: one warp per row plus the helper warp), 8 rows (8 warps, no
+// helper), and 15 rows (16 warps) for the FP32 reference-rounding form.
+// Threads of one stage CTA: a warp per row, plus the helper warp for
+// heights 2^n - 1 (TileShape in mpcf_stage.cuh).
+int stage_block_threads(int ty) { return ((ty + 1) & ty) == 0 ? 32 * (ty + 1) : 32 * ty; }
+
 bool valid_ty(const mpcf_solver* s, int ty)
 {
-    if (ty == 3 || ty == 7) return true;
+    if (ty == 3 || ty == 7 || ty == 8) return true;
     return ty == 15 && s->pol == 0;
 }
 
@@ -272,7 +276,7 @@ int persistent_grid(mpcf_solver* s, int ty)
 {
     StageKernelInfo I = stage_info(s, ty, true, false, s->tma != 0);
     int nb = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, I.fn, 32 * (ty + 1), I.smem) != cudaSuccess || nb < 1)
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, I.fn, stage_block_threads(ty), I.smem) != cudaSuccess || nb < 1)
     {
         cudaGetLastError();
         nb = 1;
@@ -479,8 +483,8 @@ int mpcf_create(mpcf_solver** out, int ndomains, const int* dims, const int* bc,
     { cudaGetLastError(); return bail(fail(MPCF_ERR_NOMEM, "cudaMallocHost failed")); }
 
     // allow the large shared-memory footprints of every tiling variant
-    const int tys[3] = {3, 7, 15};
-    for (int i = 0; i < 3; ++i)
+    const int tys[4] = {3, 7, 8, 15};
+    for (int i = 0; i < 4; ++i)
     {
         if (!valid_ty(s, tys[i])) continue;
         for (int p = 0; p < 8; ++p)
@@ -1231,7 +1235,7 @@ int mpcf_launch_shape(const mpcf_solver* s, long long* ntiles, long long* grid, 
     if (!s) return fail(MPCF_ERR_ARG, "null solver");
     if (ntiles) *ntiles = s->ntiles;
     if (grid) *grid = s->persist ? persistent_grid(const_cast<mpcf_solver*>(s), s->ty) : s->ntiles;
-    if (threads) *threads = 32 * (s->ty + 1);
+    if (threads) *threads = stage_block_threads(s->ty);
     return MPCF_OK;
 }
 
@@ -1298,8 +1302,8 @@ int mpcf_autotune(mpcf_solver* s, int reps, int* best3, double* best_ms)
         std::vector<int> dzs;
         for (int v : {16, 32, 64, 128}) if (v < maxn) dzs.push_back(v);
         dzs.push_back(maxn);
-        const int tys[3] = {3, 7, 15};
-        for (int i = 0; i < 3 && !rc; ++i)
+        const int tys[4] = {3, 7, 8, 15};
+        for (int i = 0; i < 4 && !rc; ++i)
         {
             if (!valid_ty(s, tys[i])) continue;
             for (int dz : dzs)

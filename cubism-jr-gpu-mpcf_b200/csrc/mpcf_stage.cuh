@@ -11,16 +11,17 @@
 // PCIe streaming (GPUlab.cpp:202-372,703-793); all state stays in HBM.
 //
 // Work decomposition.  A tile is 32 x TY columns in x-y and a z-chunk of
-// depth dz.  A CTA has 32*(TY+1) threads: warp w < TY owns row w, one
-// thread per column, and warp TY (the helper) owns no column.  The CTA
-// marches up the chunk one slab at a time:
+// depth dz.  Warp w < TY owns row w, one thread per column; for TY = 2^n - 1
+// a further warp (the helper) owns no column.  The CTA marches up the chunk
+// one slab at a time:
 //   * a 6-slab ring of primitives (rho,u,v,w,p,G,P) of the tile's own
 //     columns lives in shared memory (z-stencil of the z faces);
 //   * slab k with its 3-cell x/y halo is staged in `cur` (x/y stencils);
 //   * every column thread evaluates the x face at its left, the y face below
 //     it and the z face below it; the helper evaluates the 32 y faces above
 //     the tile and the TY x faces right of it, so no warp runs more than
-//     three faces per slab and none waits on a fourth at the barrier;
+//     three faces per slab and none waits on a fourth at the barrier
+//     (without a helper, warps 0 and 1 take them as a fourth job);
 //   * x/y face results go through shared memory, the z face result stays
 //     in registers for the next slab, and the cell below is finalised:
 //     rhs = a*R - dtinvh*div(F) (with the G/P extra terms), R <- rhs,
@@ -205,14 +206,24 @@ __device__ __forceinline__ void tma_load_4d(uint32_t dst, const void* tmap, int 
 #ifndef MPCF_MIN_WARPS_PER_SM
 #define MPCF_MIN_WARPS_PER_SM 16
 #endif
+// Tile heights of the form 2^n - 1 (3, 7, 15) carry a helper warp that
+// evaluates the tile's extra faces; other heights (8) give them to warps 0
+// and 1 as a fourth face job, which suits domains whose y extents are
+// multiples of 8.
+template <int TY> struct TileShape
+{
+    static constexpr bool kHelper = ((TY + 1) & TY) == 0;
+    static constexpr int kWarps = kHelper ? TY + 1 : TY;
+};
+
 template <class T, int TY> struct MinBlocks
 {
     static constexpr int w = sizeof(T) == 8 ? MPCF_MIN_WARPS_PER_SM / 2 : MPCF_MIN_WARPS_PER_SM;
-    static constexpr int v = (w / (TY + 1)) > 0 ? (w / (TY + 1)) : 1;
+    static constexpr int v = (w / TileShape<TY>::kWarps) > 0 ? (w / TileShape<TY>::kWarps) : 1;
 };
 
-// Threads of one CTA: TY column warps and the helper warp.
-template <int TY> __host__ __device__ constexpr int stage_threads() { return kTX * (TY + 1); }
+// Threads of one CTA: TY column warps and, with a helper, the helper warp.
+template <int TY> __host__ __device__ constexpr int stage_threads() { return kTX * TileShape<TY>::kWarps; }
 
 template <class Pol, int TY, bool PERSIST, bool SUMS, bool TMA>
 __global__ void __launch_bounds__(stage_threads<TY>(), MinBlocks<typename Pol::T, TY>::v)
@@ -455,9 +466,10 @@ stage_kernel(const StageArgs A)
 
             // (C) faces of slab k.  Column warps: job 0 = z face k-1/2 of the
             // own column (kept in registers), job 1 = x face left of the own
-            // cell, job 2 = y face below it.  Helper warp: job 3 = y face above
-            // the tile (row TY, lane = column), job 4 = x face right of the
-            // tile (column 32, lane = row, lanes < TY).
+            // cell, job 2 = y face below it.  Helper warp (or warps 0 and 1
+            // as a fourth job without one): job 3 = y face above the tile
+            // (row TY, lane = column), job 4 = x face right of the tile
+            // (column 32, lane = row, lanes < TY).
             // One face instance serves every job (runtime direction and
             // stencil addresses).  R and U of cell k-1 are first prefetched
             // into L1, so that the finalisation after the faces finds them.
@@ -470,12 +482,17 @@ stage_kernel(const StageArgs A)
             }
             FaceOut<T> zf;
             {
+                constexpr bool kHelper = TileShape<TY>::kHelper;
                 const int jb = row ? 0 : 3;
-                const int je = row ? ((k < z1) ? 3 : 1) : ((k < z1) ? (tx < TY ? 5 : 4) : 3);
+                int je;
+                if (kHelper) je = row ? ((k < z1) ? 3 : 1) : ((k < z1) ? (tx < TY ? 5 : 4) : 3);
+                else         je = (k < z1) ? ((ty == 0 || (ty == 1 && tx < TY)) ? 4 : 3) : 1;
                 const int zs0 = (k + 3) % 6;          // ring slot of slab k-3
 #pragma unroll 1
-                for (int job = jb; job < je; ++job)
+                for (int jb_ = jb; jb_ < je; ++jb_)
                 {
+                    // without a helper, warp 1's fourth job is the right x faces
+                    const int job = (!kHelper && jb_ == 3 && ty == 1) ? 4 : jb_;
                     int addr[6];
                     int dir, dst;
                     if (job == 0)

@@ -44,6 +44,7 @@ struct StageDispatch
         {
             case 3: return tma ? go_ty<3, true>(persist, A, grid, st) : go_ty<3, false>(persist, A, grid, st);
             case 7: return tma ? go_ty<7, true>(persist, A, grid, st) : go_ty<7, false>(persist, A, grid, st);
+            case 8: return tma ? go_ty<8, true>(persist, A, grid, st) : go_ty<8, false>(persist, A, grid, st);
             case 15:
                 if (kWithTY15)
                     return tma ? go_ty<kWithTY15 ? 15 : 7, true>(persist, A, grid, st)
@@ -59,6 +60,7 @@ struct StageDispatch
         {
             case 3: return tma ? info_ty<3, true>(persist, sums) : info_ty<3, false>(persist, sums);
             case 7: return tma ? info_ty<7, true>(persist, sums) : info_ty<7, false>(persist, sums);
+            case 8: return tma ? info_ty<8, true>(persist, sums) : info_ty<8, false>(persist, sums);
             case 15:
                 if (kWithTY15)
                     return tma ? info_ty<kWithTY15 ? 15 : 7, true>(persist, sums) : info_ty<kWithTY15 ? 15 : 7, false>(persist, sums);

@@ -288,8 +288,9 @@ int mpcf_set_time(mpcf_solver* s, int dom, double t);
 int mpcf_get_time(mpcf_solver* s, int dom, double* t);
 
 /* ---- launch configuration ------------------------------------------------- *
- * tile = 32 x ty columns x dz slabs (ty 3 or 7; 15 for MPCF_PREC_FP32_REF),
- * one CTA of 32*(ty+1) threads per tile;
+ * tile = 32 x ty columns x dz slabs (ty 3, 7 or 8; 15 also for
+ * MPCF_PREC_FP32_REF), one CTA per tile of 32*(ty+1) threads for ty = 3, 7,
+ * 15 (a helper warp evaluates the tile's extra faces) and 32*ty for ty = 8;
  * flags = MPCF_TILE_PERSISTENT | MPCF_TILE_TMA.  With MPCF_TILE_TMA, domains
  * whose rows are multiples of 16 bytes stage their slabs with bulk tensor
  * copies (other domains keep ordinary loads).  mpcf_autotune times the
