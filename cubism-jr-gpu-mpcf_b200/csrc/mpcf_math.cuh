@@ -276,6 +276,44 @@ __device__ __forceinline__ void weno_pair_packed(const float s0, const float s1,
     p = fminf(fmaxf(r.y, min3f(s2, s3, s4)), max3f(s2, s3, s4));
 }
 
+// Both edge values of one cell (fast policies), from the cell and its two
+// neighbours on either side, y0..y4 = cells l-2..l+2:
+//   R = value at the right edge l+1/2 (minus side of that face),
+//   L = value at the left edge l-1/2 (plus side of that face).
+// The Jiang-Shu smoothness indicators of the three sub-stencils
+// (l-2..l, l-1..l+1, l..l+2) integrate over cell l, so they are the same for
+// both edges (GPUonly.cuh:99-194 evaluates them again for every face): with
+//   k_j = y_j - 2 y_{j+1} + y_{j+2},  a_0 = y0-4y1+3y2, a_1 = y1-y3,
+//   a_2 = 3y2-4y3+y4,  g_j = 1/(13/3 k_j^2 + a_j^2 + 4 eps)^2
+// (the indicators times 12/3, a common factor that cancels), the two edges
+// weigh them with mirrored linear weights d = (1, 6, 3):
+//   R = (y2+y3)/2 - k1/6 + (g0 (k0-k1)/3 + g2 (k1-k2)/2) / (g0 + 6 g1 + 3 g2)
+//   L = (y2+y1)/2 - k1/6 - (g2 (k1-k2)/3 + g0 (k0-k1)/2) / (3 g0 + 6 g1 + g2)
+// and both are clipped to [min, max] of y1, y2, y3.  Lane x of every pair
+// is the right edge, lane y the left edge.
+__device__ __forceinline__ void weno_cell_packed(const float y0, const float y1, const float y2,
+                                                 const float y3, const float y4, float& R, float& L)
+{
+    constexpr float e4 = (float)(4.0 * MPCF_WENOEPS);
+    const float2 Y04 = f2(y0, y4), Y13 = f2(y1, y3), Y22 = f2s(y2);
+    const float2 K02 = fma2(Y13, f2s(-2.f), add2(Y04, Y22));                    // (k0, k2)
+    const float  k1  = fmaf(y2, -2.f, y1 + y3);
+    const float2 A02 = fma2(Y22, f2s(3.f), fma2(Y13, f2s(-4.f), Y04));          // (a0, a2)
+    const float  a1  = y1 - y3;
+    const float2 J02 = fma2(mul2(K02, f2s(13.f / 3.f)), K02, fma2(A02, A02, f2s(e4)));
+    const float  j1  = fmaf(k1 * (13.f / 3.f), k1, fmaf(a1, a1, e4));
+    const float2 G02 = rcp2(mul2(J02, J02));                                    // (g0, g2)
+    const float  g1  = rcp_approx(j1 * j1);
+    const float2 den = fma2(f2(G02.y, G02.x), f2s(3.f), fma2(f2s(g1), f2s(6.f), G02));
+    const float2 E   = mul2(G02, f2(K02.x - k1, k1 - K02.y));                   // (g0 D0, g2 D2)
+    const float2 num = fma2(E, f2(1.f / 3.f, -1.f / 3.f), mul2(f2(E.y, E.x), f2(0.5f, -0.5f)));
+    const float2 p1  = fma2(f2s(k1), f2s(-1.f / 6.f), mul2(add2(Y22, f2(y3, y1)), f2s(0.5f)));
+    const float2 r   = fma2(num, rcp2(den), p1);
+    const float lo = min3f(y1, y2, y3), hi = max3f(y1, y2, y3);
+    R = fminf(fmaxf(r.x, lo), hi);
+    L = fminf(fmaxf(r.y, lo), hi);
+}
+
 // ---------------------------------------------------------------------------
 // HLLC pieces.  sign_star in {-1,0,1}; the two weights (1+s)/2 and (1-s)/2.
 // ---------------------------------------------------------------------------

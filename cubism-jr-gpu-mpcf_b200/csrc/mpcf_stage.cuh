@@ -61,24 +61,30 @@ __host__ __device__ constexpr size_t align_up(size_t v, size_t a) { return (v + 
 // addr[j] + q*kPP with kPP a compile-time constant:
 //   plane q:  ring [6 slots][TY][32]      z-ring of the tile's own columns
 //             cur  [TY+6][38]             slab k with 3-cell x/y halos
-// Face results, 12 planes each, pitch kFP = (TY+1)*32:
-//   fx   [12][TY][33]                     x faces of slab k
-//   fy   [12][TY+1][32]                   y faces of slab k
+// Face slots, pitch kFP = (TY+1)*32, NF planes each:
+//   fx   [NF][TY][33]                     x faces of slab k
+//   fy   [NF][TY+1][32]                   y faces of slab k
+// Planes 0..11 of a slot hold the face's results (7 fluxes, G-, G+, P-, P+,
+// the extra-term velocity).  With per-cell reconstruction (fast policies)
+// NF = 14: before the fluxes, planes 0..6 hold the face's minus side and
+// planes 7..13 its plus side, and the face's evaluation overwrites them in
+// place.  Otherwise NF = 12.
 // then, in bytes: the FP64 reduction scratch [TY][5], the tile broadcast,
 // two mbarriers and, with TMA, the two staging buffers (128-byte aligned):
 //   A     [7][TY+6][40]                   halo box, x from x0-4, y from y0-3
 //   B     [7][TY][32]                     interior of a slab
-template <class T, int TY, bool TMA>
+template <class T, int TY, bool TMA, bool PC>
 struct StageLayout
 {
+    static constexpr int kNF     = PC ? 14 : 12;           // planes of a face slot
     static constexpr int kCurW   = kTX + 6;                // cur row width
     static constexpr int kRing   = TY * kTX;               // one ring slot of a plane
     static constexpr int kCurOff = 6 * kRing;              // cur inside a plane
     static constexpr int kPP     = kCurOff + (TY + 6) * kCurW;
     static constexpr int kFP     = (TY + 1) * kTX;         // >= TY * 33 for TY <= 32
     static constexpr int kFx     = 7 * kPP;
-    static constexpr int kFy     = kFx + 12 * kFP;
-    static constexpr int kEnd    = kFy + 12 * kFP;
+    static constexpr int kFy     = kFx + kNF * kFP;
+    static constexpr int kEnd    = kFy + kNF * kFP;
     static constexpr int kAW     = kTX + 8;                // staged halo box width
     static constexpr int kAH     = TY + 6;                 // staged halo box height
     static constexpr size_t kRedBytes  = align_up(kEnd * sizeof(T), 16);
@@ -230,7 +236,10 @@ __global__ void __launch_bounds__(stage_threads<TY>(), MinBlocks<typename Pol::T
 stage_kernel(const StageArgs A)
 {
     typedef typename Pol::T T;
-    typedef StageLayout<T, TY, TMA> L;
+    // per-cell reconstruction (both edge values of a cell from one set of
+    // smoothness indicators) in the fast policies; per-face otherwise
+    constexpr bool PC = Pol::kFastWeno;
+    typedef StageLayout<T, TY, TMA, PC> L;
     extern __shared__ __align__(16) unsigned char smem_dyn[];
     // 128-byte aligned base (bulk tensor copies need it for their targets)
     unsigned char* smem_raw = smem_dyn + ((128u - (smem_u32(smem_dyn) & 127u)) & 127u);
@@ -249,7 +258,7 @@ stage_kernel(const StageArgs A)
     const T factor6 = (T)1.0f / (T)6.0f;   // GPUkernels.cu:1103
     bool ok = true;
     uint32_t phA = 0, phB = 0;             // mbarrier phase parities
-    __shared__ T sos_w[TY + 1];            // per-warp maxima of the fused sound speed
+    __shared__ T sos_w[TileShape<TY>::kWarps];   // per-warp maxima of the fused sound speed
     bool tma_late = false;
 
     if (TMA)
@@ -326,6 +335,7 @@ stage_kernel(const StageArgs A)
         T Sp[7];                 // x/y part of the flux bracket of cell k-1
         T sG = 0, sP = 0, dU = 0;
         T zfp[12];               // z face (k-1)-1/2
+        T Rzp[7];                // per-cell z: right edge of cell k-1 (minus side of face k-1/2)
 #pragma unroll
         for (int m = 0; m < 7; ++m) Sp[m] = 0;
 #pragma unroll
@@ -480,7 +490,176 @@ stage_kernel(const StageArgs A)
 #pragma unroll
                 for (int m = 0; m < 7; ++m) { prefetch_l1(R + m * D.fs + idx); prefetch_l1(U + m * D.fs + idx); }
             }
+            // (E) finalisation of cell k-1 of the own column from the z face
+            // k-1/2: rhs = a*R - dtinvh*div(F) (with the G/P extra terms),
+            // R <- rhs, U_next <- b*rhs + U.  It reads only this thread's
+            // registers and global memory.
+            auto finalize = [&](const FaceOut<T>& zf)
+            {
+                T Rold[7], Uold[7];
+#pragma unroll
+                for (int m = 0; m < 7; ++m) { Rold[m] = R[m * D.fs + idx]; Uold[m] = __ldg(U + m * D.fs + idx); }
+                const T sumG = sG + (zfp[8] + zf.Gm);
+                const T sumP = sP + (zfp[10] + zf.Pm);
+                const T divU = dU + (zf.vel - zfp[11]);
+                T un[7];
+#pragma unroll
+                for (int m = 0; m < 7; ++m)
+                {
+                    T br = (Sp[m] + zf.f[m]) - zfp[m];
+                    if (m == 5) br = br - divU * sumG * factor6;
+                    if (m == 6) br = br - divU * sumP * factor6;
+                    const T rhs_m = dtinvh * br;
+                    const T rhs = a * Rold[m] - rhs_m;
+                    R[m * D.fs + idx] = rhs;
+                    un[m] = b * rhs + Uold[m];
+                    Un[m * D.fs + idx] = un[m];
+                }
+                ok = ok && physical<T>(un[0], un[4], un[5], un[6]);
+                if (A.sos_bits)
+                {
+                    const T v = cell_sos_rn<Pol>(un[0], un[1], un[2], un[3], un[4], un[5], un[6]);
+                    sbad = sbad || !(v >= (T)0);   // NaN (the maximum would drop it) or negative
+                    smax = dmax(smax, v);
+                }
+                if (SUMS)
+                {
+#pragma unroll
+                    for (int m = 0; m < 5; ++m) cs[m] += (double)un[m];
+                }
+            };
             FaceOut<T> zf;
+            if constexpr (PC)
+            {
+                // (C') per-cell reconstruction.
+                //  1. z (column threads): the right edge of cell k-1 (first
+                //     slab of a chunk only; later it is carried), both edges
+                //     of cell k, the z face k-1/2 from them, then cell k-1 is
+                //     finalised;
+                //  2. x and y edges of the own cell into the face slots: the
+                //     right / upper edge to the minus side of the face right
+                //     of / above the cell, the left / lower edge to the plus
+                //     side of the face left of / below it.  The helper warp
+                //     (warps 0..2 without one) reconstructs the ghost cells
+                //     around the tile: row -1, row TY, columns -1 and 32;
+                //  3. after a barrier, the x face left of the own cell and the
+                //     y face below it, each evaluated in place in its slot;
+                //     the helper (warps 1 and 2 without one) evaluates the y
+                //     faces above the tile and the x faces right of it.
+                constexpr bool kHelper = TileShape<TY>::kHelper;
+                if (row)
+                {
+#pragma unroll 1
+                    for (int cz = (k == z0) ? k - 1 : k; cz <= k; ++cz)
+                    {
+                        int ad[5];
+#pragma unroll
+                        for (int j = 0; j < 5; ++j) ad[j] = ((cz + 4 + j) % 6) * L::kRing + own;
+                        T Rv[7], Lv[7];
+#pragma unroll
+                        for (int q = 0; q < 7; ++q)
+                        {
+                            const T* pl = sm + q * L::kPP;
+                            weno_cell_packed(pl[ad[0]], pl[ad[1]], pl[ad[2]], pl[ad[3]], pl[ad[4]], Rv[q], Lv[q]);
+                        }
+                        if (cz == k)
+                        {
+                            // z: normal w, transverse u, v
+                            FaceState<T> S;
+                            S.rm = Rzp[0]; S.rp = Lv[0]; S.nm = Rzp[3]; S.np = Lv[3];
+                            S.t1m = Rzp[1]; S.t1p = Lv[1]; S.t2m = Rzp[2]; S.t2p = Lv[2];
+                            S.pm = Rzp[4]; S.pp = Lv[4]; S.Gm = Rzp[5]; S.Gp = Lv[5]; S.Pm = Rzp[6]; S.Pp = Lv[6];
+                            hllc_face_packed(S, 2, zf);
+                        }
+#pragma unroll
+                        for (int q = 0; q < 7; ++q) Rzp[q] = Rv[q];
+                    }
+                    if (fin) finalize(zf);
+#pragma unroll
+                    for (int m = 0; m < 7; ++m) zfp[m] = zf.f[m];
+                    zfp[7] = zf.Gm; zfp[8] = zf.Gp; zfp[9] = zf.Pm; zfp[10] = zf.Pp; zfp[11] = zf.vel;
+                }
+                if (k < z1)
+                {
+                    const int nr = row ? ((!kHelper && ty < 3) ? 3 : 2) : 3;
+#pragma unroll 1
+                    for (int j = 0; j < nr; ++j)
+                    {
+                        int base, step, dR = -1, dL = -1;
+                        if (row && j < 2)
+                        {
+                            // own cell: j = 0 x, j = 1 y
+                            base = L::kCurOff + (ty + 3) * L::kCurW + tx + 3;
+                            step = j ? L::kCurW : 1;
+                            dL = j ? L::kFy + ty * kTX + tx : L::kFx + ty * (kTX + 1) + tx;
+                            dR = j ? dL + kTX : dL + 1;
+                        }
+                        else
+                        {
+                            const int g = row ? ty : j;   // 0: row -1, 1: row TY, 2: columns -1 and 32
+                            if (g == 0)      { base = L::kCurOff + 2 * L::kCurW + tx + 3;        step = L::kCurW; dR = L::kFy + tx; }
+                            else if (g == 1) { base = L::kCurOff + (TY + 3) * L::kCurW + tx + 3; step = L::kCurW; dL = L::kFy + TY * kTX + tx; }
+                            else if (tx < TY)                { base = L::kCurOff + (tx + 3) * L::kCurW + 2;        step = 1; dR = L::kFx + tx * (kTX + 1); }
+                            else if (tx >= 16 && tx < 16 + TY) { base = L::kCurOff + (tx - 13) * L::kCurW + kTX + 3; step = 1; dL = L::kFx + (tx - 16) * (kTX + 1) + kTX; }
+                            else continue;
+                        }
+                        T Rv[7], Lv[7];
+#pragma unroll
+                        for (int q = 0; q < 7; ++q)
+                        {
+                            const T* pl = sm + q * L::kPP + base;
+                            weno_cell_packed(pl[-2 * step], pl[-step], pl[0], pl[step], pl[2 * step], Rv[q], Lv[q]);
+                        }
+                        if (dR >= 0)
+                        {
+#pragma unroll
+                            for (int q = 0; q < 7; ++q) sm[dR + q * L::kFP] = Rv[q];
+                        }
+                        if (dL >= 0)
+                        {
+#pragma unroll
+                            for (int q = 0; q < 7; ++q) sm[dL + (7 + q) * L::kFP] = Lv[q];
+                        }
+                    }
+                    __syncthreads();
+                    const int nh = row ? ((!kHelper && (ty == 1 || ty == 2)) ? 3 : 2) : 2;
+#pragma unroll 1
+                    for (int j = 0; j < nh; ++j)
+                    {
+                        int src, dir;
+                        if (row && j < 2) { dir = j; src = j ? L::kFy + ty * kTX + tx : L::kFx + ty * (kTX + 1) + tx; }
+                        else
+                        {
+                            const int g = row ? ty : j + 1;   // 1: y faces above, 2: x faces right
+                            if (g == 1) { dir = 1; src = L::kFy + TY * kTX + tx; }
+                            else
+                            {
+                                if (tx >= TY) continue;
+                                dir = 0; src = L::kFx + tx * (kTX + 1) + kTX;
+                            }
+                        }
+                        // x: normal u, transverse v, w;  y: normal v, transverse u, w
+                        T* pl = sm + src;
+                        const int nq = 1 + dir, tq = 2 - dir;
+                        FaceState<T> S;
+                        S.rm  = pl[0];              S.rp  = pl[7 * L::kFP];
+                        S.nm  = pl[nq * L::kFP];    S.np  = pl[(7 + nq) * L::kFP];
+                        S.t1m = pl[tq * L::kFP];    S.t1p = pl[(7 + tq) * L::kFP];
+                        S.t2m = pl[3 * L::kFP];     S.t2p = pl[10 * L::kFP];
+                        S.pm  = pl[4 * L::kFP];     S.pp  = pl[11 * L::kFP];
+                        S.Gm  = pl[5 * L::kFP];     S.Gp  = pl[12 * L::kFP];
+                        S.Pm  = pl[6 * L::kFP];     S.Pp  = pl[13 * L::kFP];
+                        FaceOut<T> o;
+                        hllc_face_packed(S, dir, o);
+#pragma unroll
+                        for (int m = 0; m < 7; ++m) pl[m * L::kFP] = o.f[m];
+                        pl[7 * L::kFP] = o.Gm;  pl[8 * L::kFP] = o.Gp;
+                        pl[9 * L::kFP] = o.Pm;  pl[10 * L::kFP] = o.Pp;
+                        pl[11 * L::kFP] = o.vel;
+                    }
+                }
+            }
+            else
             {
                 constexpr bool kHelper = TileShape<TY>::kHelper;
                 const int jb = row ? 0 : 3;
@@ -527,43 +706,9 @@ stage_kernel(const StageArgs A)
                     }
                 }
             }
-            // (E) finalise cell k-1 of the own column.  It reads only this
-            // thread's registers and global memory, so it runs before the
-            // barrier, while the warps with a fourth face finish it.
-            if (fin)
-            {
-                T Rold[7], Uold[7];
-#pragma unroll
-                for (int m = 0; m < 7; ++m) { Rold[m] = R[m * D.fs + idx]; Uold[m] = __ldg(U + m * D.fs + idx); }
-                const T sumG = sG + (zfp[8] + zf.Gm);
-                const T sumP = sP + (zfp[10] + zf.Pm);
-                const T divU = dU + (zf.vel - zfp[11]);
-                T un[7];
-#pragma unroll
-                for (int m = 0; m < 7; ++m)
-                {
-                    T br = (Sp[m] + zf.f[m]) - zfp[m];
-                    if (m == 5) br = br - divU * sumG * factor6;
-                    if (m == 6) br = br - divU * sumP * factor6;
-                    const T rhs_m = dtinvh * br;
-                    const T rhs = a * Rold[m] - rhs_m;
-                    R[m * D.fs + idx] = rhs;
-                    un[m] = b * rhs + Uold[m];
-                    Un[m * D.fs + idx] = un[m];
-                }
-                ok = ok && physical<T>(un[0], un[4], un[5], un[6]);
-                if (A.sos_bits)
-                {
-                    const T v = cell_sos_rn<Pol>(un[0], un[1], un[2], un[3], un[4], un[5], un[6]);
-                    sbad = sbad || !(v >= (T)0);   // NaN (the maximum would drop it) or negative
-                    smax = dmax(smax, v);
-                }
-                if (SUMS)
-                {
-#pragma unroll
-                    for (int m = 0; m < 5; ++m) cs[m] += (double)un[m];
-                }
-            }
+            // (E) finalise cell k-1 (the per-face path, after its faces and
+            // before the barrier, while the warps with a fourth face finish)
+            if (!PC && fin) finalize(zf);
 
             __syncthreads();
 
@@ -582,9 +727,12 @@ stage_kernel(const StageArgs A)
                 sP = sP + (fy[10 * L::kFP] + fy[9 * L::kFP + kTX]);
                 dU = dU + (fy[11 * L::kFP + kTX] - fy[11 * L::kFP]);
             }
+            if (!PC)
+            {
 #pragma unroll
-            for (int m = 0; m < 7; ++m) zfp[m] = zf.f[m];
-            zfp[7] = zf.Gm; zfp[8] = zf.Gp; zfp[9] = zf.Pm; zfp[10] = zf.Pp; zfp[11] = zf.vel;
+                for (int m = 0; m < 7; ++m) zfp[m] = zf.f[m];
+                zfp[7] = zf.Gm; zfp[8] = zf.Gp; zfp[9] = zf.Pm; zfp[10] = zf.Pp; zfp[11] = zf.vel;
+            }
         }
 
         // ---- fused sound-speed maximum of the tile into its domain's
@@ -597,7 +745,8 @@ stage_kernel(const StageArgs A)
             __syncthreads();
             if (threadIdx.x < 32)
             {
-                T mm = threadIdx.x < TY + 1 ? sos_w[threadIdx.x] : (T)0;
+                // every warp of the CTA wrote its slot (a helper warp its 0)
+                T mm = threadIdx.x < TileShape<TY>::kWarps ? sos_w[threadIdx.x] : (T)0;
                 mm = shfl_max(mm);
                 if (threadIdx.x == 0) atomic_max_bits((char*)A.sos_bits + (size_t)d * sizeof(T), bad ? (T)NAN : mm);
             }
@@ -634,7 +783,7 @@ stage_kernel(const StageArgs A)
     if (TMA && tma_late) atomicOr(A.err, (unsigned)ERRBIT_TMA_TIMEOUT);
 }
 
-template <class T, int TY, bool TMA>
-constexpr size_t stage_smem_bytes() { return StageLayout<T, TY, TMA>::kBytes; }
+template <class Pol, int TY, bool TMA>
+constexpr size_t stage_smem_bytes() { return StageLayout<typename Pol::T, TY, TMA, Pol::kFastWeno>::kBytes; }
 
 } // namespace mpcf

@@ -16,7 +16,7 @@ struct StageDispatch
     template <int TY, bool P, bool S, bool M>
     static cudaError_t go(const StageArgs& A, int grid, cudaStream_t st)
     {
-        stage_kernel<Pol, TY, P, S, M><<<grid, stage_threads<TY>(), stage_smem_bytes<T, TY, M>(), st>>>(A);
+        stage_kernel<Pol, TY, P, S, M><<<grid, stage_threads<TY>(), stage_smem_bytes<Pol, TY, M>(), st>>>(A);
         return cudaGetLastError();
     }
 
@@ -32,7 +32,7 @@ struct StageDispatch
     static StageKernelInfo info_ty(bool persist, bool sums)
     {
         StageKernelInfo I;
-        I.smem = stage_smem_bytes<T, TY, M>();
+        I.smem = stage_smem_bytes<Pol, TY, M>();
         if (persist) I.fn = sums ? (const void*)stage_kernel<Pol, TY, true, true, M> : (const void*)stage_kernel<Pol, TY, true, false, M>;
         else         I.fn = sums ? (const void*)stage_kernel<Pol, TY, false, true, M> : (const void*)stage_kernel<Pol, TY, false, false, M>;
         return I;

@@ -176,6 +176,50 @@ def test_ensemble_matches_single_domains(mpcf):
 # ---------------------------------------------------------------------------
 # fast FP32, mixed and FP64
 # ---------------------------------------------------------------------------
+FAST_TILINGS = [(3, 3, False, False), (3, 64, False, True), (7, 5, True, True), (7, 9, True, False),
+                (7, 64, False, True), (8, 4, True, True), (8, 64, False, False), (8, 7, True, True)]
+
+
+@pytest.mark.parametrize("prec", ["fp32", "mixed"])
+@pytest.mark.parametrize("dims", [(45, 19, 14), (44, 19, 14)])
+def test_fast_forms_every_tiling_tracks_fp64_oracle(mpcf, prec, dims):
+    """The fast forms reconstruct both edge values of a cell at once and
+    evaluate the faces in a second pass; the tile's edge cells (ghost rows and
+    columns) come from other warps than its interior.  One stage on every
+    tiling -- partial tiles, 44 (bulk copies) and 45 (ordinary loads) wide
+    rows, reflecting edges -- stays within FP32 rounding of the FP64 oracle,
+    and the tilings agree with one another bit for bit (every cell and face
+    of a direction goes through the same code whichever warp evaluates it)."""
+    bc = (ABS, REF, ABS, ABS, REF, ABS)
+    U64 = [np.asarray(a, dtype=np.float64) for a in cloud_state(dims, nb=3)]
+    U = [a.copy() for a in U64]
+    R = [np.zeros_like(a) for a in U]
+    stage = (0.0, 0.25, 0.05)
+    O.stage(dims, bc, U, R, *stage)
+    U32 = [a.astype(np.float32) for a in U64]
+    first = None
+    for tiling in FAST_TILINGS:
+        with mpcf.Solver([dims], bc=[bc], precision=prec) as s:
+            s.set_tiling(*tiling)
+            s.set_state(U32)
+            s.stage(*stage)
+            Ug, Rg = s.get_state()
+            assert s.error_word() == 0
+        # FP32 pressure recovery cancels on liquid cells (p ~ 1e2 against
+        # E, P ~ 1e4): the fast FP32 form's state is ~1e-4 off FP64 there,
+        # below the reference rounding's own ~3e-4; the mixed form recovers
+        # the pressure in FP64 and stays at FP32 rounding
+        tol_u = 2e-4 if prec == "fp32" else 2e-6
+        for q in range(7):
+            assert rel_linf(Ug[q], U[q]) <= tol_u, (tiling, q, rel_linf(Ug[q], U[q]))
+            assert rel_linf(Rg[q], R[q]) <= 2e-3, (tiling, q, rel_linf(Rg[q], R[q]))
+        if first is None:
+            first = (Ug, Rg)
+        else:
+            assert_bitwise(Ug, first[0], f"state, tiling {tiling} vs {FAST_TILINGS[0]}")
+            assert_bitwise(Rg, first[1], f"register, tiling {tiling} vs {FAST_TILINGS[0]}")
+
+
 def test_fp64_matches_fp64_oracle(mpcf):
     dims = (30, 22, 14)
     bc = (ABS, REF, ABS, ABS, REF, ABS)
@@ -283,6 +327,35 @@ def test_error_word_flags_nonphysical(mpcf):
         w = s.error_word(clear=True)
         assert w & mpcf._lib.ERRBIT_NONPHYSICAL
         assert s.error_word() == 0
+
+
+@pytest.mark.parametrize("prec", ["fp32_ref", "mixed"])
+@pytest.mark.parametrize("tiling", [(3, 64, False, True), (7, 64, True, True), (7, 5, False, False),
+                                    (8, 64, True, True), (8, 5, False, False)])
+def test_fused_sound_speed_every_tiling(mpcf, prec, tiling):
+    """Steps 2 and 3 take dt from the sound speed that the previous step's
+    last stage accumulated; a solver whose state is set again before every
+    step measures it with the stand-alone reduction instead.  Both give the
+    same dt and state bit for bit on tiles with and without a helper warp."""
+    dims = (40, 24, 16)
+    U = cloud_state(dims, nb=3)
+    with mpcf.Solver([dims], precision=prec) as s:
+        s.set_tiling(*tiling)
+        s.set_state(U)
+        dts = [s.step(cfl=0.3)[0] for _ in range(3)]
+        Uf, Rf = s.get_state()
+    dts1 = []
+    with mpcf.Solver([dims], precision=prec) as s1:
+        s1.set_tiling(*tiling)
+        s1.set_state(U)
+        for _ in range(3):
+            dts1.append(s1.step(cfl=0.3)[0])
+            st, reg = s1.get_state()
+            s1.set_state(st, reg)
+        U1, R1 = s1.get_state()
+    assert dts == dts1, (dts, dts1)
+    assert_bitwise(Uf, U1, f"fused vs stand-alone sound speed, tiling={tiling}")
+    assert_bitwise(Rf, R1, f"fused vs stand-alone sound speed, tiling={tiling}")
 
 
 def test_fused_sound_speed_follows_state_changes(mpcf):
