@@ -544,9 +544,13 @@ stage_kernel(const StageArgs A)
                 //     around the tile: row -1, row TY, columns -1 and 32;
                 //  3. after a barrier, the x face left of the own cell and the
                 //     y face below it, each evaluated in place in its slot;
-                //     the helper (warps 1 and 2 without one) evaluates the y
-                //     faces above the tile and the x faces right of it.
+                //     the helper (warps 3 and 4 without one) evaluates the y
+                //     faces above the tile and the x faces right of it.  Without
+                //     a helper no warp takes more than one of the five extra
+                //     jobs, which keeps the warps even at the barriers.
                 constexpr bool kHelper = TileShape<TY>::kHelper;
+                static_assert(TY <= 16, "ghost columns -1 and 32 take lanes 0..TY-1 and 16..15+TY");
+                static_assert(kHelper || TY >= 5, "without a helper, warps 0..4 take the extra jobs");
                 if (row)
                 {
 #pragma unroll 1
@@ -622,7 +626,7 @@ stage_kernel(const StageArgs A)
                         }
                     }
                     __syncthreads();
-                    const int nh = row ? ((!kHelper && (ty == 1 || ty == 2)) ? 3 : 2) : 2;
+                    const int nh = row ? ((!kHelper && (ty == 3 || ty == 4)) ? 3 : 2) : 2;
 #pragma unroll 1
                     for (int j = 0; j < nh; ++j)
                     {
@@ -630,7 +634,7 @@ stage_kernel(const StageArgs A)
                         if (row && j < 2) { dir = j; src = j ? L::kFy + ty * kTX + tx : L::kFx + ty * (kTX + 1) + tx; }
                         else
                         {
-                            const int g = row ? ty : j + 1;   // 1: y faces above, 2: x faces right
+                            const int g = row ? ty - 2 : j + 1;   // 1: y faces above, 2: x faces right
                             if (g == 1) { dir = 1; src = L::kFy + TY * kTX + tx; }
                             else
                             {
