@@ -102,6 +102,11 @@ struct mpcf_solver
 
     void* tmaps = nullptr;          // ndom * 4 CUtensorMap (128 B each)
 
+    // linked z-slabs (lower, upper) and their device copy
+    std::vector<int> links;         // 2 per link
+    int* dlinks = nullptr;
+    long long link_plane = 0;       // largest nx*ny of a linked domain
+
     // launch configuration
     int ty = 7, dz = 64, persist = 0, tma = 0;
     int ntiles = 0;
@@ -200,13 +205,15 @@ int encode_tensor_maps(mpcf_solver* s)
         for (int b = 0; b < 2 && ok; ++b)
             for (int box = 0; box < 2 && ok; ++box)
             {
-                const cuuint64_t dims[4] = {(cuuint64_t)D.nx, (cuuint64_t)D.ny, (cuuint64_t)D.nz, 7};
+                // over the stored planes, ghost planes included (the kernel
+                // adds zlo to its z coordinates)
+                const cuuint64_t dims[4] = {(cuuint64_t)D.nx, (cuuint64_t)D.ny, (cuuint64_t)(D.nz + D.zlo + D.zhi), 7};
                 const cuuint64_t strides[3] = {(cuuint64_t)D.nx * e, (cuuint64_t)D.nx * D.ny * e, (cuuint64_t)D.fs * e};
                 const cuuint32_t boxd[4] = {box == 0 ? 40u : 32u, (cuuint32_t)(box == 0 ? s->ty + 6 : s->ty), 1u, 7u};
                 const cuuint32_t estr[4] = {1, 1, 1, 1};
                 CUresult r = enc(&h[(size_t)d * 4 + b * 2 + box],
                                  e == 8 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32,
-                                 4, D.U[b], dims, strides, boxd, estr,
+                                 4, (char*)D.U[b] - (size_t)D.zlo * D.nx * D.ny * e, dims, strides, boxd, estr,
                                  CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
                                  CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
                 ok = (r == CUDA_SUCCESS);
@@ -242,6 +249,10 @@ int apply_tiling(mpcf_solver* s)
     int t = 0, c = 0;
     for (auto& D : s->hdoms)
     {
+        const size_t zsh = (size_t)D.zlo * D.nx * D.ny * s->esz;
+        for (int b = 0; b < 2; ++b) D.Ux[b] = (char*)D.U[b] - zsh;
+        D.Rx = (char*)D.R - zsh;
+        D.nzx = D.nz + D.zlo + D.zhi;
         D.tiles_x = (D.nx + 31) / 32;
         D.tiles_y = (D.ny + s->ty - 1) / s->ty;
         D.tiles_z = (D.nz + s->dz - 1) / s->dz;
@@ -306,6 +317,10 @@ StageArgs stage_args(mpcf_solver* s, double a, double b, bool sums)
 // Enqueue one stage on the solver's stream (device dt/h) and flip parity.
 int enqueue_stage(mpcf_solver* s, double a, double b, bool sums, bool sos = false)
 {
+    // linked slabs first take their neighbours' boundary planes of the state
+    // this stage reads
+    if (!s->links.empty())
+        CK(launch_halo((int)s->esz, s->ddoms, s->dlinks, (int)s->links.size() / 2, s->link_plane, s->parity, s->stream));
     StageArgs A = stage_args(s, a, b, sums);
     if (sos) A.sos_bits = s->sos_bits;
     int grid = s->ntiles;
@@ -352,6 +367,7 @@ int enqueue_dt(mpcf_solver* s, double cfl, double dt_max)
     A.dt = s->dt;
     A.time = s->time;
     A.err = s->err;
+    A.grouped = s->links.empty() ? 0 : 1;
     CK(launch_dt(s->pol, A, s->stream));
     return MPCF_OK;
 }
@@ -428,8 +444,12 @@ int mpcf_create(mpcf_solver** out, int ndomains, const int* dims, const int* bc,
             return fail(MPCF_ERR_ARG, "domain %d: %lld cells exceed the supported 2^34", d, (long long)nx * ny * nz);
         if (bc)
             for (int f = 0; f < 6; ++f)
-                if (bc[6 * d + f] != MPCF_BC_ABSORBING && bc[6 * d + f] != MPCF_BC_REFLECTING)
-                    return fail(MPCF_ERR_ARG, "domain %d: unknown boundary condition %d on face %d", d, bc[6 * d + f], f);
+            {
+                const int c = bc[6 * d + f];
+                if (c != MPCF_BC_ABSORBING && c != MPCF_BC_REFLECTING && !(c == MPCF_BC_HALO && f >= 4))
+                    return fail(MPCF_ERR_ARG, "domain %d: boundary condition %d not valid on face %d%s", d, c, f,
+                                c == MPCF_BC_HALO ? " (halo faces are z faces)" : "");
+            }
     }
     int ndev = 0;
     CK(cudaGetDeviceCount(&ndev));
@@ -456,10 +476,20 @@ int mpcf_create(mpcf_solver** out, int ndomains, const int* dims, const int* bc,
         D.nx = dims[3 * d]; D.ny = dims[3 * d + 1]; D.nz = dims[3 * d + 2];
         for (int f = 0; f < 6; ++f) D.bc[f] = bc ? bc[6 * d + f] : MPCF_BC_ABSORBING;
         D.h = 1.0 / (double)std::max(D.nx, std::max(D.ny, D.nz));
-        const long long N = (long long)D.nx * D.ny * D.nz;
+        D.zlo = D.bc[4] == MPCF_BC_HALO ? kHaloPlanes : 0;
+        D.zhi = D.bc[5] == MPCF_BC_HALO ? kHaloPlanes : 0;
+        D.group = d;
+        // a field holds the domain's planes plus its stored ghost planes;
+        // U[b] points at plane 0 (the register has no ghost planes)
+        const long long plane = (long long)D.nx * D.ny;
+        const long long N = plane * (D.nz + D.zlo + D.zhi);
         D.fs = (N + 63) / 64 * 64;
         for (int b = 0; b < 2; ++b)
+        {
             if ((rc = dev_alloc(s, &D.U[b], (size_t)7 * D.fs * s->esz))) return bail(rc);
+            if (cudaMemsetAsync(D.U[b], 0, (size_t)7 * D.fs * s->esz, s->stream) != cudaSuccess) return bail(fail(MPCF_ERR_CUDA, "memset"));
+            D.U[b] = (char*)D.U[b] + (size_t)D.zlo * plane * s->esz;
+        }
         if ((rc = dev_alloc(s, &D.R, (size_t)7 * D.fs * s->esz))) return bail(rc);
         if (cudaMemsetAsync(D.R, 0, (size_t)7 * D.fs * s->esz, s->stream) != cudaSuccess) return bail(fail(MPCF_ERR_CUDA, "memset"));
     }
@@ -731,11 +761,85 @@ int mpcf_set_bc(mpcf_solver* s, int dom, const int* bc6)
     if (rc) return rc;
     if (!bc6) return fail(MPCF_ERR_ARG, "null bc");
     for (int f = 0; f < 6; ++f)
-        if (bc6[f] != MPCF_BC_ABSORBING && bc6[f] != MPCF_BC_REFLECTING)
+    {
+        if (bc6[f] != MPCF_BC_ABSORBING && bc6[f] != MPCF_BC_REFLECTING && bc6[f] != MPCF_BC_HALO)
             return fail(MPCF_ERR_ARG, "unknown boundary condition %d on face %d", bc6[f], f);
+        if ((bc6[f] == MPCF_BC_HALO) != (s->hdoms[dom].bc[f] == MPCF_BC_HALO))
+            return fail(MPCF_ERR_ARG, "face %d: halo faces are fixed when the solver is created", f);
+    }
     DeviceGuard g(s->device);
     for (int f = 0; f < 6; ++f) s->hdoms[dom].bc[f] = bc6[f];
     CK(cudaMemcpyAsync(s->ddoms, s->hdoms.data(), sizeof(DomDev) * s->ndom, cudaMemcpyHostToDevice, s->stream));
+    CK(cudaStreamSynchronize(s->stream));
+    return MPCF_OK;
+}
+
+int mpcf_link_z(mpcf_solver* s, int lower, int upper)
+{
+    int rc = check_dom(s, lower);
+    if (rc) return rc;
+    if ((rc = check_dom(s, upper))) return rc;
+    if (lower == upper) return fail(MPCF_ERR_ARG, "a domain cannot be linked to itself");
+    const DomDev& L = s->hdoms[lower];
+    const DomDev& H = s->hdoms[upper];
+    if (L.bc[5] != MPCF_BC_HALO) return fail(MPCF_ERR_ARG, "domain %d: the z-right face is not a halo face", lower);
+    if (H.bc[4] != MPCF_BC_HALO) return fail(MPCF_ERR_ARG, "domain %d: the z-left face is not a halo face", upper);
+    if (L.nx != H.nx || L.ny != H.ny)
+        return fail(MPCF_ERR_ARG, "linked slabs differ in x-y size (%dx%d vs %dx%d)", L.nx, L.ny, H.nx, H.ny);
+    for (size_t i = 0; i < s->links.size(); i += 2)
+        if (s->links[i] == lower || s->links[i + 1] == upper)
+            return fail(MPCF_ERR_ARG, "face already linked (domains %d, %d)", lower, upper);
+    DeviceGuard g(s->device);
+    s->links.push_back(lower);
+    s->links.push_back(upper);
+    s->link_plane = std::max(s->link_plane, (long long)L.nx * L.ny);
+    // groups: connected components of the links, named by their lowest domain
+    std::vector<int> grp(s->ndom);
+    for (int d = 0; d < s->ndom; ++d) grp[d] = d;
+    for (bool changed = true; changed;)
+    {
+        changed = false;
+        for (size_t i = 0; i < s->links.size(); i += 2)
+        {
+            const int a = s->links[i], b = s->links[i + 1];
+            const int m = std::min(grp[a], grp[b]);
+            if (grp[a] != m || grp[b] != m) { grp[a] = grp[b] = m; changed = true; }
+        }
+    }
+    for (int d = 0; d < s->ndom; ++d) s->hdoms[d].group = grp[d];
+    if (s->dlinks)
+    {
+        cudaFree(s->dlinks);
+        s->allocs.erase(std::remove(s->allocs.begin(), s->allocs.end(), (void*)s->dlinks), s->allocs.end());
+        s->dlinks = nullptr;
+    }
+    if ((rc = dev_alloc(s, (void**)&s->dlinks, sizeof(int) * s->links.size()))) return rc;
+    CK(cudaMemcpyAsync(s->dlinks, s->links.data(), sizeof(int) * s->links.size(), cudaMemcpyHostToDevice, s->stream));
+    CK(cudaMemcpyAsync(s->ddoms, s->hdoms.data(), sizeof(DomDev) * s->ndom, cudaMemcpyHostToDevice, s->stream));
+    CK(cudaStreamSynchronize(s->stream));
+    destroy_graphs(s);               // the step now begins each stage with the exchange
+    s->sos_fresh = false;            // dt of the group comes from the stand-alone reduction
+    return MPCF_OK;
+}
+
+int mpcf_set_spacing(mpcf_solver* s, int dom, double h)
+{
+    int rc = check_dom(s, dom);
+    if (rc) return rc;
+    if (!(h > 0.0) || std::isinf(h)) return fail(MPCF_ERR_ARG, "grid spacing must be positive and finite");
+    DeviceGuard g(s->device);
+    s->hdoms[dom].h = h;
+    CK(cudaMemcpyAsync(s->ddoms, s->hdoms.data(), sizeof(DomDev) * s->ndom, cudaMemcpyHostToDevice, s->stream));
+    CK(cudaStreamSynchronize(s->stream));
+    return MPCF_OK;
+}
+
+int mpcf_exchange_halos(mpcf_solver* s)
+{
+    if (!s) return fail(MPCF_ERR_ARG, "null solver");
+    if (s->links.empty()) return MPCF_OK;
+    DeviceGuard g(s->device);
+    CK(launch_halo((int)s->esz, s->ddoms, s->dlinks, (int)s->links.size() / 2, s->link_plane, s->parity, s->stream));
     CK(cudaStreamSynchronize(s->stream));
     return MPCF_OK;
 }

@@ -74,13 +74,9 @@ __global__ void __launch_bounds__(256) sos_kernel(const SosArgs A)
 // (LSRK3_IntegratorMPI.cpp:37-38, process_all(.., dt/h) converts to Real).
 // The sound-speed accumulator is cleared for the next reduction.
 template <class Pol>
-__global__ void dt_kernel(const DtArgs A)
+__device__ __forceinline__ void dt_of_domain(const DtArgs& A, const int d, const typename Pol::T sos)
 {
     typedef typename Pol::T T;
-    const int d = blockIdx.x * blockDim.x + threadIdx.x;
-    if (d >= A.ndom) return;
-    T* bits = (T*)A.sos_bits;
-    const T sos = bits[d];
     const double h = A.doms[d].h;
     double dt = A.cfl*h/sos;
     dt = A.dt_max < dt ? A.dt_max : dt;
@@ -92,7 +88,42 @@ __global__ void dt_kernel(const DtArgs A)
     ((T*)A.dtinvh)[d] = (T)(dt/h);
     A.dt[d] = dt;
     A.time[d] += dt;
+}
+
+template <class Pol>
+__global__ void dt_kernel(const DtArgs A)
+{
+    typedef typename Pol::T T;
+    const int d = blockIdx.x * blockDim.x + threadIdx.x;
+    if (d >= A.ndom) return;
+    T* bits = (T*)A.sos_bits;
+    dt_of_domain<Pol>(A, d, bits[d]);
     bits[d] = (T)0;
+}
+
+// Linked slabs of one global domain advance with one dt: each domain takes
+// the maximum sound speed of its group (a NaN anywhere in the group stays
+// NaN and is reported), the minimum dt over the slabs as the reference's
+// MPI_Allreduce(MIN) gives it.  One block: the accumulators are cleared
+// only after every domain has read its group's.
+template <class Pol>
+__global__ void dt_group_kernel(const DtArgs A)
+{
+    typedef typename Pol::T T;
+    T* bits = (T*)A.sos_bits;
+    for (int d = threadIdx.x; d < A.ndom; d += blockDim.x)
+    {
+        const int g = A.doms[d].group;
+        T sos = bits[d];
+        for (int e = 0; e < A.ndom; ++e)
+        {
+            const T v = bits[e];
+            if (A.doms[e].group == g && sos == sos && !(v <= sos)) sos = v;
+        }
+        dt_of_domain<Pol>(A, d, sos);
+    }
+    __syncthreads();
+    for (int d = threadIdx.x; d < A.ndom; d += blockDim.x) bits[d] = (T)0;
 }
 
 cudaError_t launch_sos(int pol, const SosArgs& A, cudaStream_t st)
@@ -111,6 +142,18 @@ cudaError_t launch_sos(int pol, const SosArgs& A, cudaStream_t st)
 cudaError_t launch_dt(int pol, const DtArgs& A, cudaStream_t st)
 {
     const int g = (A.ndom + 63) / 64;
+    if (A.grouped)
+    {
+        switch (pol)
+        {
+            case 0: dt_group_kernel<PolRef32><<<1, 256, 0, st>>>(A); break;
+            case 1: dt_group_kernel<PolFast32><<<1, 256, 0, st>>>(A); break;
+            case 2: dt_group_kernel<PolMixed><<<1, 256, 0, st>>>(A); break;
+            case 3: dt_group_kernel<PolFP64><<<1, 256, 0, st>>>(A); break;
+            default: return cudaErrorInvalidValue;
+        }
+        return cudaGetLastError();
+    }
     switch (pol)
     {
         case 0: dt_kernel<PolRef32><<<g, 64, 0, st>>>(A); break;
@@ -684,7 +727,10 @@ __global__ void fill_ghosts_kernel(const DomDev* dom, int parity, T* gx, T* gy, 
         bool fx, fy, fz;
         const int mx = bc_map(cx, D.nx, D.bc0, D.bc1, fx);
         const int my = bc_map(cy, D.ny, D.bc2, D.bc3, fy);
-        const int mz = bc_map(cz, D.nz, D.bc4, D.bc5, fz);
+        // a halo face's ghost planes are stored state
+        const bool zhalo = (cz < 0 && D.bc4 == BC_HALO) || (cz >= D.nz && D.bc5 == BC_HALO);
+        const int mz = zhalo ? cz : bc_map(cz, D.nz, D.bc4, D.bc5, fz);
+        if (zhalo) fz = false;
         const long long idx = (long long)mx + (long long)D.nx * ((long long)my + (long long)D.ny * mz);
         T* dst = dir == 0 ? gx : (dir == 1 ? gy : gz);
         const long long s = dir == 0 ? sx : (dir == 1 ? sy : sz);
@@ -702,6 +748,39 @@ cudaError_t launch_fill_ghosts(int is_double, const DomDev* dom, int parity,
 {
     if (is_double) fill_ghosts_kernel<double><<<148 * 4, 256, 0, st>>>(dom, parity, (double*)gx, (double*)gy, (double*)gz);
     else           fill_ghosts_kernel<float><<<148 * 4, 256, 0, st>>>(dom, parity, (float*)gx, (float*)gy, (float*)gz);
+    return cudaGetLastError();
+}
+
+// Ghost planes of linked slabs (GPUlab::load_ghosts of a rank between two
+// neighbours, GPUlab.cpp:622-644, as device-to-device copies): for link l
+// (lower, upper) and field q, direction 0 fills the 3 planes above the lower
+// slab with planes 0..2 of the upper slab, direction 1 the 3 planes below
+// the upper slab with planes nz-3..nz-1 of the lower one.  Each block row
+// (blockIdx.y = 14 l + 7 direction + q) copies one contiguous 3-plane block.
+template <class E>
+__global__ void halo_kernel(const DomDev* doms, const int* links, int parity)
+{
+    const int l = blockIdx.y / 14, r = blockIdx.y % 14, dir = r / 7, q = r % 7;
+    const DomDev& Lo = doms[links[2 * l]];
+    const DomDev& Hi = doms[links[2 * l + 1]];
+    const long long plane = (long long)Lo.nx * Lo.ny;
+    const long long n = kHaloPlanes * plane;
+    const E* src;
+    E* dst;
+    if (dir == 0) { dst = (E*)Lo.U[parity] + q * Lo.fs + Lo.nz * plane;          src = (const E*)Hi.U[parity] + q * Hi.fs; }
+    else          { dst = (E*)Hi.U[parity] + q * Hi.fs - kHaloPlanes * plane;   src = (const E*)Lo.U[parity] + q * Lo.fs + (Lo.nz - kHaloPlanes) * plane; }
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+        dst[i] = src[i];
+}
+
+cudaError_t launch_halo(int esz, const DomDev* doms, const int* links, int nlinks, long long max_plane,
+                        int parity, cudaStream_t st)
+{
+    if (nlinks <= 0) return cudaSuccess;
+    const long long n = kHaloPlanes * max_plane;
+    const dim3 grid((unsigned)std::min<long long>((n + 255) / 256, 64), (unsigned)(14 * nlinks));
+    if (esz == 8) halo_kernel<unsigned long long><<<grid, 256, 0, st>>>(doms, links, parity);
+    else          halo_kernel<unsigned><<<grid, 256, 0, st>>>(doms, links, parity);
     return cudaGetLastError();
 }
 

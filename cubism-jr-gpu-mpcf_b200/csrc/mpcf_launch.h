@@ -53,6 +53,10 @@ cudaError_t launch_ic_cloud(int is_double, const DomDev* dom, int parity, const 
 cudaError_t launch_fill_ghosts(int is_double, const DomDev* dom, int parity,
                                void* gx, void* gy, void* gz, cudaStream_t st);
 cudaError_t launch_zero(void* p, size_t bytes, cudaStream_t st);
+// ghost planes of linked slabs: links = nlinks (lower, upper) pairs on the
+// device, max_plane = the largest nx*ny among the linked domains
+cudaError_t launch_halo(int esz, const DomDev* doms, const int* links, int nlinks, long long max_plane,
+                        int parity, cudaStream_t st);
 cudaError_t launch_update(int is_double, const DomDev* doms, int ndom, int parity, double b, cudaStream_t st);
 cudaError_t launch_fma_probe(int blocks, int iters, float* out, cudaStream_t st);
 cudaError_t launch_sum_state(const DomDev* doms, int ndom, int parity, int nchunks, int chunk, int is_double,

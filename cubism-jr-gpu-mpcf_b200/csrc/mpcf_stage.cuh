@@ -102,6 +102,8 @@ struct StageLayout
 // Boundary-condition map of one coordinate: absorbing clamps to the edge
 // cell, reflecting mirrors (-1-i on the left, 2n-1-i on the right) and
 // flips the sign of the normal momentum (BoundaryConditions.h:60-109).
+// Halo faces never reach it: the stage sees a slab with its stored ghost
+// planes as one extended domain.
 __device__ __forceinline__ int bc_map(int i, const int n, const int lo, const int hi, bool& flip)
 {
     if (i < 0)       { flip = (lo == BC_REFLECTING); i = flip ? -1 - i : 0; }
@@ -282,14 +284,18 @@ stage_kernel(const StageArgs A)
         int d = 0;
         while (d + 1 < A.ndom && A.doms[d + 1].tile_begin <= t) ++d;
         const DomDev& DD = A.doms[d];
+        // A slab with halo faces is seen as its extended domain, stored
+        // ghost planes included (planes -zlo .. nz-1+zhi become 0 ..
+        // nz+zlo+zhi-1); only its own planes zlo .. zlo+nz-1 are advanced, so
+        // no stencil ever reaches past the stored planes on a halo side.
         DomRegs D;
-        D.nx = DD.nx; D.ny = DD.ny; D.nz = DD.nz;
+        D.nx = DD.nx; D.ny = DD.ny; D.nz = DD.nzx;
         D.bc0 = DD.bc[0]; D.bc1 = DD.bc[1]; D.bc2 = DD.bc[2];
         D.bc3 = DD.bc[3]; D.bc4 = DD.bc[4]; D.bc5 = DD.bc[5];
         D.fs = DD.fs;
-        const T* __restrict__ U    = (const T*)DD.U[A.parity];
-        T* __restrict__       Un   = (T*)DD.U[A.parity ^ 1];
-        T* __restrict__       R    = (T*)DD.R;
+        const T* __restrict__ U    = (const T*)DD.Ux[A.parity];
+        T* __restrict__       Un   = (T*)DD.Ux[A.parity ^ 1];
+        T* __restrict__       R    = (T*)DD.Rx;
         const T dtinvh = ((const T*)A.dtinvh)[d];
         const bool use_tma = TMA && DD.tma_ok;
         // tensor maps of the buffer read in this stage: halo box, interior box
@@ -300,8 +306,8 @@ stage_kernel(const StageArgs A)
         const int by = (lt / DD.tiles_x) % DD.tiles_y;
         const int bz = lt / (DD.tiles_x * DD.tiles_y);
         const int x0 = bx * kTX, y0 = by * TY;
-        const int z0 = bz * A.dz;
-        const int z1 = min(z0 + A.dz, D.nz);
+        const int z0 = DD.zlo + bz * A.dz;
+        const int z1 = min(z0 + A.dz, DD.zlo + DD.nz);
         const int gx = x0 + tx, gy = y0 + ty;
         const bool row = ty < TY;          // a column thread (not the helper)
         const bool valid = row && (gx < D.nx) && (gy < D.ny);

@@ -10,7 +10,11 @@ namespace mpcf {
 // Boundary condition codes per face (x-left, x-right, y-left, y-right,
 // z-left, z-right).  Absorbing = zeroth-order extrapolation, reflecting =
 // mirror with the normal momentum negated (BoundaryConditions.h:60-109).
-enum { BC_ABSORBING = 0, BC_REFLECTING = 1 };
+// Halo (z faces only) = the 3 ghost planes are stored state, filled from a
+// neighbouring slab of the same global domain (GridMPI.h:65-106 and the
+// halo exchange of GPUlab.cpp:622-644).
+enum { BC_ABSORBING = 0, BC_REFLECTING = 1, BC_HALO = 2 };
+constexpr int kHaloPlanes = 3;
 
 // Bits of the device error word.
 enum {
@@ -21,7 +25,10 @@ enum {
 
 // One domain as the kernels see it.  All 7 fields of a buffer live in one
 // allocation with a field stride `fs` (elements, a multiple of 64), cell
-// (ix,iy,iz) at ix + nx*(iy + ny*iz) inside a field (Types.h:31).
+// (ix,iy,iz) at ix + nx*(iy + ny*iz) inside a field (Types.h:31).  With
+// halo faces the state buffers hold zlo planes below plane 0 and zhi above
+// plane nz-1 (U[b] points at plane 0, iz runs over -zlo .. nz-1+zhi); the
+// register has no ghost planes.
 struct DomDev
 {
     void*  U[2];        // ping-pong state buffers (T*), 7 fields each
@@ -34,6 +41,14 @@ struct DomDev
     int    sos_chunk_begin;   // first global sound-speed chunk of this domain
     int    sos_chunks;
     int    tma_ok;      // 1: tensor maps of this domain are valid (rows of 16-byte multiples)
+    int    zlo, zhi;    // stored ghost planes below z = 0 / above z = nz-1 (0 or 3, halo faces)
+    // the extended domain the stage kernel sees: planes -zlo .. nz-1+zhi as
+    // 0 .. nzx-1 (Ux/Rx = U/R shifted back by zlo planes; the register is
+    // only ever read at the domain's own planes)
+    void*  Ux[2];
+    void*  Rx;
+    int    nzx;
+    int    group;       // domains of one group (z-slabs of a global domain) share one dt
     double h;
 };
 
@@ -74,6 +89,7 @@ struct DtArgs
     double* dt;         // [ndom]
     double* time;       // [ndom], accumulated
     unsigned* err;
+    int    grouped;     // some domains share a group (linked slabs): dt from the group's maximum
 };
 
 // Bubble-cloud initial condition (liquid with gas bubbles, tanh-smoothed

@@ -19,6 +19,7 @@ PRECISIONS = {"fp32_ref": PREC_FP32_REF, "fp32": PREC_FP32, "mixed": PREC_MIXED,
 
 BC_ABSORBING = 0
 BC_REFLECTING = 1
+BC_HALO = 2          # z faces of slabs: ghost planes filled from the neighbouring slab
 
 ERR_ARG, ERR_CUDA, ERR_NOMEM, ERR_STATE, ERR_NUMERIC = -1, -2, -3, -4, -5
 DUMP_TENSOR = 0
@@ -95,6 +96,9 @@ SIGNATURES = {
     "mpcf_error_word": (_I, [_P, _c.POINTER(_c.c_uint), _I]),
     "mpcf_set_bc": (_I, [_P, _I, _PI]),
     "mpcf_fill_ghosts": (_I, [_P, _I, _P, _P, _P, _I]),
+    "mpcf_link_z": (_I, [_P, _I, _I]),
+    "mpcf_set_spacing": (_I, [_P, _I, _D]),
+    "mpcf_exchange_halos": (_I, [_P]),
     "mpcf_ic_cloud": (_I, [_P, _I, _c.POINTER(IcParams), _I, _PD]),
     "mpcf_ic_cloud_host": (_I, [_I, _I, _I, _c.POINTER(IcParams), _I, _PD, _I, _PP]),
     "mpcf_bubbles": (_I, [_c.c_ulonglong, _I, _D, _D, _PD, _PD, _D, _I, _PD]),

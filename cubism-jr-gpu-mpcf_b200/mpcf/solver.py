@@ -151,6 +151,19 @@ class Solver:
     def set_bc(self, bc6, dom=0):
         check(lib().mpcf_set_bc(self._h, dom, (ctypes.c_int * 6)(*bc6)))
 
+    # -- z-slab decomposition ----------------------------------------------
+    def link_z(self, lower, upper):
+        """Domain `upper` sits on top of domain `lower` (mpcf_link_z): every
+        stage refreshes their facing ghost planes on the device, and the
+        linked slabs share one dt."""
+        check(lib().mpcf_link_z(self._h, lower, upper))
+
+    def set_spacing(self, h, dom=0):
+        check(lib().mpcf_set_spacing(self._h, dom, float(h)))
+
+    def exchange_halos(self):
+        check(lib().mpcf_exchange_halos(self._h))
+
     def fill_ghosts(self, dom=0):
         nx, ny, nz = self.dims[dom]
         gx = np.empty(2 * 7 * 3 * ny * nz, self.dtype)

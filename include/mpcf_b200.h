@@ -17,7 +17,8 @@
  *   double for MPCF_PREC_FP64.
  * Boundary conditions, per domain, 6 ints in the order
  *   x-left, x-right, y-left, y-right, z-left, z-right
- *   (MPCF_BC_ABSORBING / MPCF_BC_REFLECTING, BoundaryConditions.h:60-109).
+ *   (MPCF_BC_ABSORBING / MPCF_BC_REFLECTING, BoundaryConditions.h:60-109;
+ *   MPCF_BC_HALO on z faces of slabs, see the decomposition section).
  *
  * Threading: one host thread per solver at a time.  All work of a solver is
  * ordered on its own CUDA stream; calls that return host data synchronise it.
@@ -42,6 +43,7 @@ typedef struct mpcf_solver mpcf_solver;
 /* boundary conditions */
 #define MPCF_BC_ABSORBING  0
 #define MPCF_BC_REFLECTING 1
+#define MPCF_BC_HALO       2   /* z faces only: ghost planes filled from a neighbouring slab */
 
 /* status codes */
 #define MPCF_OK            0
@@ -176,6 +178,38 @@ int mpcf_error_word(mpcf_solver* s, unsigned* word, int clear);
  *   right (layer 0 innermost). */
 int mpcf_set_bc(mpcf_solver* s, int dom, const int* bc6);
 int mpcf_fill_ghosts(mpcf_solver* s, int dom, void* gx, void* gy, void* gz, int dst_is_device);
+
+/* ---- z-slab domain decomposition ------------------------------------------ *
+ * The reference spreads a global domain over MPI ranks (GridMPI.h:65-106),
+ * refreshes 3-cell halos before every stage (GPUlab::load_ghosts,
+ * GPUlab.cpp:622-644) and takes the minimum dt over ranks
+ * (LSRK3_IntegratorMPI.cpp:40).  Here a global domain is cut into z-slabs.
+ * A slab's z face towards a neighbouring slab is MPCF_BC_HALO (given to
+ * mpcf_create; z faces only, fixed for the solver's life): its state buffers
+ * then hold 3 ghost planes beyond that face, which the stage reads as stored
+ * state.  mpcf_device_pointers returns the address of plane 0 of each field;
+ * plane z of field q (-3 <= z < 0 below the slab, nz <= z < nz+3 above it)
+ * is at state7[q] + z*nx*ny elements.  Before every stage the ghost planes
+ * must hold the current state of the neighbour's boundary planes (planes
+ * nz-3..nz-1 of the slab below, planes 0..2 of the slab above).
+ *
+ * mpcf_link_z: slabs in one solver (one GPU): domain `upper` sits on top of
+ *   domain `lower` (same nx and ny, halo faces towards each other).  Every
+ *   stage then first copies the boundary planes between linked slabs on the
+ *   device (inside the captured step graph too), and linked slabs share one
+ *   dt from the largest sound speed among them.  A chain of linked slabs
+ *   advances bit-identically to the undivided domain.
+ * mpcf_set_spacing: grid spacing h of a domain (default 1/max(nx,ny,nz),
+ *   NodeBlock.h:71); a slab takes its global domain's 1/max(NX,NY,NZ).
+ * mpcf_exchange_halos: the device copies between linked slabs, on demand
+ *   (every stage does them anyway).
+ * Slabs on different GPUs exchange through the caller (NCCL send/recv of
+ *   the 3-plane blocks, e.g. the Python driver mpcf/decomp.py): per step,
+ *   mpcf_max_sos, the maximum over ranks, dt = min(cfl*h/sos, dt_max), then
+ *   per stage the exchange and mpcf_stage with dtinvh = dt/h. */
+int mpcf_link_z(mpcf_solver* s, int lower, int upper);
+int mpcf_set_spacing(mpcf_solver* s, int dom, double h);
+int mpcf_exchange_halos(mpcf_solver* s);
 
 /* ---- initial conditions --------------------------------------------------- */
 /* device generator: state of domain dom from the cloud IC, register cleared */

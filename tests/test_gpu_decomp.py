@@ -1,0 +1,150 @@
+"""z-slab decomposition on the GPU: linked slabs of one solver (ghost planes
+copied on the device inside every stage, one dt for the group) and the
+per-rank driver's halo views, both bit-identical to the undivided domain."""
+import numpy as np
+import pytest
+
+import mpcf.decomp as dc
+from conftest import cloud_state
+from test_gpu_parity import assert_bitwise
+
+pytestmark = pytest.mark.gpu
+
+ABS, REF = 0, 1
+DIMS = (40, 24, 30)
+BC = (ABS, REF, ABS, ABS, REF, ABS)
+
+
+def _state(prec, mpcf):
+    dt = mpcf.dtype_of(mpcf.PRECISIONS[prec])
+    return [np.asarray(a, dtype=dt) for a in cloud_state(DIMS, nb=3)]
+
+
+def _undivided(mpcf, prec, U0, steps, graph, tiling=None):
+    with mpcf.Solver([DIMS], bc=[BC], precision=prec) as s:
+        if tiling:
+            s.set_tiling(*tiling)
+        s.set_state(U0)
+        t = s.run(steps, cfl=0.3, graph=graph)
+        return t, s.get_state()
+
+
+@pytest.mark.parametrize("prec", ["fp32_ref", "mixed", "fp64"])
+@pytest.mark.parametrize("nslabs,graph", [(2, True), (3, False), (4, True)])
+def test_linked_slabs_match_undivided_domain(mpcf, prec, nslabs, graph):
+    U0 = _state(prec, mpcf)
+    t_ref, (U_ref, R_ref) = _undivided(mpcf, prec, U0, 3, graph)
+    s, ext = dc.slab_solver(DIMS, nslabs, bc=BC, precision=prec)
+    with s:
+        dc.scatter_state(s, DIMS, ext, U0)
+        t = s.run(3, cfl=0.3, graph=graph)
+        U, R = dc.gather_state(s, ext)
+        assert s.error_word() == 0
+    assert list(t) == [t_ref[0]] * nslabs, (t, t_ref)
+    assert_bitwise(U, U_ref, f"state, {nslabs} slabs")
+    assert_bitwise(R, R_ref, f"register, {nslabs} slabs")
+
+
+@pytest.mark.parametrize("tiling", [(3, 4, False, False), (7, 64, True, True), (8, 5, True, True), (8, 64, False, False)])
+def test_linked_slabs_every_tiling(mpcf, tiling):
+    """Ghost planes are read by the bulk-copy staging and the ordinary loads
+    alike (rows of 40 floats qualify for bulk copies), with chunks that
+    start and end next to a ghost plane."""
+    prec = "mixed"
+    U0 = _state(prec, mpcf)
+    t_ref, (U_ref, R_ref) = _undivided(mpcf, prec, U0, 2, True, tiling)
+    s, ext = dc.slab_solver(DIMS, 3, bc=BC, precision=prec)
+    with s:
+        s.set_tiling(*tiling)
+        dc.scatter_state(s, DIMS, ext, U0)
+        s.run(2, cfl=0.3, graph=True)
+        U, R = dc.gather_state(s, ext)
+    assert_bitwise(U, U_ref, f"state, tiling {tiling}")
+    assert_bitwise(R, R_ref, f"register, tiling {tiling}")
+
+
+def test_halo_faces_are_validated(mpcf):
+    with pytest.raises(mpcf.MpcfError):
+        mpcf.Solver([(16, 16, 8)], bc=[(mpcf.BC_HALO, ABS, ABS, ABS, ABS, ABS)])   # x faces cannot be halos
+    with mpcf.Solver([(16, 16, 8), (16, 16, 8), (16, 12, 8)],
+                     bc=[(ABS,) * 5 + (mpcf.BC_HALO,), (ABS,) * 4 + (mpcf.BC_HALO, ABS),
+                         (ABS,) * 4 + (mpcf.BC_HALO, ABS)]) as s:
+        with pytest.raises(mpcf.MpcfError):
+            s.link_z(1, 0)                  # domain 1's upper face is not a halo face
+        with pytest.raises(mpcf.MpcfError):
+            s.link_z(0, 2)                  # x-y sizes differ
+        with pytest.raises(mpcf.MpcfError):
+            s.set_bc((ABS,) * 6, dom=0)     # halo faces are fixed
+        s.link_z(0, 1)
+        with pytest.raises(mpcf.MpcfError):
+            s.link_z(0, 1)                  # already linked
+
+
+def test_rank_driver_halo_views(mpcf):
+    """Two SlabRank slabs in one process, their ghost planes filled through
+    the driver's torch views of the device buffers (as NCCL would fill them),
+    stage by stage with the undivided domain's dt: bit-identical."""
+    import torch
+    prec = "fp32_ref"
+    U0 = _state(prec, mpcf)
+    h = dc.global_spacing(DIMS)
+    ranks = [dc.SlabRank(DIMS, bc=BC, precision=prec, rank=r, nranks=2) for r in range(2)]
+    try:
+        for r in ranks:
+            r.set_global_state(U0)
+        with mpcf.Solver([DIMS], bc=[BC], precision=prec) as ref:
+            ref.set_state(U0)
+            for _ in range(2):
+                sos = max(r.solver.max_sos()[0] for r in ranks)
+                assert sos == ref.max_sos()[0]
+                dt = min(0.3 * h / sos, 1e30)
+                for a, b in mpcf.LSRK3:
+                    lo, hi = ranks[0].plane_blocks(), ranks[1].plane_blocks()
+                    for q in range(7):
+                        hi[2][q].copy_(lo[1][q])          # rank 1's lower ghosts <- rank 0's top planes
+                        lo[3][q].copy_(hi[0][q])          # rank 0's upper ghosts <- rank 1's bottom planes
+                    torch.cuda.synchronize()
+                    for r in ranks:
+                        r.solver.stage(a, b, [dt / h])
+                    ref.stage(a, b, [dt / h])
+            U_ref, R_ref = ref.get_state()
+        parts = [r.get_state() for r in ranks]
+        U = [np.concatenate([p[0][q] for p in parts]) for q in range(7)]
+        R = [np.concatenate([p[1][q] for p in parts]) for q in range(7)]
+        assert_bitwise(U, U_ref, "state")
+        assert_bitwise(R, R_ref, "register")
+    finally:
+        for r in ranks:
+            r.close()
+
+
+def test_single_rank_driver_matches_step(mpcf):
+    """The rank driver's host dt (maximum over a one-rank NCCL group) and
+    per-stage calls reproduce mpcf_step bit for bit."""
+    import datetime
+    import os
+    import socket
+    import torch.distributed as dist
+    sk = socket.socket()
+    sk.bind(("127.0.0.1", 0))
+    port = sk.getsockname()[1]
+    sk.close()
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("nccl", rank=0, world_size=1, timeout=datetime.timedelta(seconds=60))
+    try:
+        prec = "mixed"
+        U0 = _state(prec, mpcf)
+        with dc.SlabRank(DIMS, bc=BC, precision=prec, dist=dist) as r:
+            r.set_global_state(U0)
+            dts = [r.step(0.3) for _ in range(3)]
+            U, R = r.get_state()
+        with mpcf.Solver([DIMS], bc=[BC], precision=prec) as s:
+            s.set_state(U0)
+            dts_ref = [s.step(cfl=0.3)[0] for _ in range(3)]
+            U_ref, R_ref = s.get_state()
+        assert dts == dts_ref, (dts, dts_ref)
+        assert_bitwise(U, U_ref, "state")
+        assert_bitwise(R, R_ref, "register")
+    finally:
+        dist.destroy_process_group()
