@@ -154,47 +154,47 @@ __device__ __forceinline__ typename Pol::T weno_pluss_clipped(const typename Pol
     return dmin(dmax(r, mn), mx);
 }
 
-// Both reconstructions of one face from its 6-cell stencil s0..s5, in the
-// fast policies: the smoothness indicators are the same Jiang-Shu
-// polynomials as the reference's expanded forms (beta_f, beta_h, beta_g
-// above; the coefficients agree term by term), evaluated in factored form
-//   beta_f = 13/12 (x-2y+z)^2 + 1/4 (x-4y+3z)^2
-//   beta_h = 13/12 (x-2y+z)^2 + 1/4 (x-z)^2
-//   beta_g = 13/12 (x-2y+z)^2 + 1/4 (3x-4y+z)^2
-// so the curvature term of each of the four windows the face touches is
-// computed once and shared by the minus and plus sides, and no term
-// cancels catastrophically (the expanded form cancels ~1e4-sized products
-// down to ~1e-6 on smooth liquid stencils in FP32).
+// Both edge values of one cell in the reference-rounding policies, from the
+// cells y0..y4 = l-2..l+2: R = weno_minus_clipped(y0..y4), the minus side of
+// face l+1/2, and L = weno_pluss_clipped(y0..y4), the plus side of face
+// l-1/2.  The two evaluate the same three indicator calls --
+// beta_f(y0,y1,y2), beta_h(y1,y2,y3), beta_g(y2,y3,y4) -- with the same
+// double-precision 1/(10 (beta+eps)^2) of each and the same clip bounds;
+// those are evaluated once here, and every other operation is the one of
+// the two functions above in their order, so R and L are bit-identical to
+// them (GPUonly.cuh:99-194).
 template <class Pol>
-__device__ __forceinline__ void weno_pair_factored(const typename Pol::T s0, const typename Pol::T s1,
-        const typename Pol::T s2, const typename Pol::T s3, const typename Pol::T s4, const typename Pol::T s5,
-        typename Pol::T& m, typename Pol::T& p)
+__device__ __forceinline__ void weno_cell_ref(const typename Pol::T y0, const typename Pol::T y1,
+        const typename Pol::T y2, const typename Pol::T y3, const typename Pol::T y4,
+        typename Pol::T& R, typename Pol::T& L)
 {
     typedef typename Pol::T T;
-    const T c1312 = (T)(13. / 12.), c14 = (T)0.25;
-    // curvature of windows (s0,s1,s2) .. (s3,s4,s5)
-    const T k0 = s0 - (T)2 * s1 + s2;
-    const T k1 = s1 - (T)2 * s2 + s3;
-    const T k2 = s2 - (T)2 * s3 + s4;
-    const T k3 = s3 - (T)2 * s4 + s5;
-    const T K0 = c1312 * k0 * k0, K1 = c1312 * k1 * k1, K2 = c1312 * k2 * k2, K3 = c1312 * k3 * k3;
-    // minus side: f(s0,s1,s2), h(s1,s2,s3), g(s2,s3,s4)
+    static_assert(!Pol::kFastWeno, "reference-rounding policies only");
+    const T pf = beta_f<T>(y0, y1, y2) + (T)MPCF_WENOEPS;
+    const T ph = beta_h<T>(y1, y2, y3) + (T)MPCF_WENOEPS;
+    const T pg = beta_g<T>(y2, y3, y4) + (T)MPCF_WENOEPS;
+    // the 10.0 literal promotes these to double (GPUonly.cuh:111-113)
+    const double qf = ((T)1)/(10.0*pf*pf);
+    const double qh = ((T)1)/(10.0*ph*ph);
+    const double qg = ((T)1)/(10.0*pg*pg);
+    const T a1 = (T)((T)(6)*qh);
+    const T lo = dmin(dmin(y1, y2), y3);
+    const T hi = dmax(dmax(y1, y2), y3);
     {
-        const T a = s0 - (T)4 * s1 + (T)3 * s2, b = s1 - s3, c = (T)3 * s2 - (T)4 * s3 + s4;
-        const T is0 = K0 + c14 * a * a, is1 = K1 + c14 * b * b, is2 = K2 + c14 * c * c;
-        T w0, w1, w2;
-        weno_weights<Pol>(is0, is1, is2, w0, w1, w2);
-        const T r = w0*((T)(1.0/3.)*s0-(T)(7./6.)*s1+(T)(11./6.)*s2) + w1*(-(T)(1./6.)*s1+(T)(5./6.)*s2+(T)(1./3.)*s3) + w2*((T)(1./3.)*s2+(T)(5./6.)*s3-(T)(1./6.)*s4);
-        m = dmin(dmax(r, dmin(dmin(s1, s2), s3)), dmax(dmax(s1, s2), s3));
+        // minus side: indicators (f, h, g)
+        const T a0 = (T)((T)(1)*qf), a2 = (T)((T)(3)*qg);
+        const T inv = ((T)1)/(a0 + a1 + a2);
+        const T w0 = a0 * inv, w1 = a1 * inv, w2 = 1 - w0 - w1;
+        const T r = w0*((T)(1.0/3.)*y0-(T)(7./6.)*y1+(T)(11./6.)*y2) + w1*(-(T)(1./6.)*y1+(T)(5./6.)*y2+(T)(1./3.)*y3) + w2*((T)(1./3.)*y2+(T)(5./6.)*y3-(T)(1./6.)*y4);
+        R = dmin(dmax(r, lo), hi);
     }
-    // plus side: g(s3,s4,s5), h(s2,s3,s4), f(s1,s2,s3)
     {
-        const T a = (T)3 * s3 - (T)4 * s4 + s5, b = s2 - s4, c = s1 - (T)4 * s2 + (T)3 * s3;
-        const T is0 = K3 + c14 * a * a, is1 = K2 + c14 * b * b, is2 = K1 + c14 * c * c;
-        T w0, w1, w2;
-        weno_weights<Pol>(is0, is1, is2, w0, w1, w2);
-        const T r = w0*((T)(1./3.)*s5-(T)(7./6.)*s4+(T)(11./6.)*s3) + w1*(-(T)(1./6.)*s4+(T)(5./6.)*s3+(T)(1./3.)*s2) + w2*((T)(1./3.)*s3+(T)(5./6.)*s2-(T)(1./6.)*s1);
-        p = dmin(dmax(r, dmin(dmin(s2, s3), s4)), dmax(dmax(s2, s3), s4));
+        // plus side: indicators (g, h, f)
+        const T a0 = (T)((T)(1)*qg), a2 = (T)((T)(3)*qf);
+        const T inv = ((T)1)/(a0 + a1 + a2);
+        const T w0 = a0 * inv, w1 = a1 * inv, w2 = 1 - w0 - w1;
+        const T r = w0*((T)(1./3.)*y4-(T)(7./6.)*y3+(T)(11./6.)*y2) + w1*(-(T)(1./6.)*y3+(T)(5./6.)*y2+(T)(1./3.)*y1) + w2*((T)(1./3.)*y2+(T)(5./6.)*y1-(T)(1./6.)*y0);
+        L = dmin(dmax(r, lo), hi);
     }
 }
 
@@ -226,54 +226,6 @@ __device__ __forceinline__ float max3f(const float a, const float b, const float
     float r;
     asm("max.f32 %0, %1, %2, %3;" : "=f"(r) : "f"(a), "f"(b), "f"(c));
     return r;
-}
-
-// Both reconstructions of one face (fast policies) as one packed pair.
-// The plus side is the mirror image of the minus side: with
-//   lane x (minus): (x0..x4) = (s0, s1, s2, s3, s4)
-//   lane y (plus):  (x0..x4) = (s5, s4, s3, s2, s1)
-// both lanes evaluate the same expressions (GPUonly.cuh:99-194):
-//   is0 = 13/12 k0^2 + 1/4 (x0-4x1+3x2)^2,  k0 = x0-2x1+x2
-//   is1 = 13/12 k1^2 + 1/4 (x1-x3)^2,       k1 = x1-2x2+x3
-//   is2 = 13/12 k2^2 + 1/4 (3x2-4x3+x4)^2,  k2 = x2-2x3+x4
-//   p0 = (2x0-7x1+11x2)/6, p1 = (-x1+5x2+2x3)/6, p2 = (2x2+5x3-x4)/6
-//   r  = (a0 p0 + a1 p1 + a2 p2) / (a0 + a1 + a2),  a_k = d_k/(is_k+eps)^2,
-//   d = (1, 6, 3)
-// with the smoothness indicators in the factored, cancellation-free form
-// (the same polynomials as the reference's expanded beta_f / beta_h /
-// beta_g, coefficient by coefficient).  The candidate differences are the
-// curvature differences p0 - p1 = (k0-k1)/3 and p2 - p1 = (k1-k2)/6, so
-//   r = p1 + (b0 (k0-k1) + b2 (k1-k2)) / (3 b0 + b1 + 6 b2),
-//   b = (a0/3, a1, a2/6) = (1/3, 6, 1/2) / (is+eps)^2 up to a common factor,
-// and each b_k is the reciprocal square of i_k = c_k (13 k^2 + 3 a^2 +
-// 12 eps) with c = (sqrt 3, 1/sqrt 6, sqrt 2).  Each lane is then clipped
-// to [min, max] of its three central cells.
-__device__ __forceinline__ void weno_pair_packed(const float s0, const float s1, const float s2,
-                                                 const float s3, const float s4, const float s5,
-                                                 float& m, float& p)
-{
-    constexpr double e12 = 12.0 * MPCF_WENOEPS;
-    constexpr float c0 = 1.7320508075688772f, c1 = 0.40824829046386302f, c2 = 1.4142135623730951f;
-    const float2 X = f2(s0, s5), Y = f2(s1, s4), Z = f2(s2, s3), W = f2(s3, s2), V = f2(s4, s1);
-    const float2 k0 = fma2(Y, f2s(-2.f), add2(X, Z));
-    const float2 k1 = fma2(Z, f2s(-2.f), add2(Y, W));
-    const float2 k2 = fma2(W, f2s(-2.f), add2(Z, V));
-    const float2 a0 = fma2(Z, f2s(3.f), fma2(Y, f2s(-4.f), X));
-    const float2 a1 = sub2(Y, W);
-    const float2 a2 = fma2(Z, f2s(3.f), fma2(W, f2s(-4.f), V));
-    const float2 i0 = fma2(mul2(k0, f2s(13.f * c0)), k0, fma2(mul2(a0, f2s(3.f * c0)), a0, f2s((float)(e12 * 1.7320508075688772))));
-    const float2 i1 = fma2(mul2(k1, f2s(13.f * c1)), k1, fma2(mul2(a1, f2s(3.f * c1)), a1, f2s((float)(e12 * 0.40824829046386302))));
-    const float2 i2 = fma2(mul2(k2, f2s(13.f * c2)), k2, fma2(mul2(a2, f2s(3.f * c2)), a2, f2s((float)(e12 * 1.4142135623730951))));
-    const float2 b0 = rcp2(mul2(i0, i0));
-    const float2 b1 = rcp2(mul2(i1, i1));
-    const float2 b2 = rcp2(mul2(i2, i2));
-    const float2 inv = rcp2(fma2(b2, f2s(6.f), fma2(b0, f2s(3.f), b1)));
-    const float2 num = fma2(b0, sub2(k0, k1), mul2(b2, sub2(k1, k2)));
-    // p1 = (x2 + x3)/2 - k1/6
-    const float2 p1 = fma2(k1, f2s(-1.f / 6.f), mul2(add2(Z, W), f2s(0.5f)));
-    const float2 r = fma2(num, inv, p1);
-    m = fminf(fmaxf(r.x, min3f(s1, s2, s3)), max3f(s1, s2, s3));
-    p = fminf(fmaxf(r.y, min3f(s2, s3, s4)), max3f(s2, s3, s4));
 }
 
 // Both edge values of one cell (fast policies), from the cell and its two
@@ -512,40 +464,20 @@ __device__ __forceinline__ void hllc_face_packed(const FaceState<float>& S, cons
     o.Gm = S.Gm; o.Gp = S.Gp; o.Pm = S.Pm; o.Pp = S.Pp;
 }
 
-// Full face from primitives in shared memory: cell j (j = 0..5 for cells
-// i-3..i+2 around face i-1/2) of primitive plane q sits at
-// sm[addr[j] + q*PP].  PP, the plane pitch, is a compile-time constant, so
-// every plane's six loads share the six addresses (immediate offsets).  The
-// velocity planes are reconstructed in (u, v, w) order and permuted by `dir`
-// into (normal, first transverse, second transverse) as the reference
-// passes them to the HLLC functions (x: u,v,w; y: v,u,w; z: w,u,v).
-template <class Pol, int PP>
-__device__ __forceinline__ void face_flux(const typename Pol::T* __restrict__ sm, const int (&addr)[6],
-                                          const int dir, FaceOut<typename Pol::T>& o)
+// Both edge values of one cell in the policy's arithmetic.
+template <class Pol>
+__device__ __forceinline__ void weno_cell(const typename Pol::T y0, const typename Pol::T y1,
+        const typename Pol::T y2, const typename Pol::T y3, const typename Pol::T y4,
+        typename Pol::T& R, typename Pol::T& L)
 {
-    typedef typename Pol::T T;
-    FaceState<T> S;
-    T m1, p1, m2, p2, m3, p3;
-#define MPCF_RECON(q, M, P) { \
-        const T s0 = sm[addr[0] + (q) * PP], s1 = sm[addr[1] + (q) * PP], s2 = sm[addr[2] + (q) * PP], \
-                s3 = sm[addr[3] + (q) * PP], s4 = sm[addr[4] + (q) * PP], s5 = sm[addr[5] + (q) * PP]; \
-        if constexpr (Pol::kFastWeno) weno_pair_packed(s0, s1, s2, s3, s4, s5, M, P); \
-        else { M = weno_minus_clipped<Pol>(s0, s1, s2, s3, s4); \
-               P = weno_pluss_clipped<Pol>(s1, s2, s3, s4, s5); } }
-    MPCF_RECON(0, S.rm, S.rp);
-    MPCF_RECON(1, m1, p1);
-    MPCF_RECON(2, m2, p2);
-    MPCF_RECON(3, m3, p3);
-    MPCF_RECON(4, S.pm, S.pp);
-    MPCF_RECON(5, S.Gm, S.Gp);
-    MPCF_RECON(6, S.Pm, S.Pp);
-#undef MPCF_RECON
-    S.nm  = dir == 0 ? m1 : (dir == 1 ? m2 : m3);
-    S.np  = dir == 0 ? p1 : (dir == 1 ? p2 : p3);
-    S.t1m = dir == 0 ? m2 : m1;
-    S.t1p = dir == 0 ? p2 : p1;
-    S.t2m = dir == 2 ? m2 : m3;
-    S.t2p = dir == 2 ? p2 : p3;
+    if constexpr (Pol::kFastWeno) weno_cell_packed(y0, y1, y2, y3, y4, R, L);
+    else                          weno_cell_ref<Pol>(y0, y1, y2, y3, y4, R, L);
+}
+
+// Wave speeds and fluxes of one face in the policy's arithmetic.
+template <class Pol>
+__device__ __forceinline__ void face_hllc(const FaceState<typename Pol::T>& S, const int dir, FaceOut<typename Pol::T>& o)
+{
     if constexpr (Pol::kFastWeno) hllc_face_packed(S, dir, o);
     else                          hllc_face<Pol>(S, dir, o);
 }

@@ -17,15 +17,22 @@
 //   * a 6-slab ring of primitives (rho,u,v,w,p,G,P) of the tile's own
 //     columns lives in shared memory (z-stencil of the z faces);
 //   * slab k with its 3-cell x/y halo is staged in `cur` (x/y stencils);
-//   * every column thread evaluates the x face at its left, the y face below
-//     it and the z face below it; the helper evaluates the 32 y faces above
-//     the tile and the TY x faces right of it, so no warp runs more than
-//     three faces per slab and none waits on a fourth at the barrier
-//     (without a helper, warps 0 and 1 take them as a fourth job);
-//   * x/y face results go through shared memory, the z face result stays
-//     in registers for the next slab, and the cell below is finalised:
-//     rhs = a*R - dtinvh*div(F) (with the G/P extra terms), R <- rhs,
-//     U_next <- b*rhs + U.
+//   * reconstruction is per cell: the three WENO5 smoothness indicators of
+//     a cell serve both its edge values (the minus side of the face right
+//     of it and the plus side of the face left of it), in every direction;
+//   * z: every column thread reconstructs its cell k, evaluates the z face
+//     k-1/2 from the carried upper edge of cell k-1, and finalises cell
+//     k-1: rhs = a*R - dtinvh*div(F) (with the G/P extra terms),
+//     R <- rhs, U_next <- b*rhs + U;
+//   * x, y: every column thread writes its cell's edge values into the face
+//     slots in shared memory; the helper warp (warps 0..4 without one)
+//     reconstructs the ghost cells around the tile (rows -1 and TY,
+//     columns -1 and 32); after a barrier each face is evaluated in place
+//     in its slot, the x face left of every cell and the y face below it
+//     by the cell's thread, the faces above and right of the tile by the
+//     helper, so no warp takes more than one extra job per slab;
+//   * after a second barrier every cell gathers its x/y flux differences,
+//     carried to its finalisation in the next slab.
 // Each cell is converted to primitives once per stage (the reference
 // converts the six stencil cells again at every face).  The state is
 // ping-ponged (read U[parity], write U[parity^1]) so neighbouring tiles
@@ -73,10 +80,10 @@ __host__ __device__ constexpr size_t align_up(size_t v, size_t a) { return (v + 
 // two mbarriers and, with TMA, the two staging buffers (128-byte aligned):
 //   A     [7][TY+6][40]                   halo box, x from x0-4, y from y0-3
 //   B     [7][TY][32]                     interior of a slab
-template <class T, int TY, bool TMA, bool PC>
+template <class T, int TY, bool TMA>
 struct StageLayout
 {
-    static constexpr int kNF     = PC ? 14 : 12;           // planes of a face slot
+    static constexpr int kNF     = 14;                     // planes of a face slot
     static constexpr int kCurW   = kTX + 6;                // cur row width
     static constexpr int kRing   = TY * kTX;               // one ring slot of a plane
     static constexpr int kCurOff = 6 * kRing;              // cur inside a plane
@@ -215,9 +222,9 @@ __device__ __forceinline__ void tma_load_4d(uint32_t dst, const void* tmap, int 
 #define MPCF_MIN_WARPS_PER_SM 16
 #endif
 // Tile heights of the form 2^n - 1 (3, 7, 15) carry a helper warp that
-// evaluates the tile's extra faces; other heights (8) give them to warps 0
-// and 1 as a fourth face job, which suits domains whose y extents are
-// multiples of 8.
+// takes the tile's extra jobs (ghost rows and columns, the faces above and
+// right of the tile); other heights (8) give them to warps 0..4, one each,
+// which suits domains whose y extents are multiples of 8.
 template <int TY> struct TileShape
 {
     static constexpr bool kHelper = ((TY + 1) & TY) == 0;
@@ -238,10 +245,7 @@ __global__ void __launch_bounds__(stage_threads<TY>(), MinBlocks<typename Pol::T
 stage_kernel(const StageArgs A)
 {
     typedef typename Pol::T T;
-    // per-cell reconstruction (both edge values of a cell from one set of
-    // smoothness indicators) in the fast policies; per-face otherwise
-    constexpr bool PC = Pol::kFastWeno;
-    typedef StageLayout<T, TY, TMA, PC> L;
+    typedef StageLayout<T, TY, TMA> L;
     extern __shared__ __align__(16) unsigned char smem_dyn[];
     // 128-byte aligned base (bulk tensor copies need it for their targets)
     unsigned char* smem_raw = smem_dyn + ((128u - (smem_u32(smem_dyn) & 127u)) & 127u);
@@ -480,15 +484,8 @@ stage_kernel(const StageArgs A)
                 }
             }
 
-            // (C) faces of slab k.  Column warps: job 0 = z face k-1/2 of the
-            // own column (kept in registers), job 1 = x face left of the own
-            // cell, job 2 = y face below it.  Helper warp (or warps 0 and 1
-            // as a fourth job without one): job 3 = y face above the tile
-            // (row TY, lane = column), job 4 = x face right of the tile
-            // (column 32, lane = row, lanes < TY).
-            // One face instance serves every job (runtime direction and
-            // stencil addresses).  R and U of cell k-1 are first prefetched
-            // into L1, so that the finalisation after the faces finds them.
+            // R and U of cell k-1 are first prefetched into L1, so that its
+            // finalisation after the z face finds them.
             const bool fin = (k > z0) && valid;
             const long long idx = (long long)gx + (long long)D.nx * ((long long)gy + (long long)D.ny * (k - 1));
             if (fin)
@@ -535,9 +532,8 @@ stage_kernel(const StageArgs A)
                 }
             };
             FaceOut<T> zf;
-            if constexpr (PC)
             {
-                // (C') per-cell reconstruction.
+                // (C) per-cell reconstruction and faces of slab k.
                 //  1. z (column threads): the right edge of cell k-1 (first
                 //     slab of a chunk only; later it is carried), both edges
                 //     of cell k, the z face k-1/2 from them, then cell k-1 is
@@ -570,7 +566,7 @@ stage_kernel(const StageArgs A)
                         for (int q = 0; q < 7; ++q)
                         {
                             const T* pl = sm + q * L::kPP;
-                            weno_cell_packed(pl[ad[0]], pl[ad[1]], pl[ad[2]], pl[ad[3]], pl[ad[4]], Rv[q], Lv[q]);
+                            weno_cell<Pol>(pl[ad[0]], pl[ad[1]], pl[ad[2]], pl[ad[3]], pl[ad[4]], Rv[q], Lv[q]);
                         }
                         if (cz == k)
                         {
@@ -579,7 +575,7 @@ stage_kernel(const StageArgs A)
                             S.rm = Rzp[0]; S.rp = Lv[0]; S.nm = Rzp[3]; S.np = Lv[3];
                             S.t1m = Rzp[1]; S.t1p = Lv[1]; S.t2m = Rzp[2]; S.t2p = Lv[2];
                             S.pm = Rzp[4]; S.pp = Lv[4]; S.Gm = Rzp[5]; S.Gp = Lv[5]; S.Pm = Rzp[6]; S.Pp = Lv[6];
-                            hllc_face_packed(S, 2, zf);
+                            face_hllc<Pol>(S, 2, zf);
                         }
 #pragma unroll
                         for (int q = 0; q < 7; ++q) Rzp[q] = Rv[q];
@@ -618,7 +614,7 @@ stage_kernel(const StageArgs A)
                         for (int q = 0; q < 7; ++q)
                         {
                             const T* pl = sm + q * L::kPP + base;
-                            weno_cell_packed(pl[-2 * step], pl[-step], pl[0], pl[step], pl[2 * step], Rv[q], Lv[q]);
+                            weno_cell<Pol>(pl[-2 * step], pl[-step], pl[0], pl[step], pl[2 * step], Rv[q], Lv[q]);
                         }
                         if (dR >= 0)
                         {
@@ -660,7 +656,7 @@ stage_kernel(const StageArgs A)
                         S.Gm  = pl[5 * L::kFP];     S.Gp  = pl[12 * L::kFP];
                         S.Pm  = pl[6 * L::kFP];     S.Pp  = pl[13 * L::kFP];
                         FaceOut<T> o;
-                        hllc_face_packed(S, dir, o);
+                        face_hllc<Pol>(S, dir, o);
 #pragma unroll
                         for (int m = 0; m < 7; ++m) pl[m * L::kFP] = o.f[m];
                         pl[7 * L::kFP] = o.Gm;  pl[8 * L::kFP] = o.Gp;
@@ -669,57 +665,6 @@ stage_kernel(const StageArgs A)
                     }
                 }
             }
-            else
-            {
-                constexpr bool kHelper = TileShape<TY>::kHelper;
-                const int jb = row ? 0 : 3;
-                int je;
-                if (kHelper) je = row ? ((k < z1) ? 3 : 1) : ((k < z1) ? (tx < TY ? 5 : 4) : 3);
-                else         je = (k < z1) ? ((ty == 0 || (ty == 1 && tx < TY)) ? 4 : 3) : 1;
-                const int zs0 = (k + 3) % 6;          // ring slot of slab k-3
-#pragma unroll 1
-                for (int jb_ = jb; jb_ < je; ++jb_)
-                {
-                    // without a helper, warp 1's fourth job is the right x faces
-                    const int job = (!kHelper && jb_ == 3 && ty == 1) ? 4 : jb_;
-                    int addr[6];
-                    int dir, dst;
-                    if (job == 0)
-                    {
-                        dir = 2; dst = -1;
-#pragma unroll
-                        for (int j = 0; j < 6; ++j) { const int sl = zs0 + j; addr[j] = (sl >= 6 ? sl - 6 : sl) * L::kRing + own; }
-                    }
-                    else
-                    {
-                        const bool xdir = (job == 1) || (job == 4);
-                        dir = xdir ? 0 : 1;
-                        int base;
-                        if (job == 1)      { base = (ty + 3) * L::kCurW + tx;  dst = L::kFx + ty * (kTX + 1) + tx; }
-                        else if (job == 2) { base = ty * L::kCurW + tx + 3;    dst = L::kFy + ty * kTX + tx; }
-                        else if (job == 3) { base = TY * L::kCurW + tx + 3;    dst = L::kFy + TY * kTX + tx; }
-                        else               { base = (tx + 3) * L::kCurW + kTX; dst = L::kFx + tx * (kTX + 1) + kTX; }
-                        const int step = xdir ? 1 : L::kCurW;
-#pragma unroll
-                        for (int j = 0; j < 6; ++j) addr[j] = L::kCurOff + base + j * step;
-                    }
-                    FaceOut<T> o;
-                    face_flux<Pol, L::kPP>(sm, addr, dir, o);
-                    if (dst < 0) zf = o;
-                    else
-                    {
-#pragma unroll
-                        for (int m = 0; m < 7; ++m) sm[dst + m * L::kFP] = o.f[m];
-                        sm[dst + 7 * L::kFP] = o.Gm;  sm[dst + 8 * L::kFP] = o.Gp;
-                        sm[dst + 9 * L::kFP] = o.Pm;  sm[dst + 10 * L::kFP] = o.Pp;
-                        sm[dst + 11 * L::kFP] = o.vel;
-                    }
-                }
-            }
-            // (E) finalise cell k-1 (the per-face path, after its faces and
-            // before the barrier, while the warps with a fourth face finish)
-            if (!PC && fin) finalize(zf);
-
             __syncthreads();
 
             // (F) x/y part of cell k, carried to the next slab
@@ -736,12 +681,6 @@ stage_kernel(const StageArgs A)
                 sG = sG + (fy[8 * L::kFP] + fy[7 * L::kFP + kTX]);
                 sP = sP + (fy[10 * L::kFP] + fy[9 * L::kFP + kTX]);
                 dU = dU + (fy[11 * L::kFP + kTX] - fy[11 * L::kFP]);
-            }
-            if (!PC)
-            {
-#pragma unroll
-                for (int m = 0; m < 7; ++m) zfp[m] = zf.f[m];
-                zfp[7] = zf.Gm; zfp[8] = zf.Gp; zfp[9] = zf.Pm; zfp[10] = zf.Pp; zfp[11] = zf.vel;
             }
         }
 
@@ -794,6 +733,6 @@ stage_kernel(const StageArgs A)
 }
 
 template <class Pol, int TY, bool TMA>
-constexpr size_t stage_smem_bytes() { return StageLayout<typename Pol::T, TY, TMA, Pol::kFastWeno>::kBytes; }
+constexpr size_t stage_smem_bytes() { return StageLayout<typename Pol::T, TY, TMA>::kBytes; }
 
 } // namespace mpcf
