@@ -42,10 +42,11 @@ METRIC = "cell-stage updates/s on 1 B200: mixed vs plain FP64 at stated L1 error
 UNIT = "cell-stage updates/s"
 BYTES_PER_CELL_STAGE = {"fp32_ref": 112, "fp32": 112, "mixed": 112, "fp64": 224}
 # DRAM bytes per cell-stage of the mixed stage kernel measured by ncu
-# (dram__bytes_read.sum + dram__bytes_write.sum = 1.851 GB for one launch
-# over the 256^3 cloud, 16.78 M cells).  Traffic grows in proportion to the
-# cells, so the per-launch figure of a larger workload is this times its cells.
-MEASURED_DRAM_BYTES_PER_CELL_STAGE = {"mixed": 1.851e9 / 256 ** 3}
+# (dram__bytes_read.sum + dram__bytes_write.sum = 8.87 + 7.48 GB for one
+# full-size launch over the 512^3 cloud, 134.2 M cells, 32 x 8 tiles over
+# whole columns, persistent, bulk-copy staging: a one-pass capture).  The
+# per-launch figure of the bench line is this times the workload's cells.
+MEASURED_DRAM_BYTES_PER_CELL_STAGE = {"mixed": 16.35e9 / 512 ** 3}
 
 
 # Algorithmic floating-point operations of one cell-stage, counted by
@@ -385,7 +386,7 @@ def main():
                          "frac": achieved / hbm,
                          "traffic": (MEASURED_DRAM_BYTES_PER_CELL_STAGE[args.precision] * ncell
                                      if args.precision in MEASURED_DRAM_BYTES_PER_CELL_STAGE else None),
-                         "traffic_note": "ncu DRAM bytes of one 256^3 launch scaled by cells",
+                         "traffic_note": "ncu DRAM bytes of one 512^3 launch (32x8 tiles, whole columns, persistent, TMA)",
                          "kernel": "stage_kernel<Pol%s>" % {"mixed": "Mixed", "fp32": "Fast32", "fp32_ref": "Ref32", "fp64": "FP64"}[args.precision],
                          "ms_per_launch": st_ms,
                          "algorithmic_bytes_per_launch": bytes_launch, "peak_kind": peak_kind,
