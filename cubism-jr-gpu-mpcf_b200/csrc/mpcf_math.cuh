@@ -82,87 +82,22 @@ template <class T> __device__ __forceinline__ T beta_g(const T x, const T y, con
     return x*(x*(T)(10./3.) - y*(T)(31./3.) + z*(T)(11./3.)) + y*(y*(T)(25./3.) - z*(T)(19./3.)) + z*z*(T)(4./3.);
 }
 
-// Nonlinear weights (omega0, omega1, omega2) from the three indicators and
-// the linear weights (c0, c1, c2) = (1, 6, 3) of the reference.
-template <class Pol>
-__device__ __forceinline__ void weno_weights(const typename Pol::T is0, const typename Pol::T is1,
-                                             const typename Pol::T is2,
-                                             typename Pol::T& w0, typename Pol::T& w1, typename Pol::T& w2)
-{
-    typedef typename Pol::T T;
-    const T is0plus = is0 + (T)MPCF_WENOEPS;
-    const T is1plus = is1 + (T)MPCF_WENOEPS;
-    const T is2plus = is2 + (T)MPCF_WENOEPS;
-    T alpha0, alpha1, alpha2;
-    if (Pol::kFastWeno)
-    {
-        // single-precision approximate reciprocal (MUFU); the common factor
-        // 1/10 cancels in the normalisation and is dropped
-        alpha0 = (T)1 * rcp_approx(is0plus*is0plus);
-        alpha1 = (T)6 * rcp_approx(is1plus*is1plus);
-        alpha2 = (T)3 * rcp_approx(is2plus*is2plus);
-    }
-    else
-    {
-        // the 10.0 literal promotes these to double (GPUonly.cuh:111-113)
-        alpha0 = (T)((T)(1)*(((T)1)/(10.0*is0plus*is0plus)));
-        alpha1 = (T)((T)(6)*(((T)1)/(10.0*is1plus*is1plus)));
-        alpha2 = (T)((T)(3)*(((T)1)/(10.0*is2plus*is2plus)));
-    }
-    const T alphasum = alpha0 + alpha1 + alpha2;
-    T inv;
-    if (Pol::kFastWeno) inv = rcp_approx(alphasum);
-    else                inv = ((T)1)/alphasum;
-    w0 = alpha0 * inv;
-    w1 = alpha1 * inv;
-    w2 = 1 - w0 - w1;
-}
-
-// Minus-side (left state) reconstruction at face i-1/2 from cells
-// a..e = i-3..i+1, clipped to [min,max] of b,c,d (GPUonly.cuh:138-194).
-template <class Pol>
-__device__ __forceinline__ typename Pol::T weno_minus_clipped(const typename Pol::T a, const typename Pol::T b,
-        const typename Pol::T c, const typename Pol::T d, const typename Pol::T e)
-{
-    typedef typename Pol::T T;
-    const T is0 = beta_f<T>(a, b, c);
-    const T is1 = beta_h<T>(b, c, d);
-    const T is2 = beta_g<T>(c, d, e);
-    T w0, w1, w2;
-    weno_weights<Pol>(is0, is1, is2, w0, w1, w2);
-    const T r = w0*((T)(1.0/3.)*a-(T)(7./6.)*b+(T)(11./6.)*c) + w1*(-(T)(1./6.)*b+(T)(5./6.)*c+(T)(1./3.)*d) + w2*((T)(1./3.)*c+(T)(5./6.)*d-(T)(1./6.)*e);
-    const T mn = dmin(dmin(b, c), d);
-    const T mx = dmax(dmax(b, c), d);
-    return dmin(dmax(r, mn), mx);
-}
-
-// Plus-side (right state) reconstruction at face i-1/2 from cells
-// b..f = i-2..i+2, clipped to [min,max] of c,d,e (GPUonly.cuh:99-135,177-183).
-template <class Pol>
-__device__ __forceinline__ typename Pol::T weno_pluss_clipped(const typename Pol::T b, const typename Pol::T c,
-        const typename Pol::T d, const typename Pol::T e, const typename Pol::T f)
-{
-    typedef typename Pol::T T;
-    const T is0 = beta_g<T>(d, e, f);
-    const T is1 = beta_h<T>(c, d, e);
-    const T is2 = beta_f<T>(b, c, d);
-    T w0, w1, w2;
-    weno_weights<Pol>(is0, is1, is2, w0, w1, w2);
-    const T r = w0*((T)(1./3.)*f-(T)(7./6.)*e+(T)(11./6.)*d) + w1*(-(T)(1./6.)*e+(T)(5./6.)*d+(T)(1./3.)*c) + w2*((T)(1./3.)*d+(T)(5./6.)*c-(T)(1./6.)*b);
-    const T mn = dmin(dmin(c, d), e);
-    const T mx = dmax(dmax(c, d), e);
-    return dmin(dmax(r, mn), mx);
-}
-
 // Both edge values of one cell in the reference-rounding policies, from the
-// cells y0..y4 = l-2..l+2: R = weno_minus_clipped(y0..y4), the minus side of
-// face l+1/2, and L = weno_pluss_clipped(y0..y4), the plus side of face
-// l-1/2.  The two evaluate the same three indicator calls --
-// beta_f(y0,y1,y2), beta_h(y1,y2,y3), beta_g(y2,y3,y4) -- with the same
-// double-precision 1/(10 (beta+eps)^2) of each and the same clip bounds;
-// those are evaluated once here, and every other operation is the one of
-// the two functions above in their order, so R and L are bit-identical to
-// them (GPUonly.cuh:99-194).
+// cells y0..y4 = l-2..l+2 (GPUonly.cuh:99-194):
+//   R, the minus side of face l+1/2: indicators (is0, is1, is2) =
+//     (beta_f(y0,y1,y2), beta_h(y1,y2,y3), beta_g(y2,y3,y4)), candidates
+//     from y0..y4, clipped to [min, max] of y1, y2, y3;
+//   L, the plus side of face l-1/2: indicators (beta_g(y2,y3,y4),
+//     beta_h(y1,y2,y3), beta_f(y0,y1,y2)), the mirrored candidates, the same
+//     clip;
+//   weights alpha_j = c_j * (1/(10.0*(is_j+eps)^2)) with c = (1, 6, 3) (the
+//   10.0 literal promotes the reciprocal to double, GPUonly.cuh:111-113),
+//   w0 = alpha0/sum, w1 = alpha1/sum, w2 = 1 - w0 - w1.
+// The reference evaluates each face's two sides separately; the three
+// indicator calls, their double reciprocals and the clip bounds of the two
+// edges of a cell are the same operations on the same values, so they are
+// evaluated once here.  Every other operation is the reference's in its
+// order, so R and L are bit-identical to its per-face results.
 template <class Pol>
 __device__ __forceinline__ void weno_cell_ref(const typename Pol::T y0, const typename Pol::T y1,
         const typename Pol::T y2, const typename Pol::T y3, const typename Pol::T y4,

@@ -558,9 +558,11 @@ stage_kernel(const StageArgs A)
 #pragma unroll 1
                     for (int cz = (k == z0) ? k - 1 : k; cz <= k; ++cz)
                     {
+                        // ring slots of slabs cz-2 .. cz+2
+                        const int zs = (cz + 4) % 6;
                         int ad[5];
 #pragma unroll
-                        for (int j = 0; j < 5; ++j) ad[j] = ((cz + 4 + j) % 6) * L::kRing + own;
+                        for (int j = 0; j < 5; ++j) ad[j] = (zs + j < 6 ? zs + j : zs + j - 6) * L::kRing + own;
                         T Rv[7], Lv[7];
 #pragma unroll
                         for (int q = 0; q < 7; ++q)
