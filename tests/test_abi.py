@@ -60,6 +60,9 @@ def test_create_rejects_bad_arguments(mpcf):
     assert L.mpcf_create(ctypes.byref(h), 1, dims, bc, 0, 0) == -1
     assert L.mpcf_create(ctypes.byref(h), 0, dims, None, 0, 0) == -1
     assert L.mpcf_create(ctypes.byref(h), 1, dims, None, 9, 0) == -1
+    bc = (ctypes.c_int * 6)(mpcf.BC_HALO, 0, 0, 0, 0, 0)     # halo faces are z faces only
+    assert L.mpcf_create(ctypes.byref(h), 1, dims, bc, 0, 0) == -1
+    assert b"halo faces are z faces" in L.mpcf_last_error()
 
 
 def test_bubbles_are_seeded_and_disjoint(mpcf):
