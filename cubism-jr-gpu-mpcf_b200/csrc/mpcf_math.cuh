@@ -59,6 +59,14 @@ __device__ __forceinline__ float rcp_approx(float x)
 }
 __device__ __forceinline__ double rcp_approx(double x) { return 1.0 / x; }
 
+// Approximate square root of the special-function unit (fast policies).
+__device__ __forceinline__ float sqrt_approx(float x)
+{
+    float r;
+    asm("sqrt.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+    return r;
+}
+
 // ---------------------------------------------------------------------------
 // WENO5 smoothness indicators.  For a window of three consecutive cells
 // (x, y, z) left to right, the reference uses three polynomial forms:
@@ -484,10 +492,11 @@ __device__ __forceinline__ double shfl_max(double v) { for (int o = 16; o > 0; o
 // Maximum characteristic speed of one cell, |u|max + c with
 //   p = (E - (ru^2+rv^2+rw^2)*(0.5/rho) - P)/G,  c = sqrt(((p+P)/G + p)/rho)
 // (GPUkernels.cu:1182-1222; the mixed policy recovers p in FP64).  Every
-// operation is an explicit round-to-nearest intrinsic, so the result is the
-// same whatever the translation unit's contraction and division flags: the
-// stand-alone reduction and the one fused into the stage kernel agree bit
-// for bit.
+// operation is an explicit instruction -- round-to-nearest intrinsics, and
+// in the fast policies the approximate reciprocal and square root -- so the
+// result is the same whatever the translation unit's contraction and
+// division flags: the stand-alone reduction and the one fused into the stage
+// kernel agree bit for bit.
 template <class Pol>
 __device__ __forceinline__ typename Pol::T cell_sos_rn(const typename Pol::T r, const typename Pol::T u,
         const typename Pol::T v, const typename Pol::T w, const typename Pol::T e,
@@ -500,6 +509,29 @@ __device__ __forceinline__ typename Pol::T cell_sos_rn(const typename Pol::T r, 
         const double p = __ddiv_rn(__dsub_rn(__dsub_rn(e, __dmul_rn(sq, __ddiv_rn(0.5, r))), P), G);
         const double c = __dsqrt_rn(__ddiv_rn(__dadd_rn(__ddiv_rn(__dadd_rn(p, P), G), p), r));
         return __dadd_rn(c, __ddiv_rn(fmax(fmax(fabs(u), fabs(v)), fabs(w)), r));
+    }
+    else if constexpr (Pol::kFastWeno)
+    {
+        // the fast policies: reciprocals and square root of the special-
+        // function unit, refined in FP64 for the mixed pressure, every
+        // operation an explicit instruction (so the two reductions still
+        // agree bit for bit)
+        const float ir = rcp_approx(r), iG = rcp_approx(G);
+        float p;
+        if constexpr (Pol::kP64)
+        {
+            const double du = u, dv = v, dw = w;
+            const double sq = __fma_rn(dw, dw, __fma_rn(dv, dv, __dmul_rn(du, du)));
+            const double ke = __dmul_rn(sq, __dmul_rn(0.5, rcp_f64((double)r)));
+            p = (float)__dmul_rn(__dsub_rn(__dsub_rn((double)e, ke), (double)P), rcp_f64((double)G));
+        }
+        else
+        {
+            const float sq = __fmaf_rn(w, w, __fmaf_rn(v, v, __fmul_rn(u, u)));
+            p = __fmul_rn(__fsub_rn(__fsub_rn(e, __fmul_rn(sq, __fmul_rn(0.5f, ir))), P), iG);
+        }
+        const float c = sqrt_approx(__fmul_rn(__fmaf_rn(__fadd_rn(p, P), iG, p), ir));
+        return __fmaf_rn(fmaxf(fmaxf(fabsf(u), fabsf(v)), fabsf(w)), ir, c);
     }
     else
     {
