@@ -789,6 +789,9 @@ int mpcf_link_z(mpcf_solver* s, int lower, int upper)
     for (size_t i = 0; i < s->links.size(); i += 2)
         if (s->links[i] == lower || s->links[i + 1] == upper)
             return fail(MPCF_ERR_ARG, "face already linked (domains %d, %d)", lower, upper);
+    // the exchange kernel gives every link 14 block rows (grid y <= 65535)
+    if (s->links.size() / 2 + 1 > 65535 / 14)
+        return fail(MPCF_ERR_ARG, "at most %d links per solver", 65535 / 14);
     DeviceGuard g(s->device);
     s->links.push_back(lower);
     s->links.push_back(upper);
