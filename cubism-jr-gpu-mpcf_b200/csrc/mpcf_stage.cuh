@@ -68,14 +68,13 @@ __host__ __device__ constexpr size_t align_up(size_t v, size_t a) { return (v + 
 // addr[j] + q*kPP with kPP a compile-time constant:
 //   plane q:  ring [6 slots][TY][32]      z-ring of the tile's own columns
 //             cur  [TY+6][38]             slab k with 3-cell x/y halos
-// Face slots, pitch kFP = (TY+1)*32, NF planes each:
-//   fx   [NF][TY][33]                     x faces of slab k
-//   fy   [NF][TY+1][32]                   y faces of slab k
-// Planes 0..11 of a slot hold the face's results (7 fluxes, G-, G+, P-, P+,
-// the extra-term velocity).  With per-cell reconstruction (fast policies)
-// NF = 14: before the fluxes, planes 0..6 hold the face's minus side and
-// planes 7..13 its plus side, and the face's evaluation overwrites them in
-// place.  Otherwise NF = 12.
+// Face slots, pitch kFP = (TY+1)*32, 14 planes each:
+//   fx   [14][TY][33]                     x faces of slab k
+//   fy   [14][TY+1][32]                   y faces of slab k
+// Before a face is evaluated, planes 0..6 of its slot hold its minus side
+// and planes 7..13 its plus side (the reconstructed edge values of the two
+// cells it separates); the evaluation overwrites planes 0..11 in place with
+// its results (7 fluxes, G-, G+, P-, P+, the extra-term velocity).
 // then, in bytes: the FP64 reduction scratch [TY][5], the tile broadcast,
 // two mbarriers and, with TMA, the two staging buffers (128-byte aligned):
 //   A     [7][TY+6][40]                   halo box, x from x0-4, y from y0-3

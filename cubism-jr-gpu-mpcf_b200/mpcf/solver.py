@@ -13,7 +13,7 @@ import time
 import numpy as np
 
 from . import _lib
-from ._lib import check, lib, IcParams
+from ._lib import check, lib
 
 FIELDS = ("rho", "rhou", "rhov", "rhow", "E", "G", "P")
 
