@@ -476,6 +476,8 @@ int mpcf_create(mpcf_solver** out, int ndomains, const int* dims, const int* bc,
         D.nx = dims[3 * d]; D.ny = dims[3 * d + 1]; D.nz = dims[3 * d + 2];
         for (int f = 0; f < 6; ++f) D.bc[f] = bc ? bc[6 * d + f] : MPCF_BC_ABSORBING;
         D.h = 1.0 / (double)std::max(D.nx, std::max(D.ny, D.nz));
+        D.org[0] = D.org[1] = D.org[2] = 0;
+        D.gdim[0] = D.nx; D.gdim[1] = D.ny; D.gdim[2] = D.nz;
         D.zlo = D.bc[4] == MPCF_BC_HALO ? kHaloPlanes : 0;
         D.zhi = D.bc[5] == MPCF_BC_HALO ? kHaloPlanes : 0;
         D.group = d;
@@ -837,6 +839,23 @@ int mpcf_set_spacing(mpcf_solver* s, int dom, double h)
     return MPCF_OK;
 }
 
+int mpcf_set_origin(mpcf_solver* s, int dom, const int* org3, const int* global3)
+{
+    int rc = check_dom(s, dom);
+    if (rc) return rc;
+    if (!org3 || !global3) return fail(MPCF_ERR_ARG, "null origin or global size");
+    DomDev& D = s->hdoms[dom];
+    const int n[3] = {D.nx, D.ny, D.nz};
+    for (int a = 0; a < 3; ++a)
+        if (org3[a] < 0 || global3[a] < n[a] || org3[a] > global3[a] - n[a])
+            return fail(MPCF_ERR_ARG, "axis %d: cells %d..%d outside the global extent %d", a, org3[a], org3[a] + n[a] - 1, global3[a]);
+    DeviceGuard g(s->device);
+    for (int a = 0; a < 3; ++a) { D.org[a] = org3[a]; D.gdim[a] = global3[a]; }
+    CK(cudaMemcpyAsync(s->ddoms, s->hdoms.data(), sizeof(DomDev) * s->ndom, cudaMemcpyHostToDevice, s->stream));
+    CK(cudaStreamSynchronize(s->stream));
+    return MPCF_OK;
+}
+
 int mpcf_exchange_halos(mpcf_solver* s)
 {
     if (!s) return fail(MPCF_ERR_ARG, "null solver");
@@ -1050,7 +1069,8 @@ int mpcf_ic_sbi(mpcf_solver* s, int dom, const mpcf_sbi_params* p, int nbubbles,
     static_assert(sizeof(SbiParams) == sizeof(mpcf_sbi_params), "parameter layout");
     memcpy(&P, p, sizeof(P));
     const DomDev& D = s->hdoms[dom];
-    CK(launch_ic_sbi(s->esz == 8, s->ddoms + dom, D.nx, D.ny, D.nz, s->parity, P, s->bubbles, nbubbles, s->stream));
+    // h of the global domain (the bubble interface width)
+    CK(launch_ic_sbi(s->esz == 8, s->ddoms + dom, D.gdim[0], D.gdim[1], D.gdim[2], s->parity, P, s->bubbles, nbubbles, s->stream));
     s->sums_valid = false;
     CK(cudaStreamSynchronize(s->stream));
     return MPCF_OK;

@@ -213,11 +213,14 @@ __global__ void ic_cloud_kernel(const DomDev* dom, int parity, const IcParams P,
     const long long fs = D.fs;
     for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < N; i += (long long)gridDim.x * blockDim.x)
     {
-        const int ix = (int)(i % D.nx);
-        const int iy = (int)((i / D.nx) % D.ny);
-        const int iz = (int)(i / ((long long)D.nx * D.ny));
+        // the cell's place in the global grid (its noise stream too)
+        const int gx = D.org[0] + (int)(i % D.nx);
+        const int gy = D.org[1] + (int)((i / D.nx) % D.ny);
+        const int gz = D.org[2] + (int)(i / ((long long)D.nx * D.ny));
+        const unsigned long long lin = (unsigned long long)gx + (unsigned long long)D.gdim[0] *
+                                       ((unsigned long long)gy + (unsigned long long)D.gdim[1] * (unsigned long long)gz);
         double c[7];
-        ic_cell(P, bub, nb, D.h, ix, iy, iz, (unsigned long long)i, c);
+        ic_cell(P, bub, nb, D.h, gx, gy, gz, lin, c);
         for (int m = 0; m < 7; ++m) { U[m * fs + i] = (T)c[m]; R[m * fs + i] = (T)0; }
     }
 }
@@ -356,8 +359,9 @@ __global__ void __launch_bounds__(256) sic_cloud_kernel(const DomDev* dom, int p
     const int iz = blockIdx.z * 4 + (threadIdx.x >> 6);
     if (threadIdx.x == 0) cnt = 0;
     __syncthreads();
-    const double lo[3] = {hd * (blockIdx.x * 8), hd * (blockIdx.y * 8), hd * (blockIdx.z * 4)};
-    const double hi[3] = {hd * (blockIdx.x * 8 + 8), hd * (blockIdx.y * 8 + 8), hd * (blockIdx.z * 4 + 4)};
+    // the tile's sample box in global coordinates
+    const double lo[3] = {hd * (D.org[0] + blockIdx.x * 8), hd * (D.org[1] + blockIdx.y * 8), hd * (D.org[2] + blockIdx.z * 4)};
+    const double hi[3] = {hd * (D.org[0] + blockIdx.x * 8 + 8), hd * (D.org[1] + blockIdx.y * 8 + 8), hd * (D.org[2] + blockIdx.z * 4 + 4)};
     for (int i = threadIdx.x; i < nshapes; i += blockDim.x)
     {
         const double* c = shapes + 4 * (size_t)i;
@@ -378,7 +382,7 @@ __global__ void __launch_bounds__(256) sic_cloud_kernel(const DomDev* dom, int p
     Real all[4];
 
     const Real h  = (Real)hd / 2;          // sample spacing: half the grid spacing
-    const double p[3] = {hd * (ix + 0.5), hd * (iy + 0.5), hd * (iz + 0.5)};
+    const double p[3] = {hd * (D.org[0] + ix + 0.5), hd * (D.org[1] + iy + 0.5), hd * (D.org[2] + iz + 0.5)};
     const Real x0[3] = {(Real)(p[0] - (double)h), (Real)(p[1] - (double)h), (Real)(p[2] - (double)h)};
     const Real w6 = (Real)(1 / 6.), w23 = (Real)(2. / 3);
     Real acc[7];
@@ -480,7 +484,7 @@ __global__ void sod_kernel(const DomDev* dom, int parity, const SodParams P)
     for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
     {
         const int idx[3] = {(int)(i % D.nx), (int)((i / D.nx) % D.ny), (int)(i / ((long long)D.nx * D.ny))};
-        const double pos = D.h * (idx[P.axis] + 0.5);
+        const double pos = D.h * (D.org[P.axis] + idx[P.axis] + 0.5);
         const bool x = P.reverse ? pos > P.x0 : pos < P.x0;
         const bool nx = !x;
         // the reference's boolean-weighted mixture (Sim_SodMPI.cpp:69-75)
@@ -580,11 +584,13 @@ __global__ void sbi_kernel(const DomDev* dom, int parity, const SbiParams P, con
     const DomDev& D = *dom;
     Real* U = (Real*)D.U[parity];
     Real* R = (Real*)D.R;
-    const int n3[3] = {D.nx, D.ny, D.nz};
+    // global indices: the mirror is through the global domain's centre
+    const int n3[3] = {D.gdim[0], D.gdim[1], D.gdim[2]};
     const long long n = (long long)D.nx * D.ny * D.nz;
     for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
     {
-        int idx[3] = {(int)(i % D.nx), (int)((i / D.nx) % D.ny), (int)(i / ((long long)D.nx * D.ny))};
+        int idx[3] = {D.org[0] + (int)(i % D.nx), D.org[1] + (int)((i / D.nx) % D.ny),
+                      D.org[2] + (int)(i / ((long long)D.nx * D.ny))};
         bool flip = false;
         if (P.reverse && !((n3[P.axis0] & 1) && idx[P.axis0] == n3[P.axis0] / 2))
         {

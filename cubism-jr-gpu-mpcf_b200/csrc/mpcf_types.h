@@ -42,6 +42,8 @@ struct DomDev
     int    sos_chunks;
     int    tma_ok;      // 1: tensor maps of this domain are valid (rows of 16-byte multiples)
     int    zlo, zhi;    // stored ghost planes below z = 0 / above z = nz-1 (0 or 3, halo faces)
+    int    org[3];      // cell (0,0,0) is cell org of a global grid of gdim cells (initial conditions)
+    int    gdim[3];
     // the extended domain the stage kernel sees: planes -zlo .. nz-1+zhi as
     // 0 .. nzx-1 (Ux/Rx = U/R shifted back by zlo planes; the register is
     // only ever read at the domain's own planes)

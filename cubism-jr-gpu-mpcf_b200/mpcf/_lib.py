@@ -99,6 +99,7 @@ SIGNATURES = {
     "mpcf_link_z": (_I, [_P, _I, _I]),
     "mpcf_set_spacing": (_I, [_P, _I, _D]),
     "mpcf_exchange_halos": (_I, [_P]),
+    "mpcf_set_origin": (_I, [_P, _I, _PI, _PI]),
     "mpcf_ic_cloud": (_I, [_P, _I, _c.POINTER(IcParams), _I, _PD]),
     "mpcf_ic_cloud_host": (_I, [_I, _I, _I, _c.POINTER(IcParams), _I, _PD, _I, _PP]),
     "mpcf_bubbles": (_I, [_c.c_ulonglong, _I, _D, _D, _PD, _PD, _D, _I, _PD]),

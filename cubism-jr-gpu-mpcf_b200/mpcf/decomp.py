@@ -9,6 +9,10 @@ a slab's z face towards a neighbouring slab is a halo face (BC_HALO) whose 3
 ghost planes are stored state, refreshed from the neighbour before every
 stage.  Two drivers share the plan:
 
+Each slab carries its place in the global grid (mpcf_set_origin), so the
+device initial-condition generators write the global domain's values of its
+cells: a rank sets up its own slab without the global state.
+
 * ``slab_solver``: all slabs in one Solver on one GPU.  The library links
   them (mpcf_link_z), copies the ghost planes on the device at the start of
   every stage and gives the linked slabs one dt; steps, runs and CUDA graphs
@@ -82,8 +86,9 @@ def slab_solver(global_dims, nslabs, bc=None, precision="fp32_ref", device=0):
     s = Solver(dims, bc=bcs, precision=precision, device=device)
     try:
         h = global_spacing(global_dims)
-        for r in range(nslabs):
+        for r, (z0, _) in enumerate(ext):
             s.set_spacing(h, dom=r)
+            s.set_origin((0, 0, z0), (NX, NY, NZ), dom=r)
         for r in range(nslabs - 1):
             s.link_z(r, r + 1)
     except Exception:
@@ -186,6 +191,7 @@ class SlabRank:
         self.solver = Solver([(NX, NY, self.nz)], bc=[slab_bc(bc, self.rank, self.nranks)],
                              precision=precision, device=device)
         self.solver.set_spacing(self.h)
+        self.solver.set_origin((0, 0, self.z0), self.global_dims)
         self.device = device
         self.time = 0.0
         self._typestr = "<f8" if self.solver.dtype == np.float64 else "<f4"

@@ -164,6 +164,13 @@ class Solver:
     def exchange_halos(self):
         check(lib().mpcf_exchange_halos(self._h))
 
+    def set_origin(self, org, global_dims, dom=0):
+        """The domain is the block at cell `org` of a global grid of
+        `global_dims` cells (mpcf_set_origin): initial conditions are then
+        generated in the global domain's coordinates."""
+        check(lib().mpcf_set_origin(self._h, dom, (ctypes.c_int * 3)(*[int(v) for v in org]),
+                                    (ctypes.c_int * 3)(*[int(v) for v in global_dims])))
+
     def fill_ghosts(self, dom=0):
         nx, ny, nz = self.dims[dom]
         gx = np.empty(2 * 7 * 3 * ny * nz, self.dtype)

@@ -210,6 +210,14 @@ int mpcf_fill_ghosts(mpcf_solver* s, int dom, void* gx, void* gy, void* gz, int 
 int mpcf_link_z(mpcf_solver* s, int lower, int upper);
 int mpcf_set_spacing(mpcf_solver* s, int dom, double h);
 int mpcf_exchange_halos(mpcf_solver* s);
+/* The domain is the block of cells org3 .. org3 + dims - 1 of a global grid
+ * of global3 cells (GridMPI's per-rank block offset): the initial-condition
+ * generators (mpcf_ic_cloud, mpcf_ic_sic_cloud, mpcf_ic_steady, mpcf_ic_sod,
+ * mpcf_ic_sbi) then write the global domain's values of these cells, so
+ * slabs set up on their own GPUs equal the slices of the undivided domain's
+ * initial condition.  Default: origin 0, global = the domain.  The spacing
+ * is set separately (mpcf_set_spacing). */
+int mpcf_set_origin(mpcf_solver* s, int dom, const int* org3, const int* global3);
 
 /* ---- initial conditions --------------------------------------------------- */
 /* device generator: state of domain dom from the cloud IC, register cleared */
