@@ -299,6 +299,29 @@ def test_fast_forms_track_fp64(mpcf):
     assert e_mix <= 1.5 * e_ref + 1e-9, (e_mix, e_ref)
 
 
+def test_fast_forms_track_fp64_over_many_steps(mpcf):
+    """A longer run (40 steps, the bubbles start to collapse): the fast forms
+    stay physical and within 1e-5 of the all-FP64 run in L1 of every
+    conserved field relative to its mean magnitude, and the mixed form stays
+    at least as close as the reference rounding in rho."""
+    dims = (64, 48, 40)
+    U64 = cloud_state(dims, nb=4, dtype=np.float64, p_liquid=1000.0)
+    res, t = {}, {}
+    for prec in ("fp64", "fp32_ref", "fp32", "mixed"):
+        dt = mpcf.dtype_of(mpcf.PRECISIONS[prec])
+        with mpcf.Solver([dims], precision=prec) as s:
+            s.set_state([a.astype(dt) for a in U64])
+            t[prec] = s.run(40, cfl=0.3, graph=True)[0]
+            res[prec] = s.get_state(with_reg=False)
+            assert s.error_word() == 0, prec
+    for prec in ("fp32", "mixed"):
+        assert abs(t[prec] - t["fp64"]) <= 1e-5 * t["fp64"], (prec, t[prec], t["fp64"])
+        for q in (0, 4, 5, 6):
+            e = rel_l1(res[prec][q], res["fp64"][q])
+            assert e <= 1e-5, (prec, q, e)
+    assert rel_l1(res["mixed"][0], res["fp64"][0]) <= 1.5 * rel_l1(res["fp32_ref"][0], res["fp64"][0]) + 1e-9
+
+
 def test_convection_then_update_equals_fused_stage(mpcf):
     """Convection_CUDA (stage with b = 0) followed by Update_CUDA (mpcf_update)
     is bit-identical to one fused stage, like the reference's two kernels."""
