@@ -9,6 +9,7 @@
 #include <cuda_runtime.h>
 #include <cuda.h>
 #include <cudaTypedefs.h>
+#include <nvtx3/nvToolsExt.h>
 #include <algorithm>
 #include <cstdarg>
 #include <cstdio>
@@ -60,6 +61,14 @@ namespace {
 
 #define CK(call) do { cudaError_t e_ = (call); if (e_ != cudaSuccess) \
     return fail(MPCF_ERR_CUDA, "%s failed: %s (%s:%d)", #call, cudaGetErrorString(e_), __FILE__, __LINE__); } while (0)
+
+// NVTX range over an entry point (header-only NVTX 3: no-ops unless a
+// profiler is attached), so a timeline shows the host calls of the path.
+struct Range
+{
+    explicit Range(const char* name) { nvtxRangePushA(name); }
+    ~Range() { nvtxRangePop(); }
+};
 
 struct DeviceGuard
 {
@@ -554,6 +563,7 @@ int mpcf_precision(const mpcf_solver* s) { return s ? s->pol : fail(MPCF_ERR_ARG
 
 int mpcf_set_state(mpcf_solver* s, int dom, const void* const* state7, const void* const* reg7, int src_is_device)
 {
+    Range nvtx("mpcf_set_state");
     int rc = check_dom(s, dom);
     if (rc) return rc;
     if (!state7) return fail(MPCF_ERR_ARG, "null state pointers");
@@ -571,6 +581,7 @@ int mpcf_set_state(mpcf_solver* s, int dom, const void* const* state7, const voi
 
 int mpcf_get_state(mpcf_solver* s, int dom, void* const* state7, void* const* reg7, int dst_is_device)
 {
+    Range nvtx("mpcf_get_state");
     int rc = check_dom(s, dom);
     if (rc) return rc;
     DeviceGuard g(s->device);
@@ -598,6 +609,7 @@ int mpcf_device_pointers(mpcf_solver* s, int dom, void** state7, void** reg7)
 
 int mpcf_max_sos(mpcf_solver* s, double* sos)
 {
+    Range nvtx("mpcf_max_sos");
     if (!s) return fail(MPCF_ERR_ARG, "null solver");
     DeviceGuard g(s->device);
     s->sos_fresh = false;                   // the state (or the accumulator) changes
@@ -615,6 +627,7 @@ int mpcf_max_sos(mpcf_solver* s, double* sos)
 
 int mpcf_stage(mpcf_solver* s, double a, double b, const double* dtinvh)
 {
+    Range nvtx("mpcf_stage");
     if (!s) return fail(MPCF_ERR_ARG, "null solver");
     DeviceGuard g(s->device);
     s->sos_fresh = false;                   // the state (or the accumulator) changes
@@ -636,6 +649,7 @@ int mpcf_stage(mpcf_solver* s, double a, double b, const double* dtinvh)
 
 int mpcf_compute_dt(mpcf_solver* s, double cfl, double dt_max, double* dt_out)
 {
+    Range nvtx("mpcf_compute_dt");
     if (!s) return fail(MPCF_ERR_ARG, "null solver");
     if (!(cfl > 0) || !(dt_max > 0)) return fail(MPCF_ERR_ARG, "cfl and dt_max must be positive");
     DeviceGuard g(s->device);
@@ -650,6 +664,7 @@ int mpcf_compute_dt(mpcf_solver* s, double cfl, double dt_max, double* dt_out)
 
 int mpcf_step(mpcf_solver* s, double cfl, double dt_max, double* dt_out)
 {
+    Range nvtx("mpcf_step");
     if (!s) return fail(MPCF_ERR_ARG, "null solver");
     if (!(cfl > 0) || !(dt_max > 0)) return fail(MPCF_ERR_ARG, "cfl and dt_max must be positive");
     DeviceGuard g(s->device);
@@ -666,6 +681,7 @@ int mpcf_step(mpcf_solver* s, double cfl, double dt_max, double* dt_out)
 
 int mpcf_run(mpcf_solver* s, int nsteps, double cfl, double dt_max, int use_graph, double* time_out)
 {
+    Range nvtx("mpcf_run");
     if (!s) return fail(MPCF_ERR_ARG, "null solver");
     if (nsteps < 0) return fail(MPCF_ERR_ARG, "nsteps < 0");
     if (!(cfl > 0) || !(dt_max > 0)) return fail(MPCF_ERR_ARG, "cfl and dt_max must be positive");
@@ -732,6 +748,7 @@ int mpcf_set_track_conservation(mpcf_solver* s, int on)
 
 int mpcf_conserved_sums(mpcf_solver* s, double* out)
 {
+    Range nvtx("mpcf_conserved_sums");
     if (!s || !out) return fail(MPCF_ERR_ARG, "null argument");
     DeviceGuard g(s->device);
     if (!s->sums_valid)
@@ -778,6 +795,7 @@ int mpcf_set_bc(mpcf_solver* s, int dom, const int* bc6)
 
 int mpcf_link_z(mpcf_solver* s, int lower, int upper)
 {
+    Range nvtx("mpcf_link_z");
     int rc = check_dom(s, lower);
     if (rc) return rc;
     if ((rc = check_dom(s, upper))) return rc;
@@ -858,6 +876,7 @@ int mpcf_set_origin(mpcf_solver* s, int dom, const int* org3, const int* global3
 
 int mpcf_exchange_halos(mpcf_solver* s)
 {
+    Range nvtx("mpcf_exchange_halos");
     if (!s) return fail(MPCF_ERR_ARG, "null solver");
     if (s->links.empty()) return MPCF_OK;
     DeviceGuard g(s->device);
@@ -899,6 +918,7 @@ int mpcf_fill_ghosts(mpcf_solver* s, int dom, void* gx, void* gy, void* gz, int 
 
 int mpcf_ic_cloud(mpcf_solver* s, int dom, const mpcf_ic_params* p, int nbubbles, const double* bubbles4)
 {
+    Range nvtx("mpcf_ic_cloud");
     int rc = check_dom(s, dom);
     if (rc) return rc;
     if (!p || nbubbles < 0 || (nbubbles > 0 && !bubbles4)) return fail(MPCF_ERR_ARG, "bad IC arguments");
@@ -963,6 +983,7 @@ int mpcf_sic_post_shock(const mpcf_sic_params* p, int precision, double* post4)
 
 int mpcf_ic_sic_cloud(mpcf_solver* s, int dom, const mpcf_sic_params* p, int nshapes, const double* shapes4)
 {
+    Range nvtx("mpcf_ic_sic_cloud");
     int rc = check_dom(s, dom);
     if (rc) return rc;
     if ((rc = sic_check(p))) return rc;
@@ -1011,6 +1032,7 @@ void mpcf_case_default_params(mpcf_steady_params* st, mpcf_sod_params* sod, mpcf
 
 int mpcf_ic_steady(mpcf_solver* s, int dom, const mpcf_steady_params* p)
 {
+    Range nvtx("mpcf_ic_steady");
     int rc = check_dom(s, dom);
     if (rc) return rc;
     if (!p || !(p->g > 1) || !(p->rho > 0)) return fail(MPCF_ERR_ARG, "bad SteadyState parameters");
@@ -1027,6 +1049,7 @@ int mpcf_ic_steady(mpcf_solver* s, int dom, const mpcf_steady_params* p)
 
 int mpcf_ic_sod(mpcf_solver* s, int dom, const mpcf_sod_params* p)
 {
+    Range nvtx("mpcf_ic_sod");
     int rc = check_dom(s, dom);
     if (rc) return rc;
     if (!p || p->axis < 0 || p->axis > 2 || !(p->g1 > 1) || !(p->g2 > 1) || !(p->rho1 > 0) || !(p->rho2 > 0))
@@ -1044,6 +1067,7 @@ int mpcf_ic_sod(mpcf_solver* s, int dom, const mpcf_sod_params* p)
 
 int mpcf_ic_sbi(mpcf_solver* s, int dom, const mpcf_sbi_params* p, int nbubbles, const double* bubbles4)
 {
+    Range nvtx("mpcf_ic_sbi");
     int rc = check_dom(s, dom);
     if (rc) return rc;
     if (!p || p->axis0 < 0 || p->axis0 > 2 || p->axis1 < 0 || p->axis1 > 2 || p->axis0 == p->axis1 ||
@@ -1132,6 +1156,7 @@ static std::string join_path(const char* dir, const std::string& name)
 
 int mpcf_pack(mpcf_solver* s, int dom, int kind, void* host_out)
 {
+    Range nvtx("mpcf_pack");
     int rc = check_dom(s, dom);
     if (rc) return rc;
     if (!host_out || (kind != MPCF_DUMP_TENSOR && kind != MPCF_DUMP_SAVE)) return fail(MPCF_ERR_ARG, "bad arguments");
@@ -1144,6 +1169,7 @@ int mpcf_pack(mpcf_solver* s, int dom, int kind, void* host_out)
 
 int mpcf_unpack_save(mpcf_solver* s, int dom, const void* host_in)
 {
+    Range nvtx("mpcf_unpack_save");
     int rc = check_dom(s, dom);
     if (rc) return rc;
     if (!host_in) return fail(MPCF_ERR_ARG, "null input");
@@ -1159,6 +1185,7 @@ int mpcf_unpack_save(mpcf_solver* s, int dom, const void* host_in)
 
 int mpcf_dump(mpcf_solver* s, int dom, int kind, const char* dir, const char* name, int step)
 {
+    Range nvtx("mpcf_dump");
     int rc = check_dom(s, dom);
     if (rc) return rc;
     if (!name || !name[0] || (kind != MPCF_DUMP_TENSOR && kind != MPCF_DUMP_SAVE)) return fail(MPCF_ERR_ARG, "bad arguments");
@@ -1231,6 +1258,7 @@ int mpcf_get_time(mpcf_solver* s, int dom, double* t)
 
 int mpcf_save(mpcf_solver* s, int dom, const char* dir, double t, int step, int fcount)
 {
+    Range nvtx("mpcf_save");
     int rc = check_dom(s, dom);
     if (rc) return rc;
     const std::string info = join_path(dir, "save.info");
@@ -1243,6 +1271,7 @@ int mpcf_save(mpcf_solver* s, int dom, const char* dir, double t, int step, int 
 
 int mpcf_restart(mpcf_solver* s, int dom, const char* dir, double* t, int* step, int* fcount)
 {
+    Range nvtx("mpcf_restart");
     int rc = check_dom(s, dom);
     if (rc) return rc;
     const std::string info = join_path(dir, "save.info");
@@ -1368,6 +1397,7 @@ int mpcf_launch_shape(const mpcf_solver* s, long long* ntiles, long long* grid, 
 
 int mpcf_time_stages(mpcf_solver* s, int reps, double dtinvh, double* ms_per_stage)
 {
+    Range nvtx("mpcf_time_stages");
     if (!s || reps < 1) return fail(MPCF_ERR_ARG, "bad arguments");
     DeviceGuard g(s->device);
     s->sos_fresh = false;                   // the state (or the accumulator) changes
@@ -1398,6 +1428,7 @@ int mpcf_time_stages(mpcf_solver* s, int reps, double dtinvh, double* ms_per_sta
 
 int mpcf_autotune(mpcf_solver* s, int reps, int* best3, double* best_ms)
 {
+    Range nvtx("mpcf_autotune");
     if (!s) return fail(MPCF_ERR_ARG, "null solver");
     if (reps < 1) reps = 3;
     DeviceGuard g(s->device);
@@ -1515,6 +1546,7 @@ int mpcf_probe_fp32_peak(int device, double* tflops)
 
 int mpcf_time_run(mpcf_solver* s, int nsteps, double cfl, double dt_max, double* ms)
 {
+    Range nvtx("mpcf_time_run");
     if (!s || nsteps < 1 || !ms) return fail(MPCF_ERR_ARG, "bad arguments");
     DeviceGuard g(s->device);
     int rc = mpcf_run(s, 0, cfl, dt_max, 1, nullptr);   // builds the graphs
@@ -1543,6 +1575,7 @@ int mpcf_time_run(mpcf_solver* s, int nsteps, double cfl, double dt_max, double*
 
 int mpcf_update(mpcf_solver* s, double b)
 {
+    Range nvtx("mpcf_update");
     if (!s) return fail(MPCF_ERR_ARG, "null solver");
     DeviceGuard g(s->device);
     s->sos_fresh = false;                   // the state (or the accumulator) changes

@@ -125,18 +125,36 @@ struct DomRegs
     long long fs;
 };
 
+// Bounds-checking build (MPCF_CHECK_BOUNDS, libmpcf_b200_check.so): every
+// computed shared-memory and global index of the stage kernel is checked
+// against its region; one outside sets ERRBIT_BOUNDS and is clamped into the
+// region, so no access leaves its buffer (the results are then void).
+// Without the flag the checks compile to nothing.
+#ifdef MPCF_CHECK_BOUNDS
+template <class I> __device__ __forceinline__ I in_bounds(const I i, const I lo, const I hi, bool& oob)
+{
+    if (i < lo || i >= hi) { oob = true; return lo; }
+    return i;
+}
+#define MPCF_IN(i, lo, hi) in_bounds<decltype(i)>((i), (decltype(i))(lo), (decltype(i))(hi), oob)
+#else
+#define MPCF_IN(i, lo, hi) (i)
+#endif
+
 // Load the conserved state of (ix,iy,iz) (any integers: out-of-domain cells
 // are synthesised from the boundary conditions) and convert to primitives.
 template <class Pol>
 __device__ __forceinline__ void load_prim(const DomRegs& D, const typename Pol::T* __restrict__ U,
-                                          int ix, int iy, int iz, typename Pol::T q[7])
+                                          int ix, int iy, int iz, typename Pol::T q[7], bool& oob)
 {
+    (void)oob;
     typedef typename Pol::T T;
     bool fx, fy, fz;
     ix = bc_map(ix, D.nx, D.bc0, D.bc1, fx);
     iy = bc_map(iy, D.ny, D.bc2, D.bc3, fy);
     iz = bc_map(iz, D.nz, D.bc4, D.bc5, fz);
-    const long long idx = (long long)ix + (long long)D.nx * ((long long)iy + (long long)D.ny * iz);
+    const long long idx = MPCF_IN((long long)ix + (long long)D.nx * ((long long)iy + (long long)D.ny * iz),
+                                  0, (long long)D.nx * D.ny * D.nz);
     T c[7];
 #pragma unroll
     for (int k = 0; k < 7; ++k) c[k] = __ldg(U + k * D.fs + idx);
@@ -245,6 +263,10 @@ stage_kernel(const StageArgs A)
 {
     typedef typename Pol::T T;
     typedef StageLayout<T, TY, TMA> L;
+#ifdef MPCF_CHECK_BOUNDS
+    // slot 0 of a face plane, x or y faces
+    auto face_slot = [](const int d) { return (d >= L::kFx && d < L::kFx + L::kFP) || (d >= L::kFy && d < L::kFy + L::kFP); };
+#endif
     extern __shared__ __align__(16) unsigned char smem_dyn[];
     // 128-byte aligned base (bulk tensor copies need it for their targets)
     unsigned char* smem_raw = smem_dyn + ((128u - (smem_u32(smem_dyn) & 127u)) & 127u);
@@ -262,6 +284,7 @@ stage_kernel(const StageArgs A)
     const T b = (T)A.b;
     const T factor6 = (T)1.0f / (T)6.0f;   // GPUkernels.cu:1103
     bool ok = true;
+    bool oob = false;                      // bounds-checking build: an index left its buffer
     uint32_t phA = 0, phB = 0;             // mbarrier phase parities
     __shared__ T sos_w[TileShape<TY>::kWarps];   // per-warp maxima of the fused sound speed
     bool tma_late = false;
@@ -325,10 +348,11 @@ stage_kernel(const StageArgs A)
         for (int sl = z0 - 3; row && sl <= z0 + 1; ++sl)
         {
             T q[7];
-            load_prim<Pol>(D, U, gx, gy, sl, q);
+            load_prim<Pol>(D, U, gx, gy, sl, q, oob);
             const int slot = (sl + 6) % 6;
+            const int ri = MPCF_IN(slot * L::kRing + own, 0, L::kCurOff);
 #pragma unroll
-            for (int m = 0; m < 7; ++m) sm[m * L::kPP + slot * L::kRing + own] = q[m];
+            for (int m = 0; m < 7; ++m) sm[m * L::kPP + ri] = q[m];
         }
         if (use_tma && threadIdx.x == 0)
         {
@@ -373,16 +397,18 @@ stage_kernel(const StageArgs A)
                     }
                     bc_map(k + 2, D.nz, D.bc4, D.bc5, fz);
                     T c[7];
+                    const int bi = MPCF_IN(my * kTX + mx, 0, TY * kTX);
 #pragma unroll
-                    for (int m = 0; m < 7; ++m) c[m] = stB[(m * TY + my) * kTX + mx];
+                    for (int m = 0; m < 7; ++m) c[m] = stB[m * TY * kTX + bi];
                     if (fx) c[1] = -c[1];
                     if (fy) c[2] = -c[2];
                     if (fz) c[3] = -c[3];
                     to_primitive<Pol>(c, q);
                 }
-                else load_prim<Pol>(D, U, gx, gy, k + 2, q);
+                else load_prim<Pol>(D, U, gx, gy, k + 2, q, oob);
+                const int ri = MPCF_IN(slot * L::kRing + own, 0, L::kCurOff);
 #pragma unroll
-                for (int m = 0; m < 7; ++m) sm[m * L::kPP + slot * L::kRing + own] = q[m];
+                for (int m = 0; m < 7; ++m) sm[m * L::kPP + ri] = q[m];
             }
             // (B) slab k with halos into cur (slab k < nz: no z mapping)
             if (k < z1)
@@ -401,13 +427,15 @@ stage_kernel(const StageArgs A)
                         const int mx = min(max(bc_map(x0 + lx, D.nx, D.bc0, D.bc1, fx) - x0 + 4, 0), L::kAW - 1);
                         const int my = min(max(bc_map(y0 + ly, D.ny, D.bc2, D.bc3, fy) - y0 + 3, 0), L::kAH - 1);
                         T c[7], q[7];
+                        const int ai = MPCF_IN(my * L::kAW + mx, 0, L::kAH * L::kAW);
 #pragma unroll
-                        for (int m = 0; m < 7; ++m) c[m] = stA[(m * L::kAH + my) * L::kAW + mx];
+                        for (int m = 0; m < 7; ++m) c[m] = stA[m * L::kAH * L::kAW + ai];
                         if (fx) c[1] = -c[1];
                         if (fy) c[2] = -c[2];
                         to_primitive<Pol>(c, q);
+                        const int ci = MPCF_IN(L::kCurOff + (ly + 3) * L::kCurW + lx + 3, L::kCurOff, L::kPP);
 #pragma unroll
-                        for (int m = 0; m < 7; ++m) sm[m * L::kPP + L::kCurOff + (ly + 3) * L::kCurW + lx + 3] = q[m];
+                        for (int m = 0; m < 7; ++m) sm[m * L::kPP + ci] = q[m];
                     }
                 }
                 else
@@ -416,9 +444,11 @@ stage_kernel(const StageArgs A)
                     // the x/y stencils read (the corners are never read)
                     if (row)
                     {
+                        const int ci = MPCF_IN(L::kCurOff + (ty + 3) * L::kCurW + tx + 3, L::kCurOff, L::kPP);
+                        const int ri = MPCF_IN(slot * L::kRing + own, 0, L::kCurOff);
 #pragma unroll
                         for (int m = 0; m < 7; ++m)
-                            sm[m * L::kPP + L::kCurOff + (ty + 3) * L::kCurW + tx + 3] = sm[m * L::kPP + slot * L::kRing + own];
+                            sm[m * L::kPP + ci] = sm[m * L::kPP + ri];
                     }
                     if (use_tma)
                     {
@@ -452,15 +482,17 @@ stage_kernel(const StageArgs A)
                                 my = min(max(bc_map(y0 + ly, D.ny, D.bc2, D.bc3, fy) - y0 + 3, 0), L::kAH - 1);
                             }
                             T c[7];
+                            const int ai = MPCF_IN(my * L::kAW + mx, 0, L::kAH * L::kAW);
 #pragma unroll
-                            for (int m = 0; m < 7; ++m) c[m] = stA[(m * L::kAH + my) * L::kAW + mx];
+                            for (int m = 0; m < 7; ++m) c[m] = stA[m * L::kAH * L::kAW + ai];
                             if (fx) c[1] = -c[1];
                             if (fy) c[2] = -c[2];
                             to_primitive<Pol>(c, q);
                         }
-                        else load_prim<Pol>(D, U, x0 + lx, y0 + ly, k, q);
+                        else load_prim<Pol>(D, U, x0 + lx, y0 + ly, k, q, oob);
+                        const int ci = MPCF_IN(L::kCurOff + (ly + 3) * L::kCurW + lx + 3, L::kCurOff, L::kPP);
 #pragma unroll
-                        for (int m = 0; m < 7; ++m) sm[m * L::kPP + L::kCurOff + (ly + 3) * L::kCurW + lx + 3] = q[m];
+                        for (int m = 0; m < 7; ++m) sm[m * L::kPP + ci] = q[m];
                     }
                 }
             }
@@ -486,7 +518,14 @@ stage_kernel(const StageArgs A)
             // R and U of cell k-1 are first prefetched into L1, so that its
             // finalisation after the z face finds them.
             const bool fin = (k > z0) && valid;
+#ifdef MPCF_CHECK_BOUNDS
+            // cell k-1 of the own column: inside the domain's own planes
+            const long long idx = fin ? MPCF_IN((long long)gx + (long long)D.nx * ((long long)gy + (long long)D.ny * (k - 1)),
+                                                (long long)DD.zlo * DD.nx * DD.ny, (long long)(DD.zlo + DD.nz) * DD.nx * DD.ny)
+                                      : 0;
+#else
             const long long idx = (long long)gx + (long long)D.nx * ((long long)gy + (long long)D.ny * (k - 1));
+#endif
             if (fin)
             {
 #pragma unroll
@@ -561,7 +600,7 @@ stage_kernel(const StageArgs A)
                         const int zs = (cz + 4) % 6;
                         int ad[5];
 #pragma unroll
-                        for (int j = 0; j < 5; ++j) ad[j] = (zs + j < 6 ? zs + j : zs + j - 6) * L::kRing + own;
+                        for (int j = 0; j < 5; ++j) ad[j] = MPCF_IN((zs + j < 6 ? zs + j : zs + j - 6) * L::kRing + own, 0, L::kCurOff);
                         T Rv[7], Lv[7];
 #pragma unroll
                         for (int q = 0; q < 7; ++q)
@@ -614,6 +653,11 @@ stage_kernel(const StageArgs A)
                             else if (tx >= 16 && tx < 16 + TY) { base = L::kCurOff + (tx - 13) * L::kCurW + kTX + 3; step = 1; dL = L::kFx + (tx - 16) * (kTX + 1) + kTX; }
                             else continue;
                         }
+#ifdef MPCF_CHECK_BOUNDS
+                        if (base - 2 * step < L::kCurOff || base + 2 * step >= L::kPP) { oob = true; base = L::kCurOff + 2 * step; }
+                        if (dR >= 0 && !face_slot(dR)) { oob = true; dR = -1; }
+                        if (dL >= 0 && !face_slot(dL)) { oob = true; dL = -1; }
+#endif
                         T Rv[7], Lv[7];
 #pragma unroll
                         for (int q = 0; q < 7; ++q)
@@ -649,6 +693,9 @@ stage_kernel(const StageArgs A)
                                 dir = 0; src = L::kFx + tx * (kTX + 1) + kTX;
                             }
                         }
+#ifdef MPCF_CHECK_BOUNDS
+                        if (!face_slot(src)) { oob = true; continue; }
+#endif
                         // x: normal u, transverse v, w;  y: normal v, transverse u, w
                         T* pl = sm + src;
                         const int nq = 1 + dir, tq = 2 - dir;
@@ -675,8 +722,9 @@ stage_kernel(const StageArgs A)
             // (F) x/y part of cell k, carried to the next slab
             if (k < z1 && row)
             {
-                const T* fx = sm + L::kFx + ty * (kTX + 1) + tx;
-                const T* fy = sm + L::kFy + ty * kTX + tx;
+                // the slot right of / above the cell is read too
+                const T* fx = sm + L::kFx + MPCF_IN(ty * (kTX + 1) + tx, 0, L::kFP - 1);
+                const T* fy = sm + L::kFy + MPCF_IN(ty * kTX + tx, 0, L::kFP - kTX);
 #pragma unroll
                 for (int m = 0; m < 7; ++m)
                     Sp[m] = ((fx[m * L::kFP + 1] - fx[m * L::kFP]) + fy[m * L::kFP + kTX]) - fy[m * L::kFP];
@@ -735,6 +783,9 @@ stage_kernel(const StageArgs A)
 
     if (!__all_sync(0xffffffffu, ok) && tx == 0) atomicOr(A.err, (unsigned)ERRBIT_NONPHYSICAL);
     if (TMA && tma_late) atomicOr(A.err, (unsigned)ERRBIT_TMA_TIMEOUT);
+#ifdef MPCF_CHECK_BOUNDS
+    if (__any_sync(0xffffffffu, oob) && tx == 0) atomicOr(A.err, (unsigned)ERRBIT_BOUNDS);
+#endif
 }
 
 template <class Pol, int TY, bool TMA>

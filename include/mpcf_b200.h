@@ -57,6 +57,8 @@ typedef struct mpcf_solver mpcf_solver;
 #define MPCF_ERRBIT_NONPHYSICAL  1u  /* rho<=0, E<=0, G<=0, P<0 or non-finite after an update */
 #define MPCF_ERRBIT_SOS          2u  /* maximum speed of sound not finite or not positive */
 #define MPCF_ERRBIT_TMA_TIMEOUT  4u  /* a bulk tensor copy did not complete within the wait limit */
+#define MPCF_ERRBIT_BOUNDS       8u  /* bounds-checking build (libmpcf_b200_check.so): a stage-kernel index
+                                        left its buffer; it was clamped into it and the results are void */
 
 /* stage-kernel tiling flags (mpcf_set_tiling / mpcf_get_tiling / mpcf_autotune) */
 #define MPCF_TILE_PERSISTENT 1  /* one CTA per resident slot pulling tiles from a work counter */
