@@ -182,3 +182,34 @@ def test_slab_initial_conditions_match_undivided_domain(mpcf, prec):
                 ic(s, r)
             got = dc.gather_state(s, ext_, with_reg=False)
         assert_bitwise(got, want, f"{name} initial condition over 3 slabs")
+
+
+def test_linked_slabs_autotune_and_restart(mpcf, tmp_path):
+    """The autotuner's trial stages on linked slabs exchange their ghost
+    planes too and leave the state as it was; each slab saves and restarts
+    like a domain; a run continued from the restarted slabs equals the
+    undivided run bit for bit."""
+    prec = "mixed"
+    U0 = _state(prec, mpcf)
+    t_ref, (U_ref, R_ref) = _undivided(mpcf, prec, U0, 4, True)
+    s, ext = dc.slab_solver(DIMS, 3, bc=BC, precision=prec)
+    with s:
+        dc.scatter_state(s, DIMS, ext, U0)
+        before = dc.gather_state(s, ext)
+        s.autotune(reps=1)
+        after = dc.gather_state(s, ext)
+        assert_bitwise(after[0], before[0], "state after autotune")
+        t2 = s.run(2, cfl=0.3, graph=True)
+        for r in range(3):
+            d = tmp_path / f"slab{r}"
+            d.mkdir()
+            s.save(d, t2[r], 2, dom=r)
+    s2, _ = dc.slab_solver(DIMS, 3, bc=BC, precision=prec)
+    with s2:
+        for r in range(3):
+            t, step, _ = s2.restart(tmp_path / f"slab{r}", dom=r)
+            assert step == 2
+        t4 = s2.run(2, cfl=0.3, graph=True)
+        U, _ = dc.gather_state(s2, ext)
+    assert t4 == pytest.approx([t_ref[0]] * 3, rel=1e-14)
+    assert_bitwise(U, U_ref, "state after save, restart and two more steps")
