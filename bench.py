@@ -349,8 +349,11 @@ def main():
     if not args.no_e2e:
         ke = max(2, min(K, 4))
         e2e = e2e_measure(mpcf, cfg, K=ke, W=1, cfl=cfl, dist=dist, precision=args.precision)
-        e2e["with_register"] = e2e_measure(mpcf, cfg, K=ke, W=1, cfl=cfl, dist=dist,
-                                           precision=args.precision, with_register=True)
+        if world == 1:
+            # informational: the register moved too (7.5 GB more pinned host
+            # memory, so not on every rank of a multi-GPU run)
+            e2e["with_register"] = e2e_measure(mpcf, cfg, K=ke, W=1, cfl=cfl, dist=dist,
+                                               precision=args.precision, with_register=True)
 
     # ---------------- CPU baseline (rank 0, N=1 only)
     cpu = None
