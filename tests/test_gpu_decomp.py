@@ -78,6 +78,13 @@ def test_halo_faces_are_validated(mpcf):
         s.link_z(0, 1)
         with pytest.raises(mpcf.MpcfError):
             s.link_z(0, 1)                  # already linked
+        with pytest.raises(mpcf.MpcfError):
+            s.set_origin((0, 0, 9), (16, 16, 16), dom=0)     # planes 9..16 past the global extent
+        with pytest.raises(mpcf.MpcfError):
+            s.set_origin((0, -1, 0), (16, 16, 16), dom=0)    # negative origin
+        with pytest.raises(mpcf.MpcfError):
+            s.set_spacing(0.0, dom=0)                         # spacing must be positive
+        s.set_origin((0, 0, 8), (16, 16, 16), dom=1)
 
 
 def test_rank_driver_halo_views(mpcf):
