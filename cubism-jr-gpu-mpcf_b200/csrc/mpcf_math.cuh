@@ -369,37 +369,31 @@ __device__ __forceinline__ void hllc_face_packed(const FaceState<float>& S, cons
     const float2 chi = mul2(SU, rcp2(sub2(f2(sm, sp), SS)));
     const float2 Wb  = f2(0.5f * (float)(1 + s), 0.5f * (float)(1 - s));
 
+    // every advected quantity X has the star-state flux S (X chi - X) + X u
+    // = X V with V = S (chi - 1) + u, the extra-term velocity's argument too
+    const float2 V = fma2(Sg, add2(chi, f2s(-1.0f)), Uh);
     // rho, G, P (passive)
-    o.f[0] = blend2(Wb, fma2(Sg, fma2(Rh, chi, f2(-S.rm, -S.rp)), mul2(Rh, Uh)));
-    o.f[5] = blend2(Wb, fma2(Sg, fma2(Gh, chi, f2(-S.Gm, -S.Gp)), mul2(Gh, Uh)));
-    o.f[6] = blend2(Wb, fma2(Sg, fma2(Qh, chi, f2(-S.Pm, -S.Pp)), mul2(Qh, Uh)));
-    // normal momentum
-    float fn;
-    {
-        const float2 Q = mul2(Rh, Uh);
-        const float2 qd = sub2(mul2(mul2(Rh, SS), chi), Q);
-        fn = blend2(Wb, fma2(Sg, qd, fma2(Q, Uh, Ph)));
-    }
+    o.f[0] = blend2(Wb, mul2(Rh, V));
+    o.f[5] = blend2(Wb, mul2(Gh, V));
+    o.f[6] = blend2(Wb, mul2(Qh, V));
+    // normal momentum: S (rho s* chi - rho u) + rho u^2 + p
+    // = rho (S (s* chi - u) + u^2) + p
+    const float2 U2 = mul2(Uh, Uh);
+    const float fn = blend2(Wb, fma2(Rh, fma2(Sg, fma2(SS, chi, f2(-um, -up)), U2), Ph));
     // transverse momenta
-    float ft1, ft2;
-    {
-        const float2 Q = mul2(Rh, T1);
-        ft1 = blend2(Wb, fma2(Sg, sub2(mul2(Q, chi), Q), mul2(Q, Uh)));
-    }
-    {
-        const float2 Q = mul2(Rh, T2);
-        ft2 = blend2(Wb, fma2(Sg, sub2(mul2(Q, chi), Q), mul2(Q, Uh)));
-    }
+    const float2 RV = mul2(Rh, V);
+    const float ft1 = blend2(Wb, mul2(T1, RV));
+    const float ft2 = blend2(Wb, mul2(T2, RV));
     // energy
     {
-        const float2 ke = fma2(T2, T2, fma2(T1, T1, mul2(Uh, Uh)));
+        const float2 ke = fma2(T2, T2, fma2(T1, T1, U2));
         const float2 Q  = fma2(mul2(f2s(0.5f), Rh), ke, fma2(Gh, Ph, Qh));
         const float2 inner = fma2(Rh, SS, mul2(Ph, rcp2(SU)));
         const float2 qd = sub2(mul2(chi, fma2(sub2(SS, Uh), inner, Q)), Q);
         o.f[4] = blend2(Wb, fma2(Sg, qd, mul2(Uh, add2(Q, Ph))));
     }
     // extra-term velocity
-    o.vel = blend2(Wb, fma2(Sg, add2(chi, f2s(-1.0f)), Uh));
+    o.vel = blend2(Wb, V);
 
     o.f[1] = dir == 0 ? fn : ft1;
     o.f[2] = dir == 1 ? fn : (dir == 0 ? ft1 : ft2);
