@@ -337,8 +337,11 @@ __device__ __forceinline__ void hllc_face(const FaceState<typename Pol::T>& S, c
 
 // The same face in the fast policies: every left/right-symmetric quantity is
 // one packed pair (lane x = minus / left, lane y = plus / right) and the
-// divisions are single-precision reciprocals.  The operations follow
-// hllc_face above term by term.
+// divisions are single-precision reciprocals.  The wave speeds follow
+// hllc_face above term by term; the fluxes are the same expressions
+// factored: the advected quantities share V = S (chi - 1) + u, and the
+// energy flux cancels the (s - u) of chi against the p/(s - u) of the
+// reference's star-state energy.
 __device__ __forceinline__ void hllc_face_packed(const FaceState<float>& S, const int dir, FaceOut<float>& o)
 {
     const float2 Rh = f2(S.rm, S.rp), Uh = f2(S.nm, S.np), Ph = f2(S.pm, S.pp);
@@ -366,7 +369,8 @@ __device__ __forceinline__ void hllc_face_packed(const FaceState<float>& S, cons
     const int s = sign_star_of(ss);
     const float2 Sg  = f2(fminf(0.0f, sm), fmaxf(0.0f, sp));
     const float2 SS  = f2s(ss);
-    const float2 chi = mul2(SU, rcp2(sub2(f2(sm, sp), SS)));
+    const float2 Dinv = rcp2(sub2(f2(sm, sp), SS));           // 1/(s - s*)
+    const float2 chi = mul2(SU, Dinv);
     const float2 Wb  = f2(0.5f * (float)(1 + s), 0.5f * (float)(1 - s));
 
     // every advected quantity X has the star-state flux S (X chi - X) + X u
@@ -384,13 +388,14 @@ __device__ __forceinline__ void hllc_face_packed(const FaceState<float>& S, cons
     const float2 RV = mul2(Rh, V);
     const float ft1 = blend2(Wb, mul2(T1, RV));
     const float ft2 = blend2(Wb, mul2(T2, RV));
-    // energy
+    // energy: S (chi (Q + (s* - u)(rho s* + p/(s - u))) - Q) + u (Q + p)
+    // = Q V + S (s* - u)(rho s* (s - u) + p)/(s - s*) + u p, Q = E
     {
         const float2 ke = fma2(T2, T2, fma2(T1, T1, U2));
         const float2 Q  = fma2(mul2(f2s(0.5f), Rh), ke, fma2(Gh, Ph, Qh));
-        const float2 inner = fma2(Rh, SS, mul2(Ph, rcp2(SU)));
-        const float2 qd = sub2(mul2(chi, fma2(sub2(SS, Uh), inner, Q)), Q);
-        o.f[4] = blend2(Wb, fma2(Sg, qd, mul2(Uh, add2(Q, Ph))));
+        const float2 inner = fma2(mul2(Rh, SS), SU, Ph);
+        const float2 A = mul2(Sg, mul2(sub2(SS, Uh), Dinv));
+        o.f[4] = blend2(Wb, fma2(Q, V, fma2(A, inner, mul2(Uh, Ph))));
     }
     // extra-term velocity
     o.vel = blend2(Wb, V);
