@@ -370,12 +370,14 @@ __device__ __forceinline__ void hllc_face_packed(const FaceState<float>& S, cons
     const float2 Sg  = f2(fminf(0.0f, sm), fmaxf(0.0f, sp));
     const float2 SS  = f2s(ss);
     const float2 Dinv = rcp2(sub2(f2(sm, sp), SS));           // 1/(s - s*)
-    const float2 chi = mul2(SU, Dinv);
+    const float2 D   = sub2(SS, Uh);                          // s* - u
+    const float2 C1  = mul2(D, Dinv);                         // chi - 1 = (s* - u)/(s - s*)
     const float2 Wb  = f2(0.5f * (float)(1 + s), 0.5f * (float)(1 - s));
 
     // every advected quantity X has the star-state flux S (X chi - X) + X u
     // = X V with V = S (chi - 1) + u, the extra-term velocity's argument too
-    const float2 V = fma2(Sg, add2(chi, f2s(-1.0f)), Uh);
+    const float2 A = mul2(Sg, C1);
+    const float2 V = add2(A, Uh);
     // rho, G, P (passive)
     o.f[0] = blend2(Wb, mul2(Rh, V));
     o.f[5] = blend2(Wb, mul2(Gh, V));
@@ -383,7 +385,8 @@ __device__ __forceinline__ void hllc_face_packed(const FaceState<float>& S, cons
     // normal momentum: S (rho s* chi - rho u) + rho u^2 + p
     // = rho (S (s* chi - u) + u^2) + p
     const float2 U2 = mul2(Uh, Uh);
-    const float fn = blend2(Wb, fma2(Rh, fma2(Sg, fma2(SS, chi, f2(-um, -up)), U2), Ph));
+    // (s* chi - u = s* (chi - 1) + s* - u)
+    const float fn = blend2(Wb, fma2(Rh, fma2(Sg, fma2(SS, C1, D), U2), Ph));
     // transverse momenta
     const float2 RV = mul2(Rh, V);
     const float ft1 = blend2(Wb, mul2(T1, RV));
@@ -394,7 +397,6 @@ __device__ __forceinline__ void hllc_face_packed(const FaceState<float>& S, cons
         const float2 ke = fma2(T2, T2, fma2(T1, T1, U2));
         const float2 Q  = fma2(mul2(f2s(0.5f), Rh), ke, fma2(Gh, Ph, Qh));
         const float2 inner = fma2(mul2(Rh, SS), SU, Ph);
-        const float2 A = mul2(Sg, mul2(sub2(SS, Uh), Dinv));
         o.f[4] = blend2(Wb, fma2(Q, V, fma2(A, inner, mul2(Uh, Ph))));
     }
     // extra-term velocity
