@@ -25,12 +25,13 @@
 //     k-1: rhs = a*R - dtinvh*div(F) (with the G/P extra terms),
 //     R <- rhs, U_next <- b*rhs + U;
 //   * x, y: every column thread writes its cell's edge values into the face
-//     slots in shared memory; the helper warp (warps 0..4 without one)
-//     reconstructs the ghost cells around the tile (rows -1 and TY,
-//     columns -1 and 32); after a barrier each face is evaluated in place
-//     in its slot, the x face left of every cell and the y face below it
-//     by the cell's thread, the faces above and right of the tile by the
-//     helper, so no warp takes more than one extra job per slab;
+//     slots in shared memory; the helper warp reconstructs the ghost cells
+//     around the tile (rows -1 and TY, columns -1 and 32; without a helper
+//     warps 0..2 take one job each, or every warp a share of their planes
+//     in the reference-rounding forms); after a barrier each face is
+//     evaluated in place in its slot, the x face left of every cell and the
+//     y face below it by the cell's thread, the faces above and right of
+//     the tile by the helper (warps 3 and 4 without one);
 //   * after a second barrier every cell gathers its x/y flux differences,
 //     carried to its finalisation in the next slab.
 // Each cell is converted to primitives once per stage (the reference
@@ -240,8 +241,9 @@ __device__ __forceinline__ void tma_load_4d(uint32_t dst, const void* tmap, int 
 #endif
 // Tile heights of the form 2^n - 1 (3, 7, 15) carry a helper warp that
 // takes the tile's extra jobs (ghost rows and columns, the faces above and
-// right of the tile); other heights (8) give them to warps 0..4, one each,
-// which suits domains whose y extents are multiples of 8.
+// right of the tile); other heights (8) give them to warps 0..4, one each
+// (the reference-rounding forms spread the ghost reconstructions over all
+// warps), which suits domains whose y extents are multiples of 8.
 template <int TY> struct TileShape
 {
     static constexpr bool kHelper = ((TY + 1) & TY) == 0;
@@ -256,6 +258,22 @@ template <class T, int TY> struct MinBlocks
 
 // Threads of one CTA: TY column warps and, with a helper, the helper warp.
 template <int TY> __host__ __device__ constexpr int stage_threads() { return kTX * TileShape<TY>::kWarps; }
+
+// Ghost job g of a tile (0: row -1, 1: row TY, 2: columns -1 and 32) for
+// lane tx: the centre of the stencil in the cur slab, its step, and the face
+// slot that takes the edge value (dR: a minus slot, from the right / upper
+// edge; dL: a plus slot, from the left / lower edge).  Columns -1 and 32
+// take lanes 0..TY-1 and 16..15+TY; false for the idle lanes.
+template <class L, int TY>
+__device__ __forceinline__ bool ghost_job(const int g, const int tx, int& base, int& step, int& dR, int& dL)
+{
+    if (g == 0)      { base = L::kCurOff + 2 * L::kCurW + tx + 3;        step = L::kCurW; dR = L::kFy + tx; }
+    else if (g == 1) { base = L::kCurOff + (TY + 3) * L::kCurW + tx + 3; step = L::kCurW; dL = L::kFy + TY * kTX + tx; }
+    else if (tx < TY)                  { base = L::kCurOff + (tx + 3) * L::kCurW + 2;        step = 1; dR = L::kFx + tx * (kTX + 1); }
+    else if (tx >= 16 && tx < 16 + TY) { base = L::kCurOff + (tx - 13) * L::kCurW + kTX + 3; step = 1; dL = L::kFx + (tx - 16) * (kTX + 1) + kTX; }
+    else return false;
+    return true;
+}
 
 template <class Pol, int TY, bool PERSIST, bool SUMS, bool TMA>
 __global__ void __launch_bounds__(stage_threads<TY>(), MinBlocks<typename Pol::T, TY>::v)
@@ -580,14 +598,15 @@ stage_kernel(const StageArgs A)
                 //     right / upper edge to the minus side of the face right
                 //     of / above the cell, the left / lower edge to the plus
                 //     side of the face left of / below it.  The helper warp
-                //     (warps 0..2 without one) reconstructs the ghost cells
-                //     around the tile: row -1, row TY, columns -1 and 32;
+                //     (without one: warps 0..2, or all warps in shares)
+                //     reconstructs the ghost cells around the tile: row -1,
+                //     row TY, columns -1 and 32;
                 //  3. after a barrier, the x face left of the own cell and the
                 //     y face below it, each evaluated in place in its slot;
                 //     the helper (warps 3 and 4 without one) evaluates the y
                 //     faces above the tile and the x faces right of it.  Without
-                //     a helper no warp takes more than one of the five extra
-                //     jobs, which keeps the warps even at the barriers.
+                //     a helper no warp takes more than one of the extra jobs,
+                //     which keeps the warps even at the barriers.
                 constexpr bool kHelper = TileShape<TY>::kHelper;
                 static_assert(TY <= 16, "ghost columns -1 and 32 take lanes 0..TY-1 and 16..15+TY");
                 static_assert(kHelper || TY >= 5, "without a helper, warps 0..4 take the extra jobs");
@@ -631,7 +650,13 @@ stage_kernel(const StageArgs A)
                 constexpr int kXYUnroll = Pol::kFastWeno ? 2 : 1;
                 if (k < z1)
                 {
-                    const int nr = row ? ((!kHelper && ty < 3) ? 3 : 2) : 3;
+                    // Own cells (x, then y) and the three ghost jobs: with a
+                    // helper, the helper warp takes them whole (it has no z
+                    // part); without one, in the fast forms warps 0..2 take
+                    // one each, and in the other forms every warp takes a
+                    // share of their 21 planes (below).
+                    constexpr bool kSplitGhosts = !kHelper && !Pol::kFastWeno;
+                    const int nr = row ? ((!kHelper && !kSplitGhosts && ty < 3) ? 3 : 2) : 3;
 #pragma unroll kXYUnroll
                     for (int j = 0; j < nr; ++j)
                     {
@@ -644,15 +669,7 @@ stage_kernel(const StageArgs A)
                             dL = j ? L::kFy + ty * kTX + tx : L::kFx + ty * (kTX + 1) + tx;
                             dR = j ? dL + kTX : dL + 1;
                         }
-                        else
-                        {
-                            const int g = row ? ty : j;   // 0: row -1, 1: row TY, 2: columns -1 and 32
-                            if (g == 0)      { base = L::kCurOff + 2 * L::kCurW + tx + 3;        step = L::kCurW; dR = L::kFy + tx; }
-                            else if (g == 1) { base = L::kCurOff + (TY + 3) * L::kCurW + tx + 3; step = L::kCurW; dL = L::kFy + TY * kTX + tx; }
-                            else if (tx < TY)                { base = L::kCurOff + (tx + 3) * L::kCurW + 2;        step = 1; dR = L::kFx + tx * (kTX + 1); }
-                            else if (tx >= 16 && tx < 16 + TY) { base = L::kCurOff + (tx - 13) * L::kCurW + kTX + 3; step = 1; dL = L::kFx + (tx - 16) * (kTX + 1) + kTX; }
-                            else continue;
-                        }
+                        else if (!ghost_job<L, TY>(row ? ty : j, tx, base, step, dR, dL)) continue;
 #ifdef MPCF_CHECK_BOUNDS
                         if (base - 2 * step < L::kCurOff || base + 2 * step >= L::kPP) { oob = true; base = L::kCurOff + 2 * step; }
                         if (dR >= 0 && !face_slot(dR)) { oob = true; dR = -1; }
@@ -674,6 +691,39 @@ stage_kernel(const StageArgs A)
                         {
 #pragma unroll
                             for (int q = 0; q < 7; ++q) sm[dL + (7 + q) * L::kFP] = Lv[q];
+                        }
+                    }
+                    if constexpr (kSplitGhosts)
+                    {
+                        // The 21 planes of the ghost jobs (3 jobs x 7
+                        // quantities) in contiguous ranges over the warps
+                        // (TY = 8: warps 0..4 take 3, the others 2), so that no
+                        // warp reaches the barrier 7 planes after another.  In
+                        // the reference-rounding forms this is 5% faster at
+                        // TY = 8; the fast forms lose the independent chains of
+                        // a whole job and are 3% slower with it.
+                        constexpr int kPer = 21 / TY, kRem = 21 % TY;
+                        int gi = ty * kPer + (ty < kRem ? ty : kRem);
+                        const int ge = gi + kPer + (ty < kRem ? 1 : 0);
+#pragma unroll 1
+                        for (; gi < ge; ++gi)
+                        {
+                            const int g = gi >= 14 ? 2 : (gi >= 7 ? 1 : 0);
+                            const int q = gi - 7 * g;
+                            int base, step, dR = -1, dL = -1;
+                            if (!ghost_job<L, TY>(g, tx, base, step, dR, dL)) continue;
+#ifdef MPCF_CHECK_BOUNDS
+                            if (base - 2 * step < L::kCurOff || base + 2 * step >= L::kPP) { oob = true; base = L::kCurOff + 2 * step; }
+                            if (dR >= 0 && !face_slot(dR)) { oob = true; continue; }
+                            if (dL >= 0 && !face_slot(dL)) { oob = true; continue; }
+#endif
+                            const T* pl = sm + q * L::kPP + base;
+                            T rv, lv;
+                            weno_cell<Pol>(pl[-2 * step], pl[-step], pl[0], pl[step], pl[2 * step], rv, lv);
+                            // the right / upper edge fills a minus slot, the
+                            // left / lower edge a plus slot
+                            if (dR >= 0) sm[dR + q * L::kFP] = rv;
+                            else         sm[dL + (7 + q) * L::kFP] = lv;
                         }
                     }
                     __syncthreads();
