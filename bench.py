@@ -205,6 +205,18 @@ def sample_dims(dims, target=4 << 20):
     return (nx, ny, max(1, min(nz, -(-target // (nx * ny)))))
 
 
+def cpu_model():
+    """The host CPU's model name (first entry of /proc/cpuinfo), or None."""
+    try:
+        with open("/proc/cpuinfo") as f:
+            for line in f:
+                if line.startswith("model name"):
+                    return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return None
+
+
 def reference_arm(args):
     rank, world, _ = env_rank()
     if rank != 0:
@@ -245,7 +257,8 @@ def reference_arm(args):
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": 3.0 * ncell / value * 1e3,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
             "data": "synthetic", "config": {"workload": args.workload, "sample": f"{sub[0]}x{sub[1]}x{sub[2]} slab, 1 LSRK3 step"},
-            "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "port", "sample": sample},
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "port", "sample": sample,
+                             "cpu_model": cpu_model()},
             "reference_sos_cpu": sos,
             "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
@@ -363,7 +376,7 @@ def main():
         v, dtc = cpu_sample(cfg["params"], cfg["bubbles"][0], sub, cores)
         cpu = {"value": v, "unit": UNIT, "cores": cores, "kind": "port",
                "sample": "C restatement of the reference kernels (oracle/), OpenMP, one LSRK3 step of a "
-                         "512x512x16 slab of the workload (%.1f s)" % dtc}
+                         "512x512x16 slab of the workload (%.1f s)" % dtc, "cpu_model": cpu_model()}
 
     if rank == 0:
         fp32_peak = ctypes.c_double()

@@ -1426,6 +1426,44 @@ int mpcf_time_stages(mpcf_solver* s, int reps, double dtinvh, double* ms_per_sta
     return MPCF_OK;
 }
 
+// z-chunk depths the autotuner tries for tile height ty: 16, 32, 64 and 128
+// below the deepest domain, and the whole depth.  When 16-deep chunks do not
+// fill one wave of resident CTAs (small domains), also the shallowest depth
+// whose CTAs still fit in one wave, and 8: a CTA walks its chunk slab by
+// slab, so there the chunk depth is the latency of the stage (64^3, mixed:
+// 4-deep chunks of 32x8 tiles, 256 CTAs, run a step 1.9x faster than the
+// best 16-deep tiling).
+static std::vector<int> dz_candidates(mpcf_solver* s, int ty, int maxn, bool tma)
+{
+    auto tiles = [&](int dz)
+    {
+        long long t = 0;
+        for (auto& D : s->hdoms) t += (long long)((D.nx + 31) / 32) * ((D.ny + ty - 1) / ty) * ((D.nz + dz - 1) / dz);
+        return t;
+    };
+    std::vector<int> dzs;
+    for (int v : {16, 32, 64, 128}) if (v < maxn) dzs.push_back(v);
+    dzs.push_back(maxn);
+    const StageKernelInfo I = stage_info(s, ty, false, false, tma);
+    int nb = 0;
+    if (!I.fn || cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, I.fn, stage_block_threads(ty), I.smem) != cudaSuccess || nb < 1)
+    {
+        cudaGetLastError();
+        nb = 1;
+    }
+    const long long slots = (long long)nb * s->num_sms;
+    if (maxn > 4 && tiles(std::min(16, maxn)) < slots)
+    {
+        int fit = 0;
+        for (int dz = 4; dz < 16 && dz < maxn && !fit; ++dz) if (tiles(dz) <= slots) fit = dz;
+        if (fit) dzs.push_back(fit);
+        if (fit != 8 && 8 < maxn) dzs.push_back(8);
+    }
+    std::sort(dzs.begin(), dzs.end());
+    dzs.erase(std::unique(dzs.begin(), dzs.end()), dzs.end());
+    return dzs;
+}
+
 int mpcf_autotune(mpcf_solver* s, int reps, int* best3, double* best_ms)
 {
     Range nvtx("mpcf_autotune");
@@ -1457,14 +1495,11 @@ int mpcf_autotune(mpcf_solver* s, int reps, int* best3, double* best_ms)
     {
         int maxn = 0;
         for (auto& D : s->hdoms) maxn = std::max(maxn, D.nz);
-        std::vector<int> dzs;
-        for (int v : {16, 32, 64, 128}) if (v < maxn) dzs.push_back(v);
-        dzs.push_back(maxn);
         const int tys[4] = {3, 7, 8, 15};
         for (int i = 0; i < 4 && !rc; ++i)
         {
             if (!valid_ty(s, tys[i])) continue;
-            for (int dz : dzs)
+            for (int dz : dz_candidates(s, tys[i], maxn, can_tma))
             {
                 for (int f = 0; f < 4 && !rc; ++f)
                 {

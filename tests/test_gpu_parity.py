@@ -71,7 +71,7 @@ def test_ref32_stage_bitexact(mpcf, dims, bc):
 
 @pytest.mark.parametrize("tiling", [(3, 3, False, False), (3, 64, False, True), (7, 5, True, True), (15, 7, False, True),
                                     (3, 1, True, True), (7, 9, True, False), (15, 2, True, True), (8, 4, True, True),
-                                    (8, 64, False, False)])
+                                    (8, 64, False, False), (3, 5, False, True)])
 @pytest.mark.parametrize("dims", [(45, 19, 14), (44, 19, 14)])
 def test_ref32_tiling_invariant(mpcf, tiling, dims):
     # rows of 45 floats are not 16-byte multiples (ordinary loads even with
@@ -177,7 +177,7 @@ def test_ensemble_matches_single_domains(mpcf):
 # fast FP32, mixed and FP64
 # ---------------------------------------------------------------------------
 FAST_TILINGS = [(3, 3, False, False), (3, 64, False, True), (7, 5, True, True), (7, 9, True, False),
-                (7, 64, False, True), (8, 4, True, True), (8, 64, False, False), (8, 7, True, True)]
+                (7, 64, False, True), (8, 4, True, True), (8, 64, False, False), (8, 7, True, True), (8, 4, False, True)]
 
 
 @pytest.mark.parametrize("prec", ["fp32", "mixed"])
