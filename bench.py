@@ -46,6 +46,10 @@ BYTES_PER_CELL_STAGE = {"fp32_ref": 112, "fp32": 112, "mixed": 112, "fp64": 224}
 # full-size launch over the 512^3 cloud, 134.2 M cells, 32 x 8 tiles over
 # whole columns, persistent, bulk-copy staging: a one-pass capture).  The
 # per-launch figure of the bench line is this times the workload's cells.
+# the arithmetic each precision form computes in, and its name in the workload
+DTYPE_OF = {"mixed": "f32+f64 (mixed)", "fp32": "f32", "fp32_ref": "f32 (reference rounding)", "fp64": "f64"}
+FORM_OF = {"mixed": "mixed form", "fp32": "fast FP32 form", "fp32_ref": "FP32 reference-rounding form",
+           "fp64": "FP64 form"}
 MEASURED_DRAM_BYTES_PER_CELL_STAGE = {"mixed": 16.39e9 / 512 ** 3}
 
 
@@ -386,8 +390,8 @@ def main():
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": K, "warmup": W,
             "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-            "dtype": "f32+f64 (mixed)", "data": "synthetic",
-            "config": {"workload": cfg["name"] + ": " + cfg["desc"] + ", absorbing, CFL 0.3, mixed form",
+            "dtype": DTYPE_OF[args.precision], "data": "synthetic",
+            "config": {"workload": cfg["name"] + ": " + cfg["desc"] + ", absorbing, CFL 0.3, " + FORM_OF[args.precision],
                        "cells_per_gpu": ncell, "l2": "inputs 11 GB > 126 MB L2 (no flush needed)",
                        "parallelism": "replicas" if world > 1 else "single GPU",
                        "tiling": {"ty": tiling[0], "dz": tiling[1], "persistent": tiling[2], "tma": tiling[3]},
