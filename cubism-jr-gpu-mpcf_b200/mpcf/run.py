@@ -45,6 +45,8 @@ reference reads them:
 - SICCloudMPI: -rho0 -u0 -p0 -rhoB -uB -pB -pressureratio -shockNx/Ny/Nz
   -shockSx/Sy/Sz -g1 -g2 -pc1 -pc2.  Shapes come from cloud.dat: one
   "idx x y z r" line each (Sim_SICCloudMPI.h:148-173).
+- StaticIC: -config (xy, ...) -fname: a running cell count in every field,
+  dumped once; no steps and no run options.
 """
 import os
 import sys
@@ -55,7 +57,7 @@ import numpy as np
 from . import solver as S
 from ._lib import PRECISIONS, MpcfError
 
-CASES = ("SteadyStateMPI", "SodMPI", "2DSBIMPI", "SICCloudMPI")
+CASES = ("SteadyStateMPI", "SodMPI", "2DSBIMPI", "SICCloudMPI", "StaticIC")
 CASE_FLAGS = {
     "SteadyStateMPI": ("rho", "u", "v", "w", "p", "g", "pc"),
     "SodMPI": ("x0", "rho1", "rho2", "u1", "u2", "p1", "p2", "g1", "g2", "pc1", "pc2"),
@@ -178,7 +180,13 @@ class Simulation:
         if self.case not in CASES:
             raise ArgumentError(f"Unknown simulation case {self.case}")
         self.dryrun = a.bool("dryrun")
-        if not self.dryrun:
+        if self.case == "StaticIC":
+            # Sim_StaticIC::_setup parses no run options (Sim_StaticIC.cpp:61-71)
+            self.config = a.str("config")
+            if sorted(self.config) not in (sorted(c) for c in ("xy", "xz", "yz")) or len(self.config) != 2:
+                raise ArgumentError(f"-config {self.config} is not possible")
+            self.fname = a.str("fname", "staticIC")
+        elif not self.dryrun:
             self.tend = a.float("tend")
             self.cfl = a.float("cfl")
             self.nslices = a.int("nslices")
@@ -253,7 +261,26 @@ class Simulation:
             if self.verbosity:
                 self.log("tiling %s: %.3f ms per stage" % (best, ms))
 
+    def static_ic(self):
+        """Sim_StaticIC (Sim_StaticIC.cpp:74-96): every field of every cell
+        holds a running count, axis config[0] fastest, then config[1], then
+        the third; dumped once as <fname>_0000."""
+        n = dict(zip("xyz", self.dims))
+        fast, mid = self.config
+        slow = ({"x", "y", "z"} - {fast, mid}).pop()
+        z, y, x = np.meshgrid(np.arange(n["z"]), np.arange(n["y"]), np.arange(n["x"]), indexing="ij")
+        i = {"x": x, "y": y, "z": z}
+        cnt = i[fast] + n[fast] * (i[mid] + n[mid] * i[slow])
+        os.makedirs(self.fpath, exist_ok=True)
+        self.solver = S.Solver([self.dims], bc=[S.case_bc("sod")], precision=self.precision)
+        field = cnt.astype(self.solver.dtype).ravel()
+        self.solver.set_state([field] * 7)
+        self._dump(self.fname)
+
     def run(self):
+        if self.case == "StaticIC":
+            self.static_ic()
+            return
         if self.dryrun:
             # the reference sets up its host grid and allocates no GPU; here
             # the solver is the GPU, so a dry run only checks the arguments

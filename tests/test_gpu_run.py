@@ -84,3 +84,25 @@ def test_cases_start_from_the_api_initial_condition(tmp_path, monkeypatch, case)
         api(s)
         s.dump(tmp_path / "api", "ic", 0)
     assert (tmp_path / "run" / "data_0000.bin").read_bytes() == (tmp_path / "api" / "ic.bin").read_bytes()
+
+
+@pytest.mark.parametrize("config", ["xy", "zx", "yz"])
+def test_static_ic_counts_cells_in_the_config_order(tmp_path, config):
+    nx, ny, nz = 8, 6, 4
+    run(["-sim", "StaticIC", "-config", config, "-nx", str(nx), "-ny", str(ny), "-nz", str(nz),
+         "-fpath", str(tmp_path)])
+    dump = np.fromfile(tmp_path / "staticIC_0000.bin", dtype="<f4").reshape(nz, ny, nx, 9)
+    n = {"x": nx, "y": ny, "z": nz}
+    fast, mid = config
+    slow = ({"x", "y", "z"} - set(config)).pop()
+    cnt = 0
+    expect = np.empty((nz, ny, nx), np.float32)
+    ranges = {a: range(n[a]) for a in "xyz"}
+    for k in ranges[slow]:
+        for j in ranges[mid]:
+            for i in ranges[fast]:
+                idx = {fast: i, mid: j, slow: k}
+                expect[idx["z"], idx["y"], idx["x"]] = cnt
+                cnt += 1
+    assert np.array_equal(dump[..., 0], expect)      # rho holds the count
+    assert np.array_equal(dump[..., 5], expect)      # and so does G

@@ -74,3 +74,13 @@ def test_input_files(tmp_path):
     (tmp_path / "cloud.dat").write_text("0 0.1 0.2 0.3 0.05\n1 0.4 0.5 0.6 0.07\n\n")
     c = R.read_cloud(tmp_path / "cloud.dat")
     assert np.array_equal(c, [[0.1, 0.2, 0.3, 0.05], [0.4, 0.5, 0.6, 0.07]])
+
+
+def test_static_ic_takes_no_run_options():
+    s = R.Simulation(["-sim", "StaticIC", "-config", "zx", "-fname", "pattern"] + BASE)
+    assert (s.config, s.fname) == ("zx", "pattern")
+    for bad in ("xx", "xyz", "ab"):
+        with pytest.raises(R.ArgumentError):
+            R.Simulation(["-sim", "StaticIC", "-config", bad] + BASE)
+    with pytest.raises(R.ArgumentError):
+        R.Simulation(["-sim", "StaticIC"] + BASE)          # -config is mandatory
