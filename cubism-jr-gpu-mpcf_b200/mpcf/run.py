@@ -289,7 +289,12 @@ class Simulation:
         self.setup()
         while self.t < self.tend:
             dt_max = min(self.tend - self.t, self.tnextdump - self.t)
+            t0 = time.perf_counter()
             dt = self.solver.step(cfl=self.cfl, dt_max=dt_max)[0]
+            if self.verbosity:
+                # the reference times the sound speed and each stage under
+                # -verb (LSRK3_IntegratorMPI.cpp:35-59); here one call runs them
+                self.log("step time %.3f ms (sound speed, dt and three stages)" % ((time.perf_counter() - t0) * 1e3))
             self.t += dt
             self.step += 1
             err = self.solver.error_word()

@@ -25,7 +25,8 @@ def run(argv):
 
 def test_dumps_land_on_the_dump_times(tmp_path):
     t, step, log = run(SOD + ["-tend", "0.03", "-dumpinterval", "0.01", "-saveinterval", "1000",
-                              "-fpath", str(tmp_path)])
+                              "-fpath", str(tmp_path), "-verb", "1"])
+    assert log.count("step time") == step
     assert t == pytest.approx(0.03, rel=1e-12)
     # the IC, the three dump times (the last is tend) and the final dump
     names = sorted(p.name for p in tmp_path.glob("data_*.bin"))
