@@ -168,8 +168,12 @@ __device__ __forceinline__ void load_prim(const DomRegs& D, const typename Pol::
 template <class T>
 __device__ __forceinline__ bool physical(const T r, const T e, const T G, const T P)
 {
-    // also false for NaN
-    return (r > (T)0) && (e > (T)0) && (G > (T)0) && (P >= (T)0) && (e < (T)INFINITY) && (r < (T)INFINITY);
+    // also false for NaN.  P is only required to be finite: it is 0 in pure
+    // gas, and the update leaves round-off there (about -1e-17 in every
+    // precision on a bubble cloud).  A state without a real sound speed
+    // (p + pc <= 0) is flagged by the sound speed (ERRBIT_SOS).
+    return (r > (T)0) && (e > (T)0) && (G > (T)0) && (e < (T)INFINITY) && (r < (T)INFINITY) &&
+           (P < (T)INFINITY) && (P > -(T)INFINITY);
 }
 
 // ---------------------------------------------------------------------------

@@ -18,7 +18,7 @@ constexpr int kHaloPlanes = 3;
 
 // Bits of the device error word.
 enum {
-    ERRBIT_NONPHYSICAL = 1u << 0,   // rho <= 0, E <= 0, G <= 0, P < 0 or non-finite after an update
+    ERRBIT_NONPHYSICAL = 1u << 0,   // rho <= 0, E <= 0, G <= 0 or non-finite after an update
     ERRBIT_SOS_NONFINITE = 1u << 1, // max sound speed not finite or not positive
     ERRBIT_TMA_TIMEOUT = 1u << 2,   // a bulk tensor copy did not complete within the wait limit
     ERRBIT_BOUNDS = 1u << 3,        // bounds-checking build: an index left its buffer (clamped)

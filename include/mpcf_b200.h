@@ -54,7 +54,7 @@ typedef struct mpcf_solver mpcf_solver;
 #define MPCF_ERR_NUMERIC  -5   /* the device error word reports a non-physical state */
 
 /* bits of the device error word */
-#define MPCF_ERRBIT_NONPHYSICAL  1u  /* rho<=0, E<=0, G<=0, P<0 or non-finite after an update */
+#define MPCF_ERRBIT_NONPHYSICAL  1u  /* rho<=0, E<=0, G<=0 or non-finite after an update */
 #define MPCF_ERRBIT_SOS          2u  /* maximum speed of sound not finite or not positive */
 #define MPCF_ERRBIT_TMA_TIMEOUT  4u  /* a bulk tensor copy did not complete within the wait limit */
 #define MPCF_ERRBIT_BOUNDS       8u  /* bounds-checking build (libmpcf_b200_check.so): a stage-kernel index

@@ -352,6 +352,46 @@ def test_error_word_flags_nonphysical(mpcf):
         assert s.error_word() == 0
 
 
+@pytest.mark.parametrize("prec", ["fp32_ref", "fp32", "mixed", "fp64"])
+def test_pure_gas_round_off_is_not_flagged(mpcf, prec):
+    """A bubble deep enough to hold pure gas (P = 0 exactly, as at the
+    centre of the 512^3 cloud's larger bubbles) is a physical state after
+    an update, where P there may be left at round-off below zero: the error
+    word stays clear and p + pc stays positive everywhere."""
+    dims = (96, 96, 96)
+    params = mpcf.configs.ic_params(1000.0)
+    bub = np.array([[0.5, 0.5, 0.5, 0.35], [0.15, 0.2, 0.8, 0.1]])
+    with mpcf.Solver([dims], precision=prec) as s:
+        s.ic_cloud(params, bub)
+        assert np.count_nonzero(s.get_state(with_reg=False)[6] == 0) > 0     # pure gas
+        s.run(3, cfl=0.3, graph=True)
+        w = s.error_word()
+        r, ru, rv, rw, E, G, P = [np.asarray(a, np.float64) for a in s.get_state(with_reg=False)]
+    assert w == 0, (hex(w), int(np.count_nonzero(P < 0)), P.min())
+    p = (E - 0.5 * (ru * ru + rv * rv + rw * rw) / r - P) / G
+    assert (p + P / (1 + G)).min() > 0
+
+
+def test_error_word_flags_a_state_without_sound_speed(mpcf):
+    """One liquid cell with p = -2 pc has positive rho, E and G but no real
+    sound speed: the sound-speed bit is raised, without a fault."""
+    dims = (16, 8, 6)
+    n = dims[0] * dims[1] * dims[2]
+    g, pc = 6.59, 4096.0
+    G, P = 1.0 / (g - 1.0), g * pc / (g - 1.0)
+    U = [np.full(n, 1000.0, np.float32), np.zeros(n, np.float32), np.zeros(n, np.float32),
+         np.zeros(n, np.float32), np.full(n, G * 100.0 + P, np.float32), np.full(n, G, np.float32),
+         np.full(n, P, np.float32)]
+    U[4][77] = G * (-2.0 * pc) + P          # E > 0, p + pc = -pc
+    assert U[4][77] > 0
+    with mpcf.Solver([dims], precision="fp32_ref") as s:
+        s.set_state(U)
+        s.step(cfl=0.3)
+        w = s.error_word(clear=True)
+        assert w & mpcf._lib.ERRBIT_SOS, hex(w)
+        assert s.error_word() == 0
+
+
 @pytest.mark.parametrize("prec", ["fp32_ref", "mixed"])
 @pytest.mark.parametrize("tiling", [(3, 64, False, True), (7, 64, True, True), (7, 5, False, False),
                                     (8, 64, True, True), (8, 5, False, False)])
