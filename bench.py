@@ -320,6 +320,9 @@ def main():
     value = world * ncell * 3.0 * K / (ms * 1e-3)
     ms_step = ms / K
     sums1 = s.conserved_sums()
+    # the device error word after the warm-up and timed steps (0: every
+    # update stayed physical, every sound speed real and finite)
+    err_word = s.error_word()
     derived = {}
     if rank == 0:
         derived[args.precision] = derived_fields(all_state(s))
@@ -418,6 +421,7 @@ def main():
             # the sound speed comes fused from the previous step's last
             # stage (the stand-alone reduction ran in the first warm-up step)
             "gpu_launches": 5 * K,
+            "device_error_word": err_word,
             "clocks": clk,
             "e2e": e2e,
             "cpu_baseline": cpu,
