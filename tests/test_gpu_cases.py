@@ -102,3 +102,28 @@ def test_sod_tube_is_symmetric_across_axes(mpcf):
         res[cfg] = arr
     for q in range(7):
         assert np.array_equal(res["x"][q], res["y"][q]), q
+
+
+def test_long_runs_stay_physical(mpcf):
+    """300 steps of 2DSBI (Mach 1.22, reflecting walls) and 100 steps of the
+    steady state: no error bits; the steady state is invariant bit for bit,
+    and the mixed form stays within 1e-6 (L1 of rho) of the FP64 run."""
+    dims = (192, 96, 8)
+    bub = np.array([[0.4, 0.25, 0.02, 0.1], [0.7, 0.2, 0.02, 0.08]])
+    rho = {}
+    for prec in ("fp64", "mixed"):
+        with mpcf.Solver([dims], bc=[mpcf.case_bc("sbi", "xy")], precision=prec) as s:
+            s.ic_sbi(bub, config="xy", mollfactor=1)
+            s.run(300, cfl=0.3, graph=True)
+            assert s.error_word() == 0, prec
+            rho[prec] = np.asarray(s.get_state(with_reg=False)[0], np.float64)
+    l1 = np.abs(rho["mixed"] - rho["fp64"]).mean() / np.abs(rho["fp64"]).mean()
+    assert l1 < 1e-6, l1
+    for prec in ("fp32_ref", "mixed", "fp64"):
+        with mpcf.Solver([(48, 40, 32)], bc=[mpcf.case_bc("steady")], precision=prec) as s:
+            s.ic_steady(rho=2.0, p=3.0)
+            U0 = s.get_state(with_reg=False)
+            s.run(100, cfl=0.3, graph=True)
+            assert s.error_word() == 0, prec
+            for a, b in zip(U0, s.get_state(with_reg=False)):
+                assert np.array_equal(a, b), prec
