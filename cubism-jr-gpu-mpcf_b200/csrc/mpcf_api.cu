@@ -131,6 +131,8 @@ struct mpcf_solver
     cudaGraphExec_t graph[2] = {nullptr, nullptr};
     double graph_cfl = -1, graph_dtmax = -1;
     bool graph_cons = false;
+
+    unsigned test_flags = 0;        // MPCF_TEST_* (failure-detection tests only)
 };
 
 namespace {
@@ -320,6 +322,7 @@ StageArgs stage_args(mpcf_solver* s, double a, double b, bool sums)
     A.tile_sums = sums ? s->tile_sums : nullptr;
     A.tmaps = s->tmaps;
     A.sos_bits = nullptr;
+    A.test_flags = s->test_flags;
     return A;
 }
 
@@ -1375,6 +1378,16 @@ int mpcf_set_tiling(mpcf_solver* s, int ty, int dz, int flags)
     s->persist = (flags & MPCF_TILE_PERSISTENT) != 0;
     s->tma = (flags & MPCF_TILE_TMA) != 0;
     return apply_tiling(s);
+}
+
+int mpcf_set_test_flags(mpcf_solver* s, unsigned flags)
+{
+    if (!s) return fail(MPCF_ERR_ARG, "null solver");
+    if (flags & ~(unsigned)MPCF_TEST_DROP_LAST_COPY) return fail(MPCF_ERR_ARG, "unknown test flags 0x%x", flags);
+    static_assert((unsigned)MPCF_TEST_DROP_LAST_COPY == (unsigned)TEST_DROP_LAST_COPY, "test flag");
+    s->test_flags = flags;
+    destroy_graphs(s);   // captured launches carry the old flags
+    return MPCF_OK;
 }
 
 int mpcf_get_tiling(const mpcf_solver* s, int* ty, int* dz, int* flags)

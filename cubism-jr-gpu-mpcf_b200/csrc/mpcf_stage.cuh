@@ -207,10 +207,11 @@ __device__ __forceinline__ bool mbar_try_wait(uint32_t bar, uint32_t parity)
     return ok != 0;
 }
 
-// Bounded wait for the phase with parity `parity`; false after the limit.
+// Bounded wait for the phase with parity `parity`; false after the limit:
+// 2^18 polls, about 1.3 s on the B200 (a copy completes in microseconds).
 __device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity)
 {
-    for (int i = 0; i < (1 << 20); ++i)
+    for (int i = 0; i < (1 << 18); ++i)
         if (mbar_try_wait(bar, parity)) return true;
     return false;
 }
@@ -528,7 +529,10 @@ stage_kernel(const StageArgs A)
                 if (k + 1 <= z1)
                 {
                     mbar_expect_tx(barB, (uint32_t)L::kBBytes);
-                    tma_load_4d(smem_u32(stB), tm + 128, x0, y0, bc_map(k + 3, D.nz, D.bc4, D.bc5, fz), 0, barB);
+                    // the failure-detection test drops the chunk's last copy
+                    // (nothing is issued after it, so none is left in flight)
+                    if (PERSIST || !(A.test_flags & TEST_DROP_LAST_COPY) || k + 1 < z1)
+                        tma_load_4d(smem_u32(stB), tm + 128, x0, y0, bc_map(k + 3, D.nz, D.bc4, D.bc5, fz), 0, barB);
                 }
                 if (k + 1 < z1)
                 {

@@ -70,7 +70,14 @@ struct StageArgs
     double* tile_sums;  // [ntiles][5] FP64 partial conservation sums, or null
     const void* tmaps;  // per domain 4 CUtensorMap (128 B each): [buffer 0, 1] x [halo box, interior box]
     void* sos_bits;     // per domain maximum sound speed of the new state (bits), or null
+    unsigned test_flags; // TEST_* below; 0 outside the failure-detection tests
 };
+
+// Failure-detection tests: with TEST_DROP_LAST_COPY a non-persistent stage
+// kernel arms the mbarrier of the last bulk copy of each chunk but does not
+// issue the copy, so the CTA's final bounded wait runs out (ERRBIT_TMA_TIMEOUT)
+// with no copy in flight.  Persistent instances ignore the flag.
+enum { TEST_DROP_LAST_COPY = 1u };
 
 struct SosArgs
 {

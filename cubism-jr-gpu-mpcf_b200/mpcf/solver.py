@@ -257,6 +257,10 @@ class Solver:
         flags = (_lib.TILE_PERSISTENT if persistent else 0) | (_lib.TILE_TMA if tma else 0)
         check(lib().mpcf_set_tiling(self._h, int(ty), int(dz), flags))
 
+    def set_test_flags(self, flags):
+        """Failure-detection tests only (mpcf_set_test_flags)."""
+        check(lib().mpcf_set_test_flags(self._h, int(flags)))
+
     def tiling(self):
         """(ty, dz, persistent, tma) of the current launch configuration."""
         ty, dz, f = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()

@@ -345,6 +345,17 @@ int mpcf_set_tiling(mpcf_solver* s, int ty, int dz, int flags);
 int mpcf_get_tiling(const mpcf_solver* s, int* ty, int* dz, int* flags);
 int mpcf_autotune(mpcf_solver* s, int reps, int* best3, double* best_ms);
 
+/* Failure-detection tests only.  It replaces no reference interface: the
+ * reference ignores CUDA return codes (GPUhousehold.cu) and has no device
+ * failure detection.  MPCF_TEST_DROP_LAST_COPY makes a
+ * non-persistent stage launch with bulk-copy staging arm the mbarrier of the
+ * last copy of each z-chunk without issuing the copy: the CTA's final bounded
+ * wait runs out (2^18 polls, about 1.3 s), MPCF_ERRBIT_TMA_TIMEOUT is set, no copy is
+ * left in flight and the context stays usable.  Persistent launches ignore
+ * it.  0 (the default) turns it off. */
+#define MPCF_TEST_DROP_LAST_COPY 1u
+int mpcf_set_test_flags(mpcf_solver* s, unsigned flags);
+
 /* number of tiles one stage launch processes, and of stage-kernel CTAs */
 int mpcf_launch_shape(const mpcf_solver* s, long long* ntiles, long long* grid, int* threads);
 

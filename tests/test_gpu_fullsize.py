@@ -1,4 +1,4 @@
-"""Full-size GPU checks (BASELINE sizes) through size-independent properties;
+"""Full-size GPU checks (the benchmark configurations' sizes) through size-independent properties;
 the CPU oracle is too slow at these sizes, the small-size parity tests pin
 the arithmetic."""
 import numpy as np
