@@ -322,8 +322,7 @@ def test_gpu_and_cpu_sound_speed_formulas_agree():
 
 def test_flops_constant_matches_counter():
     exe = os.path.join(O.ORACLE_DIR, "count_ops")
-    if not os.path.exists(exe):
-        pytest.skip("oracle/count_ops not built")
+    assert os.path.exists(exe), "oracle/count_ops not built: run `make -C oracle`"
     out = subprocess.run([exe], capture_output=True, text=True, check=True).stdout.split()
     n = int(out[out.index("flops_per_cell_stage") + 1])
     import importlib.util
