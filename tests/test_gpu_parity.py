@@ -444,3 +444,19 @@ def test_fused_sound_speed_follows_state_changes(mpcf):
             O.step(dims, (ABS,) * 6, Uo, Ro, cfl=0.3)
         assert_bitwise(Ug, U1, f"graph={graph} vs fresh solver")
         assert_bitwise(Ug, Uo, f"graph={graph} vs oracle")
+
+
+def test_autotune_leaves_the_state_and_picks_shallow_chunks_on_small_domains(mpcf):
+    """The autotuner times its candidates on the solver's own state and
+    leaves it unchanged.  On a 64^3 domain, whose 16-deep chunks fill less
+    than one wave of resident CTAs, it also tries shallower chunks, and
+    one of those wins."""
+    dims = (64, 64, 64)
+    U0 = cloud_state(dims, nb=1)
+    with mpcf.Solver([dims], precision="mixed") as s:
+        s.set_state(U0)
+        best, ms = s.autotune(reps=2)
+        U, R = s.get_state()
+    assert_bitwise(U, [np.asarray(a, np.float32) for a in U0], "state after autotune")
+    assert best[1] < 16, best
+    assert ms > 0
