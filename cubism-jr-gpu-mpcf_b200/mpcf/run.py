@@ -192,6 +192,8 @@ class Simulation:
             self.nslices = a.int("nslices")
             self.dumpinterval = a.float("dumpinterval")
             self.saveinterval = a.int("saveinterval")
+            if not (self.cfl > 0 and self.dumpinterval > 0 and self.saveinterval >= 1):
+                raise ArgumentError("-cfl and -dumpinterval must be positive, -saveinterval at least 1")
         self.verbosity = a.int("verb", 0)
         self.restart = a.bool("restart")
         self.nsteps = a.int("nsteps", 0)

@@ -38,6 +38,14 @@ def test_mandatory_arguments(missing):
     R.Simulation(["-sim", "SodMPI", "-dryrun", "1"] + BASE)
 
 
+@pytest.mark.parametrize("flag,value", [("-saveinterval", "0"), ("-dumpinterval", "0"), ("-cfl", "-0.3")])
+def test_run_options_are_validated(flag, value):
+    argv = list(MANDATORY)
+    argv[argv.index(flag) + 1] = value
+    with pytest.raises(R.ArgumentError):
+        R.Simulation(["-sim", "SodMPI"] + BASE + argv)
+
+
 def test_cases_and_limits():
     with pytest.raises(R.ArgumentError):
         R.Simulation(["-sim", "NoSuchCase"] + BASE + MANDATORY)
