@@ -129,7 +129,8 @@ def measured_peaks():
 
 
 def make_solver(mpcf, cfg, precision):
-    s = mpcf.Solver(cfg["dims"], precision=precision)
+    # one GPU per rank: the rank's local GPU under torchrun (LOCAL_RANK), else 0
+    s = mpcf.Solver(cfg["dims"], precision=precision, device=env_rank()[2])
     for d, bub in enumerate(cfg["bubbles"]):
         s.ic_cloud(cfg["params"], bub, dom=d)
     return s
@@ -387,7 +388,7 @@ def main():
 
     if rank == 0:
         fp32_peak = ctypes.c_double()
-        mpcf._lib.check(mpcf.lib().mpcf_probe_fp32_peak(0, ctypes.byref(fp32_peak)))
+        mpcf._lib.check(mpcf.lib().mpcf_probe_fp32_peak(local, ctypes.byref(fp32_peak)))
         fp64 = others.get("fp64", {}).get("value")
         ach_tf = FLOPS_PER_CELL_STAGE * ncell / (st_ms * 1e-3) / 1e12
         line = {
