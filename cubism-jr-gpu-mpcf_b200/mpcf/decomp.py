@@ -177,8 +177,13 @@ class SlabRank:
     with the neighbours, then runs mpcf_stage; each step takes dt from the
     maximum sound speed over the ranks."""
 
-    def __init__(self, global_dims, bc=None, precision="fp32_ref", dist=None, device=0, group=None,
+    def __init__(self, global_dims, bc=None, precision="fp32_ref", dist=None, device=None, group=None,
                  rank=None, nranks=None):
+        if device is None:
+            # one GPU per rank: the device the rank made current (with
+            # torch.cuda.set_device(LOCAL_RANK)) before joining the group
+            import torch
+            device = torch.cuda.current_device()
         self.global_dims = tuple(int(v) for v in global_dims)
         self.dist = dist
         self.group = group
