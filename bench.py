@@ -184,30 +184,46 @@ def stage_kernel_ms(mpcf, s, reps=6):
     return s.time_stages(reps, dtinvh=0.0)
 
 
-def cpu_sample(cfg_params, bub, dims, threads, U0=None):
-    """Oracle (C restatement, OpenMP) on a sub-block of the workload: one
-    LSRK3 step, timed; returns (cell-stage updates/s, seconds).  U0 (the
-    sub-block's initial state) is generated when not given."""
-    import mpcf
+# The CPU sample of a workload: the middle CPU_SAMPLE_PLANES-plane z-slab of
+# its first domain (its whole first domain when that is thinner), with the
+# domain's cell spacing, bubbles and material data; one LSRK3 step of it per
+# timed step.
+CPU_SAMPLE_PLANES = int(os.environ.get("MPCF_CPU_SAMPLE_PLANES", "64"))
+
+
+def cpu_sample_block(cfg):
+    """(dims, origin, global dims) of the CPU sample of workload `cfg`."""
+    nx, ny, nz = cfg["dims"][0]
+    p = min(nz, CPU_SAMPLE_PLANES)
+    z0 = (nz - p) // 2
+    return (nx, ny, p), (0, 0, z0), (nx, ny, nz)
+
+
+def cpu_sample_name(cfg):
+    (nx, ny, p), (_, _, z0), _ = cpu_sample_block(cfg)
+    return f"one LSRK3 step of the {nx}x{ny}x{p} z-slab at planes {z0}-{z0 + p - 1} of the first domain"
+
+
+def cpu_sample_state(cfg):
+    """The sample's FP32 state from the oracle's restatement of the cloud
+    set-up (the product library is not loaded)."""
+    sys.path.insert(0, os.path.join(REPO, "tests"))
+    import oracle_lib as O
+    dims, org, glob = cpu_sample_block(cfg)
+    return O.ic_cloud(dims, cfg["params"], cfg["bubbles"][0], np.float32, origin=org, glob=glob)
+
+
+def cpu_step(dims, U0, threads):
+    """One oracle LSRK3 step of the sample (C restatement, OpenMP); returns
+    seconds."""
     sys.path.insert(0, os.path.join(REPO, "tests"))
     import oracle_lib as O
     os.environ["OMP_NUM_THREADS"] = str(threads)
-    if U0 is None:
-        U0 = mpcf.ic_cloud_host(dims, cfg_params, bub, np.float32)
     U = [a.copy() for a in U0]
     R = [np.zeros_like(a) for a in U]
     t0 = time.perf_counter()
     O.step(dims, (0,) * 6, U, R, cfl=0.3)
-    dt = time.perf_counter() - t0
-    n = dims[0] * dims[1] * dims[2]
-    return 3.0 * n / dt, dt
-
-
-def sample_dims(dims, target=4 << 20):
-    """A z-slab of `dims` with about `target` cells (the whole domain when it
-    is smaller): same cell spacing, bubbles and material data."""
-    nx, ny, nz = dims
-    return (nx, ny, max(1, min(nz, -(-target // (nx * ny)))))
+    return time.perf_counter() - t0
 
 
 def cpu_model():
@@ -222,30 +238,56 @@ def cpu_model():
     return None
 
 
+def loaded_libs():
+    """Shared objects of this repository mapped into this process."""
+    out = set()
+    try:
+        with open("/proc/self/maps") as f:
+            for line in f:
+                path = line.split()[-1] if line.strip() else ""
+                if path.endswith(".so") or ".so." in path:
+                    if os.path.realpath(path).startswith(os.path.realpath(REPO) + os.sep):
+                        out.add(os.path.relpath(os.path.realpath(path), os.path.realpath(REPO)))
+    except OSError:
+        pass
+    return sorted(out)
+
+
+def bench_config(cfg, world):
+    """The `config` object of both arms' lines (the workload, not the
+    implementation)."""
+    return {"workload": cfg["name"] + ": " + cfg["desc"] + ", absorbing, CFL 0.3",
+            "cells_per_gpu": sum(d[0] * d[1] * d[2] for d in cfg["dims"]),
+            "l2": "inputs larger than the 126 MB L2 (no flush needed)" if cfg["name"] != "c1_64"
+                  else "state 7.3 MB: L2-resident, no flush (latency-bound size)",
+            "parallelism": "replicas" if world > 1 else "single GPU",
+            "cpu_sample": cpu_sample_name(cfg)}
+
+
 def reference_arm(args):
+    """The reference algorithm's CPU implementation (the oracle: the C
+    restatement of the reference kernels, OpenMP over all host cores) on a
+    bounded sample of the workload; the product library is never loaded."""
     rank, world, _ = env_rank()
     if rank != 0:
         return 0
-    import mpcf
     sys.path.insert(0, os.path.join(REPO, "tests"))
     import oracle_lib as O
+    from mpcf import configs   # plain data and numpy: loads no library
     cores = os.cpu_count() or 1
     os.environ["OMP_NUM_THREADS"] = str(cores)
-    cfg = mpcf.configs.config(args.workload)
-    # bounded sample of the workload: a z-slab of its first domain, one full
-    # LSRK3 step per timed step
-    sub = sample_dims(cfg["dims"][0])
-    U0 = mpcf.ic_cloud_host(sub, cfg["params"], cfg["bubbles"][0], np.float32)
-    vals = []
+    cfg = configs.config(args.workload, placer=O.bubbles)
+    sub, _, _ = cpu_sample_block(cfg)
+    U0 = cpu_sample_state(cfg)
+    secs = []
     for i in range(args.warmup + args.steps):
-        v, dt = cpu_sample(cfg["params"], cfg["bubbles"][0], sub, cores, U0)
+        dt = cpu_step(sub, U0, cores)
         if i >= args.warmup:
-            vals.append(v)
-    value = statistics.median(vals)
+            secs.append(dt)
     n_sub = sub[0] * sub[1] * sub[2]
-    ncell = sum(d[0] * d[1] * d[2] for d in cfg["dims"])
-    sample = (f"C restatement of the reference kernels (oracle/), FP32 reference rounding, one LSRK3 step of "
-              f"a {sub[0]}x{sub[1]}x{sub[2]} slab of the workload")
+    value = 3.0 * n_sub * len(secs) / sum(secs)
+    sample = ("C restatement of the reference kernels (oracle/), FP32 reference rounding, OpenMP over "
+              f"{cores} threads, {cpu_sample_name(cfg)}")
     # the reference's own CPU sound speed (source/MaxSpeedOfSound.cpp, compiled
     # from its sources into oracle/_ref, serial as written) on the same sample
     sos = None
@@ -259,13 +301,14 @@ def reference_arm(args):
         sos = {"value": n_sub / sec, "unit": "cells/s", "cores": 1, "kind": "reference",
                "sample": f"MaxSpeedOfSound_CPP::compute over the {sub[0]}x{sub[1]}x{sub[2]} sample"}
     line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
-            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 3.0 * ncell / value * 1e3,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * sum(secs) / len(secs),
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
-            "data": "synthetic", "config": {"workload": args.workload, "sample": f"{sub[0]}x{sub[1]}x{sub[2]} slab, 1 LSRK3 step"},
+            "data": "synthetic", "config": bench_config(cfg, world),
             "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "port", "sample": sample,
                              "cpu_model": cpu_model()},
             "reference_sos_cpu": sos,
-            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+            "native_libs": loaded_libs()}
     print(json.dumps(line), flush=True)
     return 0
 
@@ -376,15 +419,16 @@ def main():
             e2e["with_register"] = e2e_measure(mpcf, cfg, K=ke, W=1, cfl=cfl, dist=dist,
                                                precision=args.precision, with_register=True)
 
-    # ---------------- CPU baseline (rank 0, N=1 only)
+    # ---------------- CPU baseline (rank 0, N=1 only): the oracle on the
+    # workload's CPU sample, its state from the oracle's cloud set-up
     cpu = None
     if not args.no_cpu and world == 1 and rank == 0:
         cores = os.cpu_count() or 1
-        sub = (512, 512, 16)
-        v, dtc = cpu_sample(cfg["params"], cfg["bubbles"][0], sub, cores)
-        cpu = {"value": v, "unit": UNIT, "cores": cores, "kind": "port",
-               "sample": "C restatement of the reference kernels (oracle/), OpenMP, one LSRK3 step of a "
-                         "512x512x16 slab of the workload (%.1f s)" % dtc, "cpu_model": cpu_model()}
+        sub, _, _ = cpu_sample_block(cfg)
+        dtc = cpu_step(sub, cpu_sample_state(cfg), cores)
+        cpu = {"value": 3.0 * sub[0] * sub[1] * sub[2] / dtc, "unit": UNIT, "cores": cores, "kind": "port",
+               "sample": "C restatement of the reference kernels (oracle/), FP32 reference rounding, OpenMP over "
+                         "%d threads, %s (%.1f s)" % (cores, cpu_sample_name(cfg), dtc), "cpu_model": cpu_model()}
 
     if rank == 0:
         fp32_peak = ctypes.c_double()
@@ -395,11 +439,9 @@ def main():
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": K, "warmup": W,
             "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": DTYPE_OF[args.precision], "data": "synthetic",
-            "config": {"workload": cfg["name"] + ": " + cfg["desc"] + ", absorbing, CFL 0.3, " + FORM_OF[args.precision],
-                       "cells_per_gpu": ncell, "l2": "inputs 11 GB > 126 MB L2 (no flush needed)",
-                       "parallelism": "replicas" if world > 1 else "single GPU",
-                       "tiling": {"ty": tiling[0], "dz": tiling[1], "persistent": tiling[2], "tma": tiling[3]},
-                       "graph": True},
+            "config": bench_config(cfg, world),
+            "form": FORM_OF[args.precision],
+            "tiling": {"ty": tiling[0], "dz": tiling[1], "persistent": tiling[2], "tma": tiling[3], "graph": True},
             "fp64_value": fp64, "mixed_over_fp64": (value / fp64) if fp64 else None,
             "other_precisions": others,
             "precision_error": err,

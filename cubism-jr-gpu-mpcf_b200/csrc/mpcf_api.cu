@@ -1383,10 +1383,23 @@ int mpcf_set_tiling(mpcf_solver* s, int ty, int dz, int flags)
 int mpcf_set_test_flags(mpcf_solver* s, unsigned flags)
 {
     if (!s) return fail(MPCF_ERR_ARG, "null solver");
-    if (flags & ~(unsigned)MPCF_TEST_DROP_LAST_COPY) return fail(MPCF_ERR_ARG, "unknown test flags 0x%x", flags);
+    if (flags & ~(unsigned)(MPCF_TEST_DROP_LAST_COPY | MPCF_TEST_DROP_MID_COPY))
+        return fail(MPCF_ERR_ARG, "unknown test flags 0x%x", flags);
     static_assert((unsigned)MPCF_TEST_DROP_LAST_COPY == (unsigned)TEST_DROP_LAST_COPY, "test flag");
+    static_assert((unsigned)MPCF_TEST_DROP_MID_COPY == (unsigned)TEST_DROP_MID_COPY, "test flag");
     s->test_flags = flags;
     destroy_graphs(s);   // captured launches carry the old flags
+    return MPCF_OK;
+}
+
+int mpcf_test_copy_count(mpcf_solver* s, unsigned* count, int clear)
+{
+    if (!s || !count) return fail(MPCF_ERR_ARG, "null argument");
+    DeviceGuard g(s->device);
+    CK(cudaMemcpyAsync(s->host_stage, s->counter + 1, sizeof(unsigned), cudaMemcpyDeviceToHost, s->stream));
+    if (clear) CK(cudaMemsetAsync(s->counter + 1, 0, sizeof(unsigned), s->stream));
+    CK(cudaStreamSynchronize(s->stream));
+    *count = *(unsigned*)s->host_stage;
     return MPCF_OK;
 }
 

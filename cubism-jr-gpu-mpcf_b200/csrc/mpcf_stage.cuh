@@ -310,7 +310,31 @@ stage_kernel(const StageArgs A)
     bool oob = false;                      // bounds-checking build: an index left its buffer
     uint32_t phA = 0, phB = 0;             // mbarrier phase parities
     __shared__ T sos_w[TileShape<TY>::kWarps];   // per-warp maxima of the fused sound speed
+    // A thread whose bounded wait runs out sets tma_late and waits for no
+    // further copy.  Thread 0 issues every copy; once it has given up it
+    // issues none, and before the CTA takes another tile or exits it waits
+    // (bounded again) for its copies that no wait of its own has seen
+    // complete: pendA/pendB, with the parity of that copy's phase.
     bool tma_late = false;
+    bool pendA = false, pendB = false;
+    uint32_t parA = 0, parB = 0;
+    bool tma_inflight = false;             // a drain wait ran out as well
+    // thread 0: one bulk copy into stage buffer `st` (barrier `bar`), with
+    // its phase recorded as pending (and counted in failure-detection tests)
+    auto issue = [&](const char* tmap, const bool isA, const int c0, const int c1, const int c2)
+    {
+        if (isA) { mbar_expect_tx(barA, (uint32_t)L::kABytes); tma_load_4d(smem_u32(stA), tmap, c0, c1, c2, 0, barA); pendA = true; parA = phA; }
+        else     { mbar_expect_tx(barB, (uint32_t)L::kBBytes); tma_load_4d(smem_u32(stB), tmap + 128, c0, c1, c2, 0, barB); pendB = true; parB = phB; }
+        if (A.test_flags) atomicAdd(A.counter + 1, 1u);
+    };
+    // bounded wait of this thread on `bar` for phase `ph`; thread 0 clears
+    // the copy's pending mark when it sees it complete
+    auto wait_copy = [&](const bool isA)
+    {
+        if (tma_late) return;
+        if (!mbar_wait(isA ? barA : barB, isA ? phA : phB)) { tma_late = true; return; }
+        if (threadIdx.x == 0) { if (isA) pendA = false; else pendB = false; }
+    };
 
     if (TMA)
     {
@@ -377,15 +401,13 @@ stage_kernel(const StageArgs A)
 #pragma unroll
             for (int m = 0; m < 7; ++m) sm[m * L::kPP + ri] = q[m];
         }
-        if (use_tma && threadIdx.x == 0)
+        if (use_tma && threadIdx.x == 0 && !tma_late)
         {
             // first copies: halo box of slab z0 and interior of slab z0+2
             bool fz;
             fence_proxy_async();
-            mbar_expect_tx(barA, (uint32_t)L::kABytes);
-            tma_load_4d(smem_u32(stA), tm, x0 - 4, y0 - 3, bc_map(z0, D.nz, D.bc4, D.bc5, fz), 0, barA);
-            mbar_expect_tx(barB, (uint32_t)L::kBBytes);
-            tma_load_4d(smem_u32(stB), tm + 128, x0, y0, bc_map(z0 + 2, D.nz, D.bc4, D.bc5, fz), 0, barB);
+            issue(tm, true, x0 - 4, y0 - 3, bc_map(z0, D.nz, D.bc4, D.bc5, fz));
+            issue(tm, false, x0, y0, bc_map(z0 + 2, D.nz, D.bc4, D.bc5, fz));
         }
 
         T Sp[7];                 // x/y part of the flux bracket of cell k-1
@@ -409,7 +431,7 @@ stage_kernel(const StageArgs A)
                 T q[7];
                 if (use_tma)
                 {
-                    if (!tma_late && !mbar_wait(barB, phB)) tma_late = true;
+                    wait_copy(false);
                     phB ^= 1;
                     bool fx = false, fy = false, fz;
                     int mx = tx, my = ty;
@@ -441,7 +463,7 @@ stage_kernel(const StageArgs A)
                 {
                     // tile reaching past the domain: convert the whole staged
                     // box, mapping out-of-domain cells to their sources
-                    if (!tma_late && !mbar_wait(barA, phA)) tma_late = true;
+                    wait_copy(true);
                     phA ^= 1;
                     for (int i = threadIdx.x; i < (TY + 6) * L::kCurW; i += stage_threads<TY>())
                     {
@@ -475,7 +497,7 @@ stage_kernel(const StageArgs A)
                     }
                     if (use_tma)
                     {
-                        if (!tma_late && !mbar_wait(barA, phA)) tma_late = true;
+                        wait_copy(true);
                         phA ^= 1;
                     }
                     for (int i = threadIdx.x; i < 6 * kTX + 6 * TY; i += stage_threads<TY>())
@@ -522,23 +544,22 @@ stage_kernel(const StageArgs A)
             __syncthreads();
             // the staging buffers are free again: copy the next slab's data
             // while this slab's faces are evaluated
-            if (use_tma && threadIdx.x == 0)
+            if (use_tma && threadIdx.x == 0 && !tma_late)
             {
                 bool fz;
                 fence_proxy_async();
                 if (k + 1 <= z1)
                 {
-                    mbar_expect_tx(barB, (uint32_t)L::kBBytes);
-                    // the failure-detection test drops the chunk's last copy
-                    // (nothing is issued after it, so none is left in flight)
-                    if (PERSIST || !(A.test_flags & TEST_DROP_LAST_COPY) || k + 1 < z1)
-                        tma_load_4d(smem_u32(stB), tm + 128, x0, y0, bc_map(k + 3, D.nz, D.bc4, D.bc5, fz), 0, barB);
+                    // the failure-detection tests arm the barrier of a copy
+                    // without issuing it: the chunk's last copy, or its
+                    // first copy after the prologue (then later waits find
+                    // the CTA given up, and no further copy is issued)
+                    const bool drop = !PERSIST && (((A.test_flags & TEST_DROP_LAST_COPY) && k + 1 == z1) ||
+                                                   ((A.test_flags & TEST_DROP_MID_COPY) && k == z0));
+                    if (drop) mbar_expect_tx(barB, (uint32_t)L::kBBytes);
+                    else      issue(tm, false, x0, y0, bc_map(k + 3, D.nz, D.bc4, D.bc5, fz));
                 }
-                if (k + 1 < z1)
-                {
-                    mbar_expect_tx(barA, (uint32_t)L::kABytes);
-                    tma_load_4d(smem_u32(stA), tm, x0 - 4, y0 - 3, bc_map(k + 1, D.nz, D.bc4, D.bc5, fz), 0, barA);
-                }
+                if (k + 1 < z1) issue(tm, true, x0 - 4, y0 - 3, bc_map(k + 1, D.nz, D.bc4, D.bc5, fz));
             }
 
             // R and U of cell k-1 are first prefetched into L1, so that its
@@ -832,15 +853,26 @@ stage_kernel(const StageArgs A)
             }
         }
 
+        // copies this CTA issued and no wait of thread 0 saw complete (only
+        // after a wait ran out): wait for them, bounded, so that none lands
+        // in shared memory the CTA no longer owns; a CTA that gave up takes
+        // no further tile
+        if (TMA && threadIdx.x == 0 && (pendA || pendB))
+        {
+            if (pendA && !mbar_wait(barA, parA)) tma_inflight = true;
+            if (pendB && !mbar_wait(barB, parB)) tma_inflight = true;
+            pendA = pendB = false;
+        }
         if (!PERSIST) break;
         __syncthreads();
-        if (threadIdx.x == 0) *tile_bc = (int)atomicAdd(A.counter, 1u);
+        if (threadIdx.x == 0) *tile_bc = tma_late ? A.ntiles : (int)atomicAdd(A.counter, 1u);
         __syncthreads();
         t = *tile_bc;
     }
 
     if (!__all_sync(0xffffffffu, ok) && tx == 0) atomicOr(A.err, (unsigned)ERRBIT_NONPHYSICAL);
     if (TMA && tma_late) atomicOr(A.err, (unsigned)ERRBIT_TMA_TIMEOUT);
+    if (TMA && tma_inflight) atomicOr(A.err, (unsigned)ERRBIT_TMA_INFLIGHT);
 #ifdef MPCF_CHECK_BOUNDS
     if (__any_sync(0xffffffffu, oob) && tx == 0) atomicOr(A.err, (unsigned)ERRBIT_BOUNDS);
 #endif

@@ -22,6 +22,7 @@ enum {
     ERRBIT_SOS_NONFINITE = 1u << 1, // max sound speed not finite or not positive
     ERRBIT_TMA_TIMEOUT = 1u << 2,   // a bulk tensor copy did not complete within the wait limit
     ERRBIT_BOUNDS = 1u << 3,        // bounds-checking build: an index left its buffer (clamped)
+    ERRBIT_TMA_INFLIGHT = 1u << 4,  // after a give-up, a CTA's bounded wait for its own copies ran out too
 };
 
 // One domain as the kernels see it.  All 7 fields of a buffer live in one
@@ -76,8 +77,12 @@ struct StageArgs
 // Failure-detection tests: with TEST_DROP_LAST_COPY a non-persistent stage
 // kernel arms the mbarrier of the last bulk copy of each chunk but does not
 // issue the copy, so the CTA's final bounded wait runs out (ERRBIT_TMA_TIMEOUT)
-// with no copy in flight.  Persistent instances ignore the flag.
-enum { TEST_DROP_LAST_COPY = 1u };
+// with no copy in flight.  TEST_DROP_MID_COPY drops the chunk's first copy
+// after the prologue instead: the wait runs out one slab in, the CTA issues
+// no further copy and waits for the one still pending before it exits.
+// Persistent instances ignore both.  With any flag set, counter[1] counts the
+// bulk copies issued.
+enum { TEST_DROP_LAST_COPY = 1u, TEST_DROP_MID_COPY = 2u };
 
 struct SosArgs
 {

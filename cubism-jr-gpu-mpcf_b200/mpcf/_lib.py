@@ -27,7 +27,9 @@ DUMP_SAVE = 1
 ERRBIT_NONPHYSICAL = 1
 ERRBIT_SOS = 2
 ERRBIT_TMA_TIMEOUT = 4
+ERRBIT_TMA_INFLIGHT = 16
 TEST_DROP_LAST_COPY = 1
+TEST_DROP_MID_COPY = 2
 TILE_PERSISTENT = 1
 TILE_TMA = 2
 
@@ -120,6 +122,7 @@ SIGNATURES = {
     "mpcf_get_time": (_I, [_P, _I, _PD]),
     "mpcf_set_tiling": (_I, [_P, _I, _I, _I]),
     "mpcf_set_test_flags": (_I, [_P, _c.c_uint]),
+    "mpcf_test_copy_count": (_I, [_P, _c.POINTER(_c.c_uint), _I]),
     "mpcf_get_tiling": (_I, [_P, _PI, _PI, _PI]),
     "mpcf_autotune": (_I, [_P, _I, _PI, _PD]),
     "mpcf_launch_shape": (_I, [_P, _c.POINTER(_c.c_longlong), _c.POINTER(_c.c_longlong), _PI]),

@@ -10,7 +10,7 @@ Synthetic inputs: no dataset is involved.
 import numpy as np
 
 from ._lib import IcParams
-from .solver import bubbles as _bubbles
+from .solver import bubbles as _place
 
 CFL = 0.3
 
@@ -26,8 +26,13 @@ def extents(dims):
     return tuple(d / m for d in dims)
 
 
-def config(name, seed=1234):
-    """Return dict(dims=[...], bubbles=[array], params=IcParams, steps, precision, ...)."""
+def config(name, seed=1234, placer=None):
+    """Return dict(dims=[...], bubbles=[array], params=IcParams, steps, precision, ...).
+
+    ``placer(seed, n, rmin, rmax, lo, hi)`` places the bubbles (default: the
+    library's seeded rejection sampling, ``mpcf_bubbles``); any placer with
+    the same rules gives the same workload."""
+    _bubbles = placer or _place
     if name == "c1_64":
         dims = [(64, 64, 64)]
         bub = [np.array([[0.5, 0.5, 0.5, 0.15]])]
@@ -72,4 +77,4 @@ def small_cloud(dims, nb=3, seed=7, p_liquid=100.0):
     edge = min(ext)
     lo = tuple(0.2 * e for e in ext)
     hi = tuple(0.8 * e for e in ext)
-    return ic_params(p_liquid, seed), _bubbles(seed, nb, 0.08 * edge, 0.2 * edge, lo, hi)
+    return ic_params(p_liquid, seed), _place(seed, nb, 0.08 * edge, 0.2 * edge, lo, hi)

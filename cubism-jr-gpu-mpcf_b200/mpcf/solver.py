@@ -52,6 +52,7 @@ class Solver:
         h = ctypes.c_void_p()
         check(lib().mpcf_create(ctypes.byref(h), self.ndom, flat, bcarr, precision, device))
         self._h = h
+        self.device = int(device)
 
     # -- lifetime ---------------------------------------------------------
     def close(self):
@@ -260,6 +261,13 @@ class Solver:
     def set_test_flags(self, flags):
         """Failure-detection tests only (mpcf_set_test_flags)."""
         check(lib().mpcf_set_test_flags(self._h, int(flags)))
+
+    def test_copy_count(self, clear=False):
+        """Failure-detection tests only: bulk copies issued while a test
+        flag was set (mpcf_test_copy_count)."""
+        c = ctypes.c_uint()
+        check(lib().mpcf_test_copy_count(self._h, ctypes.byref(c), 1 if clear else 0))
+        return c.value
 
     def tiling(self):
         """(ty, dz, persistent, tma) of the current launch configuration."""

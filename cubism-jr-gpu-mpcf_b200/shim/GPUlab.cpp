@@ -60,9 +60,40 @@ namespace mpcf_shim
     }
 }
 
+namespace
+{
+    // the halo marker: a quiet NaN with a payload no arithmetic produces
+    Real halo_marker()
+    {
+        Real v;
+        if (sizeof(Real) == 4) { const unsigned int b = 0x7fc0b200u; memcpy(&v, &b, sizeof(v)); }
+        else { const unsigned long long b = 0x7ff800000000b200ULL; memcpy(&v, &b, sizeof(v)); }
+        return v;
+    }
+}
+
+GPUlab::Halo::Halo(const uint_t sizeHalo)
+    : Nhalo(sizeHalo), store((size_t)2 * NVAR * sizeHalo, halo_marker()), left(NVAR, nullptr), right(NVAR, nullptr)
+{
+    for (uint_t q = 0; q < NVAR; ++q)
+    {
+        left[q] = &store[(size_t)q * Nhalo];
+        right[q] = &store[(size_t)(NVAR + q) * Nhalo];
+    }
+}
+
+bool GPUlab::Halo::untouched() const
+{
+    const Real m = halo_marker();
+    for (size_t i = 0; i < store.size(); ++i)
+        if (memcmp(&store[i], &m, sizeof(Real)) != 0) return false;
+    return true;
+}
+
 GPUlab::GPUlab(GridMPI& G, const uint_t nslices_, const int verbosity)
     : grid(G), halox(3 * sizeY * sizeZ), haloy(sizeX * 3 * sizeZ), haloz(sizeX * sizeY * 3),
-      nslices(nslices_), m_verbosity(verbosity), m_solver(nullptr), m_bc_dirty(false), m_host_sync(true)
+      nslices(nslices_), m_verbosity(verbosity), m_solver(nullptr), m_bc_dirty(false), m_host_sync(true),
+      m_ghost_calls(0), m_check_halos(getenv("MPCF_CHECK_HALOS") && atoi(getenv("MPCF_CHECK_HALOS")) != 0)
 {
     // the reference's configuration checks and messages (GPUlab.cpp:37-47)
     if (nslices_ == 0 || sizeZ % nslices_ != 0)
@@ -134,6 +165,18 @@ void GPUlab::load_ghosts(const double t)
     // one rank: every face is a physical boundary (SKIN), no halo messages
     // (GPUlab.cpp:622-644); the subclass states its boundary conditions
     _apply_bc(t);
+    // A halo written by hand would be ignored by the device ghosts: fail
+    // loudly, like the reference's configuration errors (GPUlab.cpp:37-47).
+    // The first call is checked always, later ones with MPCF_CHECK_HALOS=1.
+    if (m_ghost_calls++ == 0 || m_check_halos)
+    {
+        if (!halox.untouched() || !haloy.untouched() || !haloz.untouched())
+        {
+            fprintf(stderr, "[GPUlab ERROR: _apply_bc wrote the halo buffers directly; the B200 lab takes its ghosts "
+                            "only from BoundaryConditions::applyBC_absorbing / applyBC_reflecting]\n");
+            exit(1);
+        }
+    }
     if (m_bc_dirty)
     {
         GPU::check(mpcf_set_bc(m_solver, 0, m_bc), "GPUlab: boundary conditions");

@@ -64,13 +64,20 @@ protected:
     enum { SKIN, FLESH } myFeature[6];
     GridMPI& grid;
 
+    // The ghosts are synthesised on the device from the recorded boundary
+    // conditions, so the halo buffers are never read.  They still hold
+    // storage in the reference's layout (NVAR arrays of Nhalo per side),
+    // filled with a marker: a subclass whose _apply_bc writes them by hand
+    // (a condition BoundaryConditions cannot express) is detected by
+    // load_ghosts instead of being ignored.
     struct Halo
     {
         static const uint_t NVAR = GridMPI::NVAR;
         const uint_t Nhalo;
-        // no host storage: the ghosts are synthesised on the device
+        std::vector<Real> store;
         RealPtrVec_t left, right;
-        Halo(const uint_t sizeHalo) : Nhalo(sizeHalo), left(NVAR, nullptr), right(NVAR, nullptr) {}
+        Halo(const uint_t sizeHalo);
+        bool untouched() const;   // every value still the marker
     };
     Halo halox, haloy, haloz;
 
@@ -84,4 +91,6 @@ private:
     int m_bc[6];
     bool m_bc_dirty;
     bool m_host_sync;
+    long m_ghost_calls;     // load_ghosts calls so far
+    bool m_check_halos;     // check the halos after every _apply_bc, not only the first
 };

@@ -8,11 +8,6 @@ class Update_CUDA
 protected:
     Real m_b;
 
-    inline bool _is_aligned(const void* const ptr, unsigned int alignment) const
-    {
-        return ((size_t)ptr) % alignment == 0;
-    }
-
 public:
     Update_CUDA(const Real b = 1) : m_b(b) {}
 

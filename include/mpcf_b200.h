@@ -59,6 +59,8 @@ typedef struct mpcf_solver mpcf_solver;
 #define MPCF_ERRBIT_TMA_TIMEOUT  4u  /* a bulk tensor copy did not complete within the wait limit */
 #define MPCF_ERRBIT_BOUNDS       8u  /* bounds-checking build (libmpcf_b200_check.so): a stage-kernel index
                                         left its buffer; it was clamped into it and the results are void */
+#define MPCF_ERRBIT_TMA_INFLIGHT 16u /* after a bulk-copy wait ran out, a CTA's bounded wait for its own
+                                       copies still in flight ran out as well */
 
 /* stage-kernel tiling flags (mpcf_set_tiling / mpcf_get_tiling / mpcf_autotune) */
 #define MPCF_TILE_PERSISTENT 1  /* one CTA per resident slot pulling tiles from a work counter */
@@ -161,7 +163,9 @@ int mpcf_set_track_conservation(mpcf_solver* s, int on);
  * device array of this library, which every GPU that loads it keeps until
  * the process exits.  The first call on a device looks up that array's
  * device address, with the device current; make that first call before any
- * stream capture.  All calls share the array: calls that overlap on a GPU
+ * stream capture.  The address is kept for the life of the process, so a
+ * cudaDeviceReset of that device after the first call is not supported.
+ * All calls share the array: calls that overlap on a GPU
  * (concurrent streams or threads) race and must be serialised by the
  * caller.  Every partial a call reads is written by that same call. */
 int mpcf_conserved_sums_noalloc(const void* const* state7, long long ncells, int elem_size,
@@ -351,10 +355,19 @@ int mpcf_autotune(mpcf_solver* s, int reps, int* best3, double* best_ms);
  * non-persistent stage launch with bulk-copy staging arm the mbarrier of the
  * last copy of each z-chunk without issuing the copy: the CTA's final bounded
  * wait runs out (2^18 polls, about 1.3 s), MPCF_ERRBIT_TMA_TIMEOUT is set, no copy is
- * left in flight and the context stays usable.  Persistent launches ignore
- * it.  0 (the default) turns it off. */
+ * left in flight and the context stays usable.  MPCF_TEST_DROP_MID_COPY drops
+ * the chunk's first copy after the prologue instead: the wait runs out one
+ * slab in, the CTA issues no further copy, waits (bounded) for the copy it
+ * issued with the dropped one, and exits with none in flight (a drain wait
+ * that also ran out would set MPCF_ERRBIT_TMA_INFLIGHT).  Persistent launches
+ * ignore both.  0 (the default) turns them off. */
 #define MPCF_TEST_DROP_LAST_COPY 1u
+#define MPCF_TEST_DROP_MID_COPY  2u
 int mpcf_set_test_flags(mpcf_solver* s, unsigned flags);
+/* Failure-detection tests only: bulk copies the stage kernel issued while a
+ * test flag was set (clear != 0 resets the count).  No reference
+ * counterpart. */
+int mpcf_test_copy_count(mpcf_solver* s, unsigned* count, int clear);
 
 /* number of tiles one stage launch processes, and of stage-kernel CTAs */
 int mpcf_launch_shape(const mpcf_solver* s, long long* ntiles, long long* grid, int* threads);

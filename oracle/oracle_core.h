@@ -432,12 +432,13 @@ static int SFX(stage)(const int NX, const int NY, const int NZ, const int bc[6],
         SFX(fill_ghosts)(NX, NY, NZ, bc, U, gx, gy, gz);
 
         /* face fluxes in x, y, z (GPUkernels.cu:104-290, 483-669, 847-964) */
-        #pragma omp parallel for schedule(static)
+        /* (iz, iy) rows shared out together: balanced for thin slabs too */
+        #pragma omp parallel for collapse(2) schedule(static)
         for (int iz = 0; iz < NZ + 1; ++iz)
+        for (int iy = 0; iy < NY + 1; ++iy)
         {
             REAL s[7][6];
             REAL out[12];
-            for (int iy = 0; iy < NY + 1; ++iy)
             for (int ix = 0; ix < NX + 1; ++ix)
             {
                 int dir;
@@ -464,7 +465,7 @@ static int SFX(stage)(const int NX, const int NY, const int NZ, const int bc[6],
 
         /* extra terms (GPUkernels.cu:35-62 "=", :422-444 and :795-817 "+="),
          * divergence (:1092-1139) and update (:1142-1179) */
-        #pragma omp parallel for schedule(static)
+        #pragma omp parallel for collapse(2) schedule(static)
         for (int iz = 0; iz < NZ; ++iz)
         for (int iy = 0; iy < NY; ++iy)
         for (int ix = 0; ix < NX; ++ix)
@@ -533,8 +534,14 @@ static int SFX(stage)(const int NX, const int NY, const int NZ, const int bc[6],
 /* ---------------------------------------------------------------------- */
 static REAL SFX(max_sos)(const long long N, REAL* const* U)
 {
+    /* per-thread maxima, then their maximum: the maximum of a set does not
+     * depend on the order it is taken in */
     REAL sos = 0;
+    #pragma omp parallel
+    {
+    REAL loc = 0;
     long long i;
+    #pragma omp for schedule(static)
     for (i = 0; i < N; ++i)
     {
         const REAL r = U[0][i];
@@ -546,7 +553,10 @@ static REAL SFX(max_sos)(const long long N, REAL* const* U)
         const REAL P = U[6][i];
         const REAL p = (e - (u*u + v*v + w*w)*(0.5f/r) - P) / G;
         const REAL c = RSQRT(((p + P) / G + p) / r);
-        sos = RMAX(sos, c + RMAX(RMAX(RABS(u), RABS(v)), RABS(w)) / r);
+        loc = RMAX(loc, c + RMAX(RMAX(RABS(u), RABS(v)), RABS(w)) / r);
+    }
+    #pragma omp critical
+    sos = RMAX(sos, loc);
     }
     return sos;
 }

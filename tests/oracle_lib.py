@@ -66,6 +66,10 @@ def oracle():
         L.oracle_stencil_f32.argtypes = [_I, _I, _I, _PPF, _PF, _PF, _PF, _I, _I, _I, _I, _I, _PF]
         L.oracle_sic_cloud_f32.argtypes = [_I, _I, _I, _PD, _I, _PD, _D, _PPF, _PD]
         L.oracle_sic_cloud_f64.argtypes = [_I, _I, _I, _PD, _I, _PD, _D, _PPD, _PD]
+        L.oracle_bubbles.restype = _I
+        L.oracle_bubbles.argtypes = [_c.c_ulonglong, _I, _D, _D, _PD, _PD, _D, _I, _PD]
+        L.oracle_ic_cloud_f32.argtypes = [_I, _I, _I, _PI, _PI, _PD, _c.c_ulonglong, _I, _PD, _PPF]
+        L.oracle_ic_cloud_f64.argtypes = [_I, _I, _I, _PI, _PI, _PD, _c.c_ulonglong, _I, _PD, _PPD]
         _oracle = L
     return _oracle
 
@@ -405,3 +409,37 @@ def case_prm(case, opts, config=None):
         else:
             prm[k] = type(prm[k])(v)
     return prm
+
+
+def bubbles(seed, n, rmin, rmax, lo=(0.2, 0.2, 0.2), hi=(0.8, 0.8, 0.8), gap=0.0, max_tries=200000):
+    """Seeded non-overlapping spheres (x, y, z, r), shape (placed, 4): the
+    oracle's restatement of the workloads' bubble placement."""
+    out = np.zeros((max(n, 1), 4), np.float64)
+    lo3 = (_D * 3)(*lo)
+    hi3 = (_D * 3)(*hi)
+    k = oracle().oracle_bubbles(_c.c_ulonglong(seed), int(n), float(rmin), float(rmax), lo3, hi3,
+                                float(gap), int(max_tries), out.ctypes.data_as(_PD))
+    return out[:k]
+
+
+def cloud_prm(params):
+    """The cloud parameters (an object with the mpcf_ic_params fields) as
+    the oracle's array, and the noise seed."""
+    names = ("rho_l", "p_l", "gamma_l", "pc_l", "rho_g", "p_g", "gamma_g", "pc_g", "noise", "width")
+    return np.array([float(getattr(params, n)) for n in names], np.float64), int(params.seed)
+
+
+def ic_cloud(dims, params, bub, dtype=np.float32, origin=None, glob=None):
+    """Bubble-cloud state of an nx*ny*nz block (7 flat arrays); the block's
+    cell (0,0,0) is global cell `origin` of a `glob`-sized domain (default:
+    the block is the domain)."""
+    nx, ny, nz = dims
+    out = [np.empty(nx * ny * nz, dtype) for _ in range(7)]
+    prm, seed = cloud_prm(params)
+    b = np.ascontiguousarray(bub, dtype=np.float64).ravel()
+    o3 = (_I * 3)(*origin) if origin is not None else None
+    g3 = (_I * 3)(*glob) if glob is not None else None
+    f = oracle().oracle_ic_cloud_f64 if dtype == np.float64 else oracle().oracle_ic_cloud_f32
+    f(nx, ny, nz, o3, g3, prm.ctypes.data_as(_PD), _c.c_ulonglong(seed), b.size // 4,
+      b.ctypes.data_as(_PD) if b.size else None, fptrs(out))
+    return out
