@@ -40,16 +40,17 @@ sys.path.insert(0, os.path.join(REPO, "cubism-jr-gpu-mpcf_b200"))
 WORKLOAD = "c3_512"
 METRIC = "cell-stage updates/s on 1 B200: mixed vs plain FP64 at stated L1 error"
 UNIT = "cell-stage updates/s"
-BYTES_PER_CELL_STAGE = {"fp32_ref": 112, "fp32": 112, "mixed": 112, "fp64": 224}
+BYTES_PER_CELL_STAGE = {"fp32_ref": 112, "fp32": 112, "mixed": 112, "fp64": 224, "fp64_fast": 224}
 # DRAM bytes per cell-stage of the mixed stage kernel measured by ncu
 # (dram__bytes_read.sum + dram__bytes_write.sum = 8.98 + 7.48 GB for one
 # full-size launch over the 512^3 cloud, 134.2 M cells, 32 x 8 tiles over
 # whole columns, persistent, bulk-copy staging: a one-pass capture).  The
 # per-launch figure of the bench line is this times the workload's cells.
 # the arithmetic each precision form computes in, and its name in the workload
-DTYPE_OF = {"mixed": "f32+f64 (mixed)", "fp32": "f32", "fp32_ref": "f32 (reference rounding)", "fp64": "f64"}
+DTYPE_OF = {"mixed": "f32+f64 (mixed)", "fp32": "f32", "fp32_ref": "f32 (reference rounding)", "fp64": "f64",
+            "fp64_fast": "f64 (fast form)"}
 FORM_OF = {"mixed": "mixed form", "fp32": "fast FP32 form", "fp32_ref": "FP32 reference-rounding form",
-           "fp64": "FP64 form"}
+           "fp64": "FP64 form", "fp64_fast": "fast FP64 form (factored algebra, refined reciprocals)"}
 MEASURED_DRAM_BYTES_PER_CELL_STAGE = {"mixed": 16.39e9 / 512 ** 3}
 
 
@@ -323,7 +324,7 @@ def main():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-fp64", action="store_true")
     ap.add_argument("--only-mixed-fp64", action="store_true", help="skip the fp32_ref / fp32 throughput runs")
-    ap.add_argument("--precision", default="mixed", choices=["mixed", "fp32", "fp32_ref", "fp64"],
+    ap.add_argument("--precision", default="mixed", choices=["mixed", "fp32", "fp32_ref", "fp64", "fp64_fast"],
                     help="precision of the headline run (profiling of the other forms)")
     ap.add_argument("--workload", default=WORKLOAD)
     args = ap.parse_args()
@@ -381,7 +382,7 @@ def main():
 
     # ---------------- the other precisions on the same workload and steps
     others = {}
-    precs = [] if args.no_fp64 else ["fp64"]
+    precs = [] if args.no_fp64 else ["fp64", "fp64_fast"]
     if not args.no_fp64 and not args.only_mixed_fp64:
         precs += ["fp32_ref", "fp32", "mixed"]
     precs = [p for p in precs if p != args.precision]
@@ -398,7 +399,7 @@ def main():
     if rank == 0 and "fp64" in derived:
         r64, p64, G64 = derived["fp64"]
         err = {}
-        for prec in ("mixed", "fp32_ref", "fp32"):
+        for prec in ("mixed", "fp32_ref", "fp32", "fp64_fast"):
             if prec not in derived or prec == "fp64":
                 continue
             r, p, G = derived[prec]
@@ -434,6 +435,7 @@ def main():
         fp32_peak = ctypes.c_double()
         mpcf._lib.check(mpcf.lib().mpcf_probe_fp32_peak(local, ctypes.byref(fp32_peak)))
         fp64 = others.get("fp64", {}).get("value")
+        fp64f = others.get("fp64_fast", {}).get("value")
         ach_tf = FLOPS_PER_CELL_STAGE * ncell / (st_ms * 1e-3) / 1e12
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": K, "warmup": W,
@@ -443,6 +445,7 @@ def main():
             "form": FORM_OF[args.precision],
             "tiling": {"ty": tiling[0], "dz": tiling[1], "persistent": tiling[2], "tma": tiling[3], "graph": True},
             "fp64_value": fp64, "mixed_over_fp64": (value / fp64) if fp64 else None,
+            "fp64_fast_value": fp64f, "mixed_over_fp64_fast": (value / fp64f) if fp64f else None,
             "other_precisions": others,
             "precision_error": err,
             "conservation_drift": {"mass": float((sums1[:, 0].sum() - sums0[:, 0].sum()) / sums0[:, 0].sum()),
@@ -453,7 +456,8 @@ def main():
                          "traffic": (MEASURED_DRAM_BYTES_PER_CELL_STAGE[args.precision] * ncell
                                      if args.precision in MEASURED_DRAM_BYTES_PER_CELL_STAGE else None),
                          "traffic_note": "ncu DRAM bytes of one 512^3 launch (32x8 tiles, whole columns, persistent, TMA)",
-                         "kernel": "stage_kernel<Pol%s>" % {"mixed": "Mixed", "fp32": "Fast32", "fp32_ref": "Ref32", "fp64": "FP64"}[args.precision],
+                         "kernel": "stage_kernel<Pol%s>" % {"mixed": "Mixed", "fp32": "Fast32", "fp32_ref": "Ref32", "fp64": "FP64",
+                                                             "fp64_fast": "Fast64"}[args.precision],
                          "ms_per_launch": st_ms,
                          "algorithmic_bytes_per_launch": bytes_launch, "peak_kind": peak_kind,
                          "note": "the stage kernel is bound by the FP32 pipe, not HBM: see roofline_fp32"},
@@ -497,8 +501,8 @@ def e2e_measure(mpcf, cfg, K, W, cfl, dist, precision="mixed", with_register=Fal
     import torch
     s = make_solver(mpcf, cfg, precision)
     L = mpcf.lib()
-    dtype = torch.float64 if precision == "fp64" else torch.float32
-    esz = 8 if precision == "fp64" else 4
+    dtype = torch.float64 if precision in ("fp64", "fp64_fast") else torch.float32
+    esz = 8 if precision in ("fp64", "fp64_fast") else 4
     nbuf = 14 if with_register else 7
     bufs = []
     ncell = 0

@@ -157,6 +157,7 @@ StageKernelInfo stage_info(const mpcf_solver* s, int ty, bool persist, bool sums
         case 0: return stage_info_ref(ty, persist, sums, tma);
         case 1: return stage_info_fast32(ty, persist, sums, tma);
         case 2: return stage_info_mixed(ty, persist, sums, tma);
+        case 4: return stage_info_fast64(ty, persist, sums, tma);
         default: return stage_info_fp64(ty, persist, sums, tma);
     }
 }
@@ -168,6 +169,7 @@ cudaError_t launch_stage(const mpcf_solver* s, const StageArgs& A, int grid, cud
         case 0: return launch_stage_ref(s->ty, s->persist != 0, s->tma != 0, A, grid, st);
         case 1: return launch_stage_fast32(s->ty, s->persist != 0, s->tma != 0, A, grid, st);
         case 2: return launch_stage_mixed(s->ty, s->persist != 0, s->tma != 0, A, grid, st);
+        case 4: return launch_stage_fast64(s->ty, s->persist != 0, s->tma != 0, A, grid, st);
         default: return launch_stage_fp64(s->ty, s->persist != 0, s->tma != 0, A, grid, st);
     }
 }
@@ -436,8 +438,8 @@ int mpcf_version(void) { return MPCF_API_VERSION; }
 const char* mpcf_last_error(void) { return g_err.c_str(); }
 int mpcf_elem_size(int precision)
 {
-    if (precision < 0 || precision > 3) return fail(MPCF_ERR_ARG, "unknown precision %d", precision);
-    return precision == MPCF_PREC_FP64 ? 8 : 4;
+    if (precision < 0 || precision > MPCF_PREC_FP64_FAST) return fail(MPCF_ERR_ARG, "unknown precision %d", precision);
+    return (precision == MPCF_PREC_FP64 || precision == MPCF_PREC_FP64_FAST) ? 8 : 4;
 }
 
 int mpcf_create(mpcf_solver** out, int ndomains, const int* dims, const int* bc, int precision, int device)
@@ -446,7 +448,7 @@ int mpcf_create(mpcf_solver** out, int ndomains, const int* dims, const int* bc,
     *out = nullptr;
     if (ndomains < 1) return fail(MPCF_ERR_ARG, "ndomains must be >= 1 (got %d)", ndomains);
     if (!dims) return fail(MPCF_ERR_ARG, "null dims");
-    if (precision < 0 || precision > 3) return fail(MPCF_ERR_ARG, "unknown precision %d", precision);
+    if (precision < 0 || precision > MPCF_PREC_FP64_FAST) return fail(MPCF_ERR_ARG, "unknown precision %d", precision);
     for (int d = 0; d < ndomains; ++d)
     {
         const int nx = dims[3 * d], ny = dims[3 * d + 1], nz = dims[3 * d + 2];
@@ -471,7 +473,7 @@ int mpcf_create(mpcf_solver** out, int ndomains, const int* dims, const int* bc,
     s->device = device;
     s->pol = precision;
     s->ndom = ndomains;
-    s->esz = precision == MPCF_PREC_FP64 ? 8 : 4;
+    s->esz = (precision == MPCF_PREC_FP64 || precision == MPCF_PREC_FP64_FAST) ? 8 : 4;
     DeviceGuard g(device);
     int rc = MPCF_OK;
     auto bail = [&](int code) { mpcf_destroy(s); return code; };
@@ -976,11 +978,11 @@ int mpcf_sic_post_shock(const mpcf_sic_params* p, int precision, double* post4)
 {
     int rc = sic_check(p);
     if (rc) return rc;
-    if (!post4 || precision < 0 || precision > 3) return fail(MPCF_ERR_ARG, "bad arguments");
+    if (!post4 || precision < 0 || precision > MPCF_PREC_FP64_FAST) return fail(MPCF_ERR_ARG, "bad arguments");
     SicParams P;
     static_assert(sizeof(SicParams) == sizeof(mpcf_sic_params), "SIC parameter layout");
     memcpy(&P, p, sizeof(P));
-    sic_post_shock(precision == MPCF_PREC_FP64, P, post4);
+    sic_post_shock(precision == MPCF_PREC_FP64 || precision == MPCF_PREC_FP64_FAST, P, post4);
     return MPCF_OK;
 }
 

@@ -134,6 +134,7 @@ cudaError_t launch_sos(int pol, const SosArgs& A, cudaStream_t st)
         case 1: sos_kernel<PolFast32><<<A.nchunks, 256, 0, st>>>(A); break;
         case 2: sos_kernel<PolMixed><<<A.nchunks, 256, 0, st>>>(A); break;
         case 3: sos_kernel<PolFP64><<<A.nchunks, 256, 0, st>>>(A); break;
+        case 4: sos_kernel<PolFast64><<<A.nchunks, 256, 0, st>>>(A); break;
         default: return cudaErrorInvalidValue;
     }
     return cudaGetLastError();
@@ -150,6 +151,7 @@ cudaError_t launch_dt(int pol, const DtArgs& A, cudaStream_t st)
             case 1: dt_group_kernel<PolFast32><<<1, 256, 0, st>>>(A); break;
             case 2: dt_group_kernel<PolMixed><<<1, 256, 0, st>>>(A); break;
             case 3: dt_group_kernel<PolFP64><<<1, 256, 0, st>>>(A); break;
+            case 4: dt_group_kernel<PolFast64><<<1, 256, 0, st>>>(A); break;
             default: return cudaErrorInvalidValue;
         }
         return cudaGetLastError();
@@ -160,6 +162,7 @@ cudaError_t launch_dt(int pol, const DtArgs& A, cudaStream_t st)
         case 1: dt_kernel<PolFast32><<<g, 64, 0, st>>>(A); break;
         case 2: dt_kernel<PolMixed><<<g, 64, 0, st>>>(A); break;
         case 3: dt_kernel<PolFP64><<<g, 64, 0, st>>>(A); break;
+        case 4: dt_kernel<PolFast64><<<g, 64, 0, st>>>(A); break;
         default: return cudaErrorInvalidValue;
     }
     return cudaGetLastError();

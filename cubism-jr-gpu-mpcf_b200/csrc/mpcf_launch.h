@@ -17,15 +17,18 @@ struct StageKernelInfo
     size_t smem;        // dynamic shared memory per CTA
 };
 
-// precision policy ids: 0 FP32 reference rounding, 1 fast FP32, 2 mixed, 3 FP64
+// precision policy ids: 0 FP32 reference rounding, 1 fast FP32, 2 mixed, 3 FP64,
+// 4 fast FP64
 cudaError_t launch_stage_ref(int ty, bool persist, bool tma, const StageArgs& A, int grid, cudaStream_t st);
 cudaError_t launch_stage_fast32(int ty, bool persist, bool tma, const StageArgs& A, int grid, cudaStream_t st);
 cudaError_t launch_stage_mixed(int ty, bool persist, bool tma, const StageArgs& A, int grid, cudaStream_t st);
 cudaError_t launch_stage_fp64(int ty, bool persist, bool tma, const StageArgs& A, int grid, cudaStream_t st);
+cudaError_t launch_stage_fast64(int ty, bool persist, bool tma, const StageArgs& A, int grid, cudaStream_t st);
 StageKernelInfo stage_info_ref(int ty, bool persist, bool sums, bool tma);
 StageKernelInfo stage_info_fast32(int ty, bool persist, bool sums, bool tma);
 StageKernelInfo stage_info_mixed(int ty, bool persist, bool sums, bool tma);
 StageKernelInfo stage_info_fp64(int ty, bool persist, bool sums, bool tma);
+StageKernelInfo stage_info_fast64(int ty, bool persist, bool sums, bool tma);
 
 // mpcf_aux.cu
 cudaError_t launch_sos(int pol, const SosArgs& A, cudaStream_t st);

@@ -21,6 +21,9 @@
 //   PolMixed   PolFast32 plus the stiffened-gas pressure recovery in FP64
 //              and FP64 conservation sums.
 //   PolFP64    double storage and arithmetic (the all-FP64 GPU oracle run).
+//   PolFast64  double storage and arithmetic with the fast forms' algebra
+//              (factored indicators and fluxes, refined double reciprocals):
+//              the tuned FP64 yardstick of the mixed form.
 //
 // Primitive index convention used throughout the device code:
 //   0 rho, 1 u, 2 v, 3 w, 4 p, 5 G = 1/(gamma-1), 6 P = gamma*pc/(gamma-1)
@@ -41,6 +44,7 @@ struct PolRef32  { typedef float  T; static constexpr bool kFastWeno = false; st
 struct PolFast32 { typedef float  T; static constexpr bool kFastWeno = true;  static constexpr bool kP64 = false; static constexpr bool kRefRounding = false; static constexpr int id = 1; };
 struct PolMixed  { typedef float  T; static constexpr bool kFastWeno = true;  static constexpr bool kP64 = true;  static constexpr bool kRefRounding = false; static constexpr int id = 2; };
 struct PolFP64   { typedef double T; static constexpr bool kFastWeno = false; static constexpr bool kP64 = false; static constexpr bool kRefRounding = true;  static constexpr int id = 3; };
+struct PolFast64 { typedef double T; static constexpr bool kFastWeno = true;  static constexpr bool kP64 = false; static constexpr bool kRefRounding = false; static constexpr int id = 4; };
 
 __device__ __forceinline__ float  dmin(float a, float b)   { return fminf(a, b); }
 __device__ __forceinline__ float  dmax(float a, float b)   { return fmaxf(a, b); }
@@ -57,7 +61,20 @@ __device__ __forceinline__ float rcp_approx(float x)
     asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
     return r;
 }
-__device__ __forceinline__ double rcp_approx(double x) { return 1.0 / x; }
+// Reciprocal in double precision without a division: the special-function
+// unit's approximate reciprocal refined by two Newton-Raphson steps
+// y <- y + y (1 - x y) (each step doubles the number of correct bits).
+__device__ __forceinline__ double rcp_f64(const double x)
+{
+    double y;
+    asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(y) : "d"(x));
+    double e = fma(-x, y, 1.0);
+    y = fma(y, e, y);
+    e = fma(-x, y, 1.0);
+    return fma(y, e, y);
+}
+// the fast FP64 form's reciprocal
+__device__ __forceinline__ double rcp_approx(double x) { return rcp_f64(x); }
 
 // Approximate square root of the special-function unit (fast policies).
 __device__ __forceinline__ float sqrt_approx(float x)
@@ -156,6 +173,20 @@ __device__ __forceinline__ float2 fma2(const float2 a, const float2 b, const flo
 __device__ __forceinline__ float2 rcp2(const float2 a) { return make_float2(rcp_approx(a.x), rcp_approx(a.y)); }
 // HLLC upwind blend w.x * F.x + w.y * F.y of a (left, right) flux pair
 __device__ __forceinline__ float blend2(const float2 w, const float2 F) { const float2 t = mul2(F, w); return t.x + t.y; }
+// The same pair operations in double precision (the fast FP64 form), lane
+// by lane: there are no packed FP64 instructions.
+__device__ __forceinline__ double2 f2(const double a, const double b) { return make_double2(a, b); }
+__device__ __forceinline__ double2 f2s(const double a) { return make_double2(a, a); }
+__device__ __forceinline__ double2 add2(const double2 a, const double2 b) { return make_double2(a.x + b.x, a.y + b.y); }
+__device__ __forceinline__ double2 sub2(const double2 a, const double2 b) { return make_double2(a.x - b.x, a.y - b.y); }
+__device__ __forceinline__ double2 mul2(const double2 a, const double2 b) { return make_double2(a.x * b.x, a.y * b.y); }
+__device__ __forceinline__ double2 fma2(const double2 a, const double2 b, const double2 c) { return make_double2(fma(a.x, b.x, c.x), fma(a.y, b.y, c.y)); }
+__device__ __forceinline__ double2 rcp2(const double2 a) { return make_double2(rcp_f64(a.x), rcp_f64(a.y)); }
+__device__ __forceinline__ double blend2(const double2 w, const double2 F) { const double2 t = mul2(F, w); return t.x + t.y; }
+// the pair type of a value type
+template <class T> struct PairOf;
+template <> struct PairOf<float>  { typedef float2 V; };
+template <> struct PairOf<double> { typedef double2 V; };
 
 // Minimum / maximum of three values in one operation (sm_100).
 __device__ __forceinline__ float min3f(const float a, const float b, const float c)
@@ -170,6 +201,8 @@ __device__ __forceinline__ float max3f(const float a, const float b, const float
     asm("max.f32 %0, %1, %2, %3;" : "=f"(r) : "f"(a), "f"(b), "f"(c));
     return r;
 }
+__device__ __forceinline__ double min3f(const double a, const double b, const double c) { return fmin(fmin(a, b), c); }
+__device__ __forceinline__ double max3f(const double a, const double b, const double c) { return fmax(fmax(a, b), c); }
 
 // Both edge values of one cell (fast policies), from the cell and its two
 // neighbours on either side, y0..y4 = cells l-2..l+2:
@@ -186,27 +219,30 @@ __device__ __forceinline__ float max3f(const float a, const float b, const float
 //   L = (y2+y1)/2 - k1/6 - (g2 (k1-k2)/3 + g0 (k0-k1)/2) / (3 g0 + 6 g1 + g2)
 // and both are clipped to [min, max] of y1, y2, y3.  Lane x of every pair
 // is the right edge, lane y the left edge.
-__device__ __forceinline__ void weno_cell_packed(const float y0, const float y1, const float y2,
-                                                 const float y3, const float y4, float& R, float& L)
+// The same algebra serves the fast FP64 form (T = double, lane by lane).
+template <class T>
+__device__ __forceinline__ void weno_cell_packed(const T y0, const T y1, const T y2,
+                                                 const T y3, const T y4, T& R, T& L)
 {
-    constexpr float e4 = (float)(4.0 * MPCF_WENOEPS);
-    const float2 Y04 = f2(y0, y4), Y13 = f2(y1, y3), Y22 = f2s(y2);
-    const float2 K02 = fma2(Y13, f2s(-2.f), add2(Y04, Y22));                    // (k0, k2)
-    const float  k1  = fmaf(y2, -2.f, y1 + y3);
-    const float2 A02 = fma2(Y22, f2s(3.f), fma2(Y13, f2s(-4.f), Y04));          // (a0, a2)
-    const float  a1  = y1 - y3;
-    const float2 J02 = fma2(mul2(K02, f2s(13.f / 3.f)), K02, fma2(A02, A02, f2s(e4)));
-    const float  j1  = fmaf(k1 * (13.f / 3.f), k1, fmaf(a1, a1, e4));
-    const float2 G02 = rcp2(mul2(J02, J02));                                    // (g0, g2)
-    const float  g1  = rcp_approx(j1 * j1);
-    const float2 den = fma2(f2(G02.y, G02.x), f2s(3.f), fma2(f2s(g1), f2s(6.f), G02));
-    const float2 E   = mul2(G02, f2(K02.x - k1, k1 - K02.y));                   // (g0 D0, g2 D2)
-    const float2 num = fma2(E, f2(1.f / 3.f, -1.f / 3.f), mul2(f2(E.y, E.x), f2(0.5f, -0.5f)));
-    const float2 p1  = fma2(f2s(k1), f2s(-1.f / 6.f), mul2(add2(Y22, f2(y3, y1)), f2s(0.5f)));
-    const float2 r   = fma2(num, rcp2(den), p1);
-    const float lo = min3f(y1, y2, y3), hi = max3f(y1, y2, y3);
-    R = fminf(fmaxf(r.x, lo), hi);
-    L = fminf(fmaxf(r.y, lo), hi);
+    typedef typename PairOf<T>::V V;
+    constexpr T e4 = (T)(4.0 * MPCF_WENOEPS);
+    const V Y04 = f2(y0, y4), Y13 = f2(y1, y3), Y22 = f2s(y2);
+    const V K02 = fma2(Y13, f2s((T)-2), add2(Y04, Y22));                        // (k0, k2)
+    const T k1  = fma(y2, (T)-2, y1 + y3);
+    const V A02 = fma2(Y22, f2s((T)3), fma2(Y13, f2s((T)-4), Y04));             // (a0, a2)
+    const T a1  = y1 - y3;
+    const V J02 = fma2(mul2(K02, f2s((T)13 / (T)3)), K02, fma2(A02, A02, f2s(e4)));
+    const T j1  = fma(k1 * ((T)13 / (T)3), k1, fma(a1, a1, e4));
+    const V G02 = rcp2(mul2(J02, J02));                                         // (g0, g2)
+    const T g1  = rcp_approx(j1 * j1);
+    const V den = fma2(f2(G02.y, G02.x), f2s((T)3), fma2(f2s(g1), f2s((T)6), G02));
+    const V E   = mul2(G02, f2(K02.x - k1, k1 - K02.y));                        // (g0 D0, g2 D2)
+    const V num = fma2(E, f2((T)1 / (T)3, -(T)1 / (T)3), mul2(f2(E.y, E.x), f2((T)0.5, (T)-0.5)));
+    const V p1  = fma2(f2s(k1), f2s(-(T)1 / (T)6), mul2(add2(Y22, f2(y3, y1)), f2s((T)0.5)));
+    const V r   = fma2(num, rcp2(den), p1);
+    const T lo = min3f(y1, y2, y3), hi = max3f(y1, y2, y3);
+    R = dmin(dmax(r.x, lo), hi);
+    L = dmin(dmax(r.y, lo), hi);
 }
 
 // ---------------------------------------------------------------------------
@@ -342,65 +378,67 @@ __device__ __forceinline__ void hllc_face(const FaceState<typename Pol::T>& S, c
 // factored: the advected quantities share V = S (chi - 1) + u, and the
 // energy flux cancels the (s - u) of chi against the p/(s - u) of the
 // reference's star-state energy.
-__device__ __forceinline__ void hllc_face_packed(const FaceState<float>& S, const int dir, FaceOut<float>& o)
+template <class T>
+__device__ __forceinline__ void hllc_face_packed(const FaceState<T>& S, const int dir, FaceOut<T>& o)
 {
-    const float2 Rh = f2(S.rm, S.rp), Uh = f2(S.nm, S.np), Ph = f2(S.pm, S.pp);
-    const float2 Gh = f2(S.Gm, S.Gp), Qh = f2(S.Pm, S.Pp);
-    const float2 T1 = f2(S.t1m, S.t1p), T2 = f2(S.t2m, S.t2p);
-    const float um = S.nm, up = S.np;
+    typedef typename PairOf<T>::V V;
+    const V Rh = f2(S.rm, S.rp), Uh = f2(S.nm, S.np), Ph = f2(S.pm, S.pp);
+    const V Gh = f2(S.Gm, S.Gp), Qh = f2(S.Pm, S.Pp);
+    const V T1 = f2(S.t1m, S.t1p), T2 = f2(S.t2m, S.t2p);
+    const T um = S.nm, up = S.np;
 
     // Einfeldt bounds
-    const float2 ir = rcp2(Rh);
-    const float Rr   = sqrtf(S.rp * ir.x);
-    const float Rinv = rcp_approx(1.0f + Rr);
-    const float2 c2 = mul2(fma2(add2(Ph, Qh), rcp2(Gh), Ph), ir);
-    const float cm = sqrtf(c2.x), cp = sqrtf(c2.y);
-    const float eta_2 = 0.5f * Rr * Rinv * Rinv;
-    const float du = up - um;
-    const float d  = sqrtf((c2.x + Rr * c2.y) * Rinv + eta_2 * du * du);
-    const float uu = (um + Rr * up) * Rinv;
-    const float sm = fminf(uu - d, um - cm);
-    const float sp = fmaxf(uu + d, up + cp);
+    const V ir = rcp2(Rh);
+    const T Rr   = dsqrt(S.rp * ir.x);
+    const T Rinv = rcp_approx((T)1 + Rr);
+    const V c2 = mul2(fma2(add2(Ph, Qh), rcp2(Gh), Ph), ir);
+    const T cm = dsqrt(c2.x), cp = dsqrt(c2.y);
+    const T eta_2 = (T)0.5 * Rr * Rinv * Rinv;
+    const T du = up - um;
+    const T d  = dsqrt((c2.x + Rr * c2.y) * Rinv + eta_2 * du * du);
+    const T uu = (um + Rr * up) * Rinv;
+    const T sm = dmin(uu - d, um - cm);
+    const T sp = dmax(uu + d, up + cp);
 
     // Batten star speed
-    const float2 SU  = sub2(f2(sm, sp), Uh);                  // (sm - um, sp - up)
-    const float2 fac = mul2(Rh, SU);
-    const float ss = (S.pp - S.pm + um * fac.x - up * fac.y) * rcp_approx(fac.x - fac.y);
+    const V SU  = sub2(f2(sm, sp), Uh);                       // (sm - um, sp - up)
+    const V fac = mul2(Rh, SU);
+    const T ss = (S.pp - S.pm + um * fac.x - up * fac.y) * rcp_approx(fac.x - fac.y);
     const int s = sign_star_of(ss);
-    const float2 Sg  = f2(fminf(0.0f, sm), fmaxf(0.0f, sp));
-    const float2 SS  = f2s(ss);
-    const float2 Dinv = rcp2(sub2(f2(sm, sp), SS));           // 1/(s - s*)
-    const float2 D   = sub2(SS, Uh);                          // s* - u
-    const float2 C1  = mul2(D, Dinv);                         // chi - 1 = (s* - u)/(s - s*)
-    const float2 Wb  = f2(0.5f * (float)(1 + s), 0.5f * (float)(1 - s));
+    const V Sg  = f2(dmin((T)0, sm), dmax((T)0, sp));
+    const V SS  = f2s(ss);
+    const V Dinv = rcp2(sub2(f2(sm, sp), SS));                // 1/(s - s*)
+    const V D   = sub2(SS, Uh);                               // s* - u
+    const V C1  = mul2(D, Dinv);                              // chi - 1 = (s* - u)/(s - s*)
+    const V Wb  = f2((T)0.5 * (T)(1 + s), (T)0.5 * (T)(1 - s));
 
     // every advected quantity X has the star-state flux S (X chi - X) + X u
     // = X V with V = S (chi - 1) + u, the extra-term velocity's argument too
-    const float2 A = mul2(Sg, C1);
-    const float2 V = add2(A, Uh);
+    const V A = mul2(Sg, C1);
+    const V V_ = add2(A, Uh);
     // rho, G, P (passive)
-    o.f[0] = blend2(Wb, mul2(Rh, V));
-    o.f[5] = blend2(Wb, mul2(Gh, V));
-    o.f[6] = blend2(Wb, mul2(Qh, V));
+    o.f[0] = blend2(Wb, mul2(Rh, V_));
+    o.f[5] = blend2(Wb, mul2(Gh, V_));
+    o.f[6] = blend2(Wb, mul2(Qh, V_));
     // normal momentum: S (rho s* chi - rho u) + rho u^2 + p
     // = rho (S (s* chi - u) + u^2) + p
-    const float2 U2 = mul2(Uh, Uh);
+    const V U2 = mul2(Uh, Uh);
     // (s* chi - u = s* (chi - 1) + s* - u)
-    const float fn = blend2(Wb, fma2(Rh, fma2(Sg, fma2(SS, C1, D), U2), Ph));
+    const T fn = blend2(Wb, fma2(Rh, fma2(Sg, fma2(SS, C1, D), U2), Ph));
     // transverse momenta
-    const float2 RV = mul2(Rh, V);
-    const float ft1 = blend2(Wb, mul2(T1, RV));
-    const float ft2 = blend2(Wb, mul2(T2, RV));
+    const V RV = mul2(Rh, V_);
+    const T ft1 = blend2(Wb, mul2(T1, RV));
+    const T ft2 = blend2(Wb, mul2(T2, RV));
     // energy: S (chi (Q + (s* - u)(rho s* + p/(s - u))) - Q) + u (Q + p)
     // = Q V + S (s* - u)(rho s* (s - u) + p)/(s - s*) + u p, Q = E
     {
-        const float2 ke = fma2(T2, T2, fma2(T1, T1, U2));
-        const float2 Q  = fma2(mul2(f2s(0.5f), Rh), ke, fma2(Gh, Ph, Qh));
-        const float2 inner = fma2(mul2(Rh, SS), SU, Ph);
-        o.f[4] = blend2(Wb, fma2(Q, V, fma2(A, inner, mul2(Uh, Ph))));
+        const V ke = fma2(T2, T2, fma2(T1, T1, U2));
+        const V Q  = fma2(mul2(f2s((T)0.5), Rh), ke, fma2(Gh, Ph, Qh));
+        const V inner = fma2(mul2(Rh, SS), SU, Ph);
+        o.f[4] = blend2(Wb, fma2(Q, V_, fma2(A, inner, mul2(Uh, Ph))));
     }
     // extra-term velocity
-    o.vel = blend2(Wb, V);
+    o.vel = blend2(Wb, V_);
 
     o.f[1] = dir == 0 ? fn : ft1;
     o.f[2] = dir == 1 ? fn : (dir == 0 ? ft1 : ft2);
@@ -414,7 +452,7 @@ __device__ __forceinline__ void weno_cell(const typename Pol::T y0, const typena
         const typename Pol::T y2, const typename Pol::T y3, const typename Pol::T y4,
         typename Pol::T& R, typename Pol::T& L)
 {
-    if constexpr (Pol::kFastWeno) weno_cell_packed(y0, y1, y2, y3, y4, R, L);
+    if constexpr (Pol::kFastWeno) weno_cell_packed<typename Pol::T>(y0, y1, y2, y3, y4, R, L);
     else                          weno_cell_ref<Pol>(y0, y1, y2, y3, y4, R, L);
 }
 
@@ -422,21 +460,8 @@ __device__ __forceinline__ void weno_cell(const typename Pol::T y0, const typena
 template <class Pol>
 __device__ __forceinline__ void face_hllc(const FaceState<typename Pol::T>& S, const int dir, FaceOut<typename Pol::T>& o)
 {
-    if constexpr (Pol::kFastWeno) hllc_face_packed(S, dir, o);
+    if constexpr (Pol::kFastWeno) hllc_face_packed<typename Pol::T>(S, dir, o);
     else                          hllc_face<Pol>(S, dir, o);
-}
-
-// Reciprocal in double precision without a division: the special-function
-// unit's approximate reciprocal refined by two Newton-Raphson steps
-// y <- y + y (1 - x y) (each step doubles the number of correct bits).
-__device__ __forceinline__ double rcp_f64(const double x)
-{
-    double y;
-    asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(y) : "d"(x));
-    double e = fma(-x, y, 1.0);
-    y = fma(y, e, y);
-    e = fma(-x, y, 1.0);
-    return fma(y, e, y);
 }
 
 // Conserved (rho, rho u, rho v, rho w, E, G, P) -> primitives (rho, u, v, w,
@@ -453,7 +478,7 @@ __device__ __forceinline__ void to_primitive(const typename Pol::T c[7], typenam
     q[0] = c[0];
     if constexpr (Pol::kFastWeno)
     {
-        const float ir = rcp_approx(c[0]);
+        const T ir = rcp_approx(c[0]);
         q[1] = c[1] * ir;
         q[2] = c[2] * ir;
         q[3] = c[3] * ir;
@@ -464,7 +489,7 @@ __device__ __forceinline__ void to_primitive(const typename Pol::T c[7], typenam
             q[4] = (T)(((double)c[4] - ke - (double)c[6]) * rcp_f64((double)c[5]));
         }
         else
-            q[4] = (c[4] - 0.5f*c[0]*(q[1]*q[1] + q[2]*q[2] + q[3]*q[3]) - c[6]) * rcp_approx(c[5]);
+            q[4] = (c[4] - (T)0.5*c[0]*(q[1]*q[1] + q[2]*q[2] + q[3]*q[3]) - c[6]) * rcp_approx(c[5]);
     }
     else
     {

@@ -15,7 +15,9 @@ PREC_FP32_REF = 0
 PREC_FP32 = 1
 PREC_MIXED = 2
 PREC_FP64 = 3
-PRECISIONS = {"fp32_ref": PREC_FP32_REF, "fp32": PREC_FP32, "mixed": PREC_MIXED, "fp64": PREC_FP64}
+PREC_FP64_FAST = 4
+PRECISIONS = {"fp32_ref": PREC_FP32_REF, "fp32": PREC_FP32, "mixed": PREC_MIXED, "fp64": PREC_FP64,
+              "fp64_fast": PREC_FP64_FAST}
 
 BC_ABSORBING = 0
 BC_REFLECTING = 1

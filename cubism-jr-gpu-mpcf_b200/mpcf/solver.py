@@ -23,7 +23,7 @@ def _ptr_array(arrays):
 
 
 def dtype_of(precision):
-    return np.float64 if precision == _lib.PREC_FP64 else np.float32
+    return np.float64 if precision in (_lib.PREC_FP64, _lib.PREC_FP64_FAST) else np.float32
 
 
 class Solver:

@@ -14,7 +14,7 @@
  *   G = 1/(gamma-1), P = gamma*pc/(gamma-1)) of nx*ny*nz elements, cell
  *   (ix,iy,iz) at ix + nx*(iy + ny*iz).  Element type: float for the
  *   MPCF_PREC_FP32_REF, MPCF_PREC_FP32 and MPCF_PREC_MIXED precisions,
- *   double for MPCF_PREC_FP64.
+ *   double for MPCF_PREC_FP64 and MPCF_PREC_FP64_FAST.
  * Boundary conditions, per domain, 6 ints in the order
  *   x-left, x-right, y-left, y-right, z-left, z-right
  *   (MPCF_BC_ABSORBING / MPCF_BC_REFLECTING, BoundaryConditions.h:60-109;
@@ -38,7 +38,8 @@ typedef struct mpcf_solver mpcf_solver;
 #define MPCF_PREC_FP32_REF 0  /* FP32, rounding of the reference source (bit-exact to the CPU restatement) */
 #define MPCF_PREC_FP32     1  /* FP32, fast weights / division, fused multiply-add */
 #define MPCF_PREC_MIXED    2  /* fast FP32 + FP64 pressure recovery + FP64 conservation sums */
-#define MPCF_PREC_FP64     3  /* all FP64 */
+#define MPCF_PREC_FP64     3  /* all FP64, rounding order of the reference source */
+#define MPCF_PREC_FP64_FAST 4 /* all FP64 with the fast forms' factored algebra and refined reciprocals */
 
 /* boundary conditions */
 #define MPCF_BC_ABSORBING  0

@@ -1,6 +1,8 @@
-"""Full-size GPU checks (the benchmark configurations' sizes) through size-independent properties;
-the CPU oracle is too slow at these sizes, the small-size parity tests pin
-the arithmetic."""
+"""Full-size GPU checks (the benchmark configurations' sizes) through
+size-independent properties: invariance of a uniform state, axis
+permutations, conservation between reflecting walls, graph replay against
+plain steps, ensembles against separate solvers.  Parity against the CPU
+oracle at these sizes and tilings is in test_gpu_parity_bench.py."""
 import numpy as np
 import pytest
 
@@ -17,7 +19,7 @@ def uniform(dims, vel=(0.0, 0.0, 0.0), dtype=np.float32):
     return [np.full(n, v, dtype) for v in (rho, rho * vel[0], rho * vel[1], rho * vel[2], E, G, P)]
 
 
-@pytest.mark.parametrize("prec", ["fp32_ref", "mixed", "fp64"])
+@pytest.mark.parametrize("prec", ["fp32_ref", "mixed", "fp64", "fp64_fast"])
 def test_uniform_state_invariant_256cube(mpcf, prec):
     dims = (256, 256, 256)
     dt = mpcf.dtype_of(mpcf.PRECISIONS[prec])

@@ -220,13 +220,16 @@ def test_fast_forms_every_tiling_tracks_fp64_oracle(mpcf, prec, dims):
             assert_bitwise(Rg, first[1], f"register, tiling {tiling} vs {FAST_TILINGS[0]}")
 
 
-def test_fp64_matches_fp64_oracle(mpcf):
+@pytest.mark.parametrize("prec", ["fp64", "fp64_fast"])
+def test_fp64_matches_fp64_oracle(mpcf, prec):
+    """Both FP64 forms: the reference-rounding one and the fast one (the fast
+    forms' factored algebra in double, refined reciprocals)."""
     dims = (30, 22, 14)
     bc = (ABS, REF, ABS, ABS, REF, ABS)
     U0 = cloud_state(dims, nb=2, dtype=np.float64)
     U = [np.array(a) for a in U0]
     R = [np.zeros_like(a) for a in U]
-    with mpcf.Solver([dims], bc=[bc], precision="fp64") as s:
+    with mpcf.Solver([dims], bc=[bc], precision=prec) as s:
         s.set_state(U, R)
         dt = s.step(cfl=0.3)[0]
         Ug, Rg = s.get_state()
@@ -352,7 +355,7 @@ def test_error_word_flags_nonphysical(mpcf):
         assert s.error_word() == 0
 
 
-@pytest.mark.parametrize("prec", ["fp32_ref", "fp32", "mixed", "fp64"])
+@pytest.mark.parametrize("prec", ["fp32_ref", "fp32", "mixed", "fp64", "fp64_fast"])
 def test_pure_gas_round_off_is_not_flagged(mpcf, prec):
     """A bubble deep enough to hold pure gas (P = 0 exactly, as at the
     centre of the 512^3 cloud's larger bubbles) is a physical state after
