@@ -327,6 +327,7 @@ def main():
     ap.add_argument("--precision", default="mixed", choices=["mixed", "fp32", "fp32_ref", "fp64", "fp64_fast"],
                     help="precision of the headline run (profiling of the other forms)")
     ap.add_argument("--workload", default=WORKLOAD)
+    ap.add_argument("--e2e-chunks", type=int, default=16, help="z-chunks of the streamed e2e run")
     args = ap.parse_args()
     if args.impl == "reference":
         return reference_arm(args)
@@ -412,13 +413,8 @@ def main():
     # ---------------- e2e through the C ABI with host buffers
     e2e = None
     if not args.no_e2e:
-        ke = max(2, min(K, 4))
-        e2e = e2e_measure(mpcf, cfg, K=ke, W=1, cfl=cfl, dist=dist, precision=args.precision)
-        if world == 1:
-            # informational: the register moved too (7.5 GB more pinned host
-            # memory, so not on every rank of a multi-GPU run)
-            e2e["with_register"] = e2e_measure(mpcf, cfg, K=ke, W=1, cfl=cfl, dist=dist,
-                                               precision=args.precision, with_register=True)
+        e2e = e2e_measure(mpcf, cfg, K=K, W=W, cfl=cfl, dist=dist, precision=args.precision, tiling=tiling,
+                          nchunks=args.e2e_chunks)
 
     # ---------------- CPU baseline (rank 0, N=1 only): the oracle on the
     # workload's CPU sample, its state from the oracle's cloud set-up
@@ -491,60 +487,75 @@ def pick_tiling(mpcf, s):
     return best
 
 
-def e2e_measure(mpcf, cfg, K, W, cfl, dist, precision="mixed", with_register=False):
-    """Same metric through the C ABI with pinned host buffers: every step
-    uploads the state of every domain, advances one LSRK3 step and downloads
-    the new state.  The register is dead between steps (stage 1 multiplies
-    it by a = 0), so the state is the step's whole input and result; with
-    `with_register` it is moved both ways as well, as the reference's
-    per-stage streaming does."""
+def e2e_measure(mpcf, cfg, K, W, cfl, dist, precision="mixed", tiling=None, nchunks=16):
+    """Same metric through the C ABI with the state in page-locked host
+    memory, as the reference keeps it: every step reads its input state from
+    the host buffers and writes its result back to them (mpcf_run_host: z-chunk
+    uploads, stage 3 chunk by chunk with each chunk downloaded as soon as it
+    is written, the next step's upload of a chunk after its download, copies
+    in both directions overlapping the kernels).  The register stays on the
+    device (stage 1 multiplies it by a = 0), so the state is the step's whole
+    input and result.  Host wall clock over the K timed steps.  Also the
+    serial form: mpcf_set_state + mpcf_step + mpcf_get_state per step."""
     import torch
     s = make_solver(mpcf, cfg, precision)
     L = mpcf.lib()
+    if tiling is not None:
+        ty, _, persist, tma = tiling
+        nz = cfg["dims"][0][2]
+        s.set_tiling(ty, max(1, nz // nchunks), persist, tma)
     dtype = torch.float64 if precision in ("fp64", "fp64_fast") else torch.float32
     esz = 8 if precision in ("fp64", "fp64_fast") else 4
-    nbuf = 14 if with_register else 7
+    ncell = sum(d[0] * d[1] * d[2] for d in cfg["dims"])
+    streamed = len(cfg["dims"]) == 1
     bufs = []
-    ncell = 0
     for d, dims in enumerate(cfg["dims"]):
         n = dims[0] * dims[1] * dims[2]
-        ncell += n
-        h = [torch.empty(n, dtype=dtype, pin_memory=True) for _ in range(nbuf)]
-        st = s.get_state(dom=d)
+        h = [torch.empty(n, dtype=dtype, pin_memory=True) for _ in range(7)]
+        st = s.get_state(dom=d, with_reg=False)
         for q in range(7):
-            h[q].numpy()[:] = st[0][q]
-            if with_register:
-                h[7 + q].numpy()[:] = st[1][q]
+            h[q].numpy()[:] = st[q]
         del st
-        up = (ctypes.c_void_p * 7)(*[h[q].data_ptr() for q in range(7)])
-        ur = (ctypes.c_void_p * 7)(*[h[7 + q].data_ptr() for q in range(7)]) if with_register else None
-        bufs.append((h, up, ur))
-
-    def one():
-        for d, (_, up, ur) in enumerate(bufs):
-            mpcf._lib.check(L.mpcf_set_state(s._h, d, up, ur, 0))
-        mpcf._lib.check(L.mpcf_step(s._h, cfl, 1e30, None))
-        for d, (_, up, ur) in enumerate(bufs):
-            mpcf._lib.check(L.mpcf_get_state(s._h, d, up, ur, 0))
-
-    for _ in range(W):
-        one()
-    if dist is not None:
-        dist.barrier()
-    torch.cuda.synchronize()
-    t0 = time.perf_counter()
-    for _ in range(K):
-        one()
-    torch.cuda.synchronize()
-    sec = time.perf_counter() - t0
+        bufs.append((h, (ctypes.c_void_p * 7)(*[h[q].data_ptr() for q in range(7)])))
     import mpcf.replicas as rp
-    value, _ = rp.throughput(dist, ncell, 3.0 * K, sec * 1e3, device="cuda" if dist is not None else None)
+
+    def timed(fn, k):
+        if dist is not None:
+            dist.barrier()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        fn(k)
+        torch.cuda.synchronize()
+        return time.perf_counter() - t0
+
+    out = {"unit": UNIT, "h2d_bytes_per_step": 7 * esz * ncell, "d2h_bytes_per_step": 7 * esz * ncell}
+    if streamed:
+        host = [b.numpy() for b in bufs[0][0]]
+        s.run_host(host, W, cfl=cfl, nchunks=nchunks)
+        sec = timed(lambda k: s.run_host(host, k, cfl=cfl, nchunks=nchunks), K)
+        out["value"], _ = rp.throughput(dist, ncell, 3.0 * K, sec * 1e3, device="cuda" if dist is not None else None)
+        out["path"] = (f"mpcf_run_host: state in pinned host memory read and written every step, {nchunks} z-chunks, "
+                       f"tiling {list(s.tiling())}, host wall clock over {K} steps")
+
+    def serial(k):
+        for _ in range(k):
+            for d, (_, up) in enumerate(bufs):
+                mpcf._lib.check(L.mpcf_set_state(s._h, d, up, None, 0))
+            mpcf._lib.check(L.mpcf_step(s._h, cfl, 1e30, None))
+            for d, (_, up) in enumerate(bufs):
+                mpcf._lib.check(L.mpcf_get_state(s._h, d, up, None, 0))
+
+    ks = max(2, min(K, 4))
+    serial(1)
+    sec = timed(serial, ks)
+    v, _ = rp.throughput(dist, ncell, 3.0 * ks, sec * 1e3, device="cuda" if dist is not None else None)
+    ser = {"value": v, "unit": UNIT, "path": f"mpcf_set_state + mpcf_step + mpcf_get_state per step, {ks} steps"}
+    if streamed:
+        out["serial"] = ser
+    else:
+        out.update(ser)
     s.close()
-    what = "state and register" if with_register else "state (the register stays on the device)"
-    return {"value": value, "unit": UNIT, "h2d_bytes_per_step": nbuf * esz * ncell,
-            "d2h_bytes_per_step": nbuf * esz * ncell,
-            "path": f"mpcf_set_state + mpcf_step + mpcf_get_state per step on pinned host buffers, {what}, "
-                    "host wall clock"}
+    return out
 
 
 if __name__ == "__main__":

@@ -133,6 +133,12 @@ struct mpcf_solver
     bool graph_cons = false;
 
     unsigned test_flags = 0;        // MPCF_TEST_* (failure-detection tests only)
+
+    // runs over host-resident state (mpcf_run_host): two copy streams and
+    // per-chunk events, made on first use
+    cudaStream_t up = nullptr, down = nullptr;
+    std::vector<cudaEvent_t> ev_up, ev_st, ev_down;
+    cudaEvent_t ev_start = nullptr;
 };
 
 namespace {
@@ -314,6 +320,7 @@ StageArgs stage_args(mpcf_solver* s, double a, double b, bool sums)
     A.doms = s->ddoms;
     A.ndom = s->ndom;
     A.ntiles = s->ntiles;
+    A.tile0 = 0;
     A.dz = s->dz;
     A.parity = s->parity;
     A.a = a;
@@ -328,6 +335,26 @@ StageArgs stage_args(mpcf_solver* s, double a, double b, bool sums)
     return A;
 }
 
+// Enqueue the stage of tiles [tile_lo, tile_hi) on the solver's stream
+// (device dt/h); the parity is left as it is (the caller flips it once the
+// whole stage is enqueued).
+int enqueue_stage_tiles(mpcf_solver* s, double a, double b, bool sums, bool sos, int tile_lo, int tile_hi)
+{
+    StageArgs A = stage_args(s, a, b, sums);
+    if (sos) A.sos_bits = s->sos_bits;
+    A.tile0 = tile_lo;
+    A.ntiles = tile_hi;
+    int grid = tile_hi - tile_lo;
+    if (s->persist)
+    {
+        grid = std::min(grid, persistent_grid(s, s->ty));
+        CK(cudaMemsetAsync(s->counter, 0, sizeof(unsigned), s->stream));
+    }
+    cudaError_t e = launch_stage(s, A, grid, s->stream);
+    if (e != cudaSuccess) return fail(MPCF_ERR_CUDA, "stage launch failed: %s", cudaGetErrorString(e));
+    return MPCF_OK;
+}
+
 // Enqueue one stage on the solver's stream (device dt/h) and flip parity.
 int enqueue_stage(mpcf_solver* s, double a, double b, bool sums, bool sos = false)
 {
@@ -335,16 +362,8 @@ int enqueue_stage(mpcf_solver* s, double a, double b, bool sums, bool sos = fals
     // this stage reads
     if (!s->links.empty())
         CK(launch_halo((int)s->esz, s->ddoms, s->dlinks, (int)s->links.size() / 2, s->link_plane, s->parity, s->stream));
-    StageArgs A = stage_args(s, a, b, sums);
-    if (sos) A.sos_bits = s->sos_bits;
-    int grid = s->ntiles;
-    if (s->persist)
-    {
-        grid = persistent_grid(s, s->ty);
-        CK(cudaMemsetAsync(s->counter, 0, sizeof(unsigned), s->stream));
-    }
-    cudaError_t e = launch_stage(s, A, grid, s->stream);
-    if (e != cudaSuccess) return fail(MPCF_ERR_CUDA, "stage launch failed: %s", cudaGetErrorString(e));
+    int rc = enqueue_stage_tiles(s, a, b, sums, sos, 0, s->ntiles);
+    if (rc) return rc;
     s->parity ^= 1;
     if (sums)
     {
@@ -363,6 +382,7 @@ int enqueue_sos(mpcf_solver* s)
     A.ndom = s->ndom;
     A.nchunks = s->nchunks;
     A.chunk = s->sos_chunk;
+    A.chunk0 = 0;
     A.parity = s->parity;
     A.sos_bits = s->sos_bits;
     CK(launch_sos(s->pol, A, s->stream));
@@ -555,6 +575,11 @@ int mpcf_destroy(mpcf_solver* s)
     if (!s) return MPCF_OK;
     DeviceGuard g(s->device);
     if (s->stream) cudaStreamSynchronize(s->stream);
+    for (cudaStream_t c : {s->up, s->down})
+        if (c) { cudaStreamSynchronize(c); cudaStreamDestroy(c); }
+    for (auto* v : {&s->ev_up, &s->ev_st, &s->ev_down})
+        for (cudaEvent_t e : *v) cudaEventDestroy(e);
+    if (s->ev_start) cudaEventDestroy(s->ev_start);
     destroy_graphs(s);
     for (void* p : s->allocs) cudaFree(p);
     if (s->host_stage) cudaFreeHost(s->host_stage);
@@ -732,6 +757,119 @@ int mpcf_run(mpcf_solver* s, int nsteps, double cfl, double dt_max, int use_grap
         }
     }
     if (time_out) CK(cudaMemcpyAsync(time_out, s->time, sizeof(double) * s->ndom, cudaMemcpyDeviceToHost, s->stream));
+    CK(cudaStreamSynchronize(s->stream));
+    return MPCF_OK;
+}
+
+int mpcf_run_host(mpcf_solver* s, int nsteps, double cfl, double dt_max, void* const* host7, int nchunks,
+                  double* time_out)
+{
+    Range nvtx("mpcf_run_host");
+    if (!s) return fail(MPCF_ERR_ARG, "null solver");
+    if (nsteps < 0 || nchunks < 1) return fail(MPCF_ERR_ARG, "nsteps < 0 or nchunks < 1");
+    if (!(cfl > 0) || !(dt_max > 0)) return fail(MPCF_ERR_ARG, "cfl and dt_max must be positive");
+    if (!host7) return fail(MPCF_ERR_ARG, "null host state");
+    for (int q = 0; q < 7; ++q) if (!host7[q]) return fail(MPCF_ERR_ARG, "host field %d is null", q);
+    if (s->ndom != 1) return fail(MPCF_ERR_ARG, "mpcf_run_host streams one domain (the solver has %d)", s->ndom);
+    if (!s->links.empty() || s->hdoms[0].zlo || s->hdoms[0].zhi)
+        return fail(MPCF_ERR_ARG, "mpcf_run_host: slabs with halo faces are not streamed");
+    DeviceGuard g(s->device);
+    const DomDev& D = s->hdoms[0];
+    const long long plane = (long long)D.nx * D.ny;
+    const size_t esz = s->esz;
+    // chunks of whole tile layers (tiles never straddle two chunks); the
+    // tiles of layers l0..l1-1 are the contiguous range l0*txy .. l1*txy-1
+    const int layers = D.tiles_z, txy = D.tiles_x * D.tiles_y;
+    const int nch = std::min(nchunks, layers);
+    std::vector<int> lc(nch + 1), zc(nch + 1);
+    for (int c = 0; c <= nch; ++c)
+    {
+        lc[c] = (int)((long long)layers * c / nch);
+        zc[c] = std::min(D.nz, lc[c] * s->dz);
+    }
+    // streams and events, made once
+    if (!s->up)
+    {
+        CK(cudaStreamCreateWithFlags(&s->up, cudaStreamNonBlocking));
+        CK(cudaStreamCreateWithFlags(&s->down, cudaStreamNonBlocking));
+        CK(cudaEventCreateWithFlags(&s->ev_start, cudaEventDisableTiming));
+    }
+    for (auto* v : {&s->ev_up, &s->ev_st, &s->ev_down})
+        while ((int)v->size() < nch)
+        {
+            cudaEvent_t e;
+            CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+            v->push_back(e);
+        }
+    // the first upload overwrites the state only after the work already
+    // queued on the solver's stream
+    CK(cudaEventRecord(s->ev_start, s->stream));
+    CK(cudaStreamWaitEvent(s->up, s->ev_start, 0));
+    int rc;
+    for (int n = 0; n < nsteps; ++n)
+    {
+        // (1) the step's input: chunk c of the host state into the state
+        // buffer, once the previous step's result of chunk c is on the host
+        char* dev = (char*)D.U[s->parity];
+        for (int c = 0; c < nch; ++c)
+        {
+            if (n > 0) CK(cudaStreamWaitEvent(s->up, s->ev_down[c], 0));
+            const size_t off = (size_t)zc[c] * plane * esz, bytes = (size_t)(zc[c + 1] - zc[c]) * plane * esz;
+            for (int q = 0; q < 7; ++q)
+                CK(cudaMemcpyAsync(dev + (size_t)q * D.fs * esz + off, (const char*)host7[q] + off, bytes,
+                                   cudaMemcpyHostToDevice, s->up));
+            CK(cudaEventRecord(s->ev_up[c], s->up));
+        }
+        // (2) its maximum sound speed, chunk by chunk as the chunks land
+        CK(cudaMemsetAsync(s->sos_bits, 0, esz, s->stream));
+        int done = 0;
+        for (int c = 0; c < nch; ++c)
+        {
+            CK(cudaStreamWaitEvent(s->stream, s->ev_up[c], 0));
+            const int upto = c == nch - 1 ? s->nchunks : (int)((long long)zc[c + 1] * plane / s->sos_chunk);
+            if (upto <= done) continue;
+            SosArgs A;
+            A.doms = s->ddoms;
+            A.ndom = 1;
+            A.nchunks = upto - done;
+            A.chunk = s->sos_chunk;
+            A.chunk0 = done;
+            A.parity = s->parity;
+            A.sos_bits = s->sos_bits;
+            CK(launch_sos(s->pol, A, s->stream));
+            done = upto;
+        }
+        // (3) dt, stages 1 and 2 over the whole domain
+        if ((rc = enqueue_dt(s, cfl, dt_max))) return rc;
+        for (int k = 0; k < 2; ++k)
+            if ((rc = enqueue_stage(s, kLSRK3[k][0], kLSRK3[k][1], false))) return rc;
+        // (4) stage 3 chunk by chunk; each chunk of the new state goes to the
+        // host as soon as it is written
+        for (int c = 0; c < nch; ++c)
+        {
+            if ((rc = enqueue_stage_tiles(s, kLSRK3[2][0], kLSRK3[2][1], false, false, lc[c] * txy, lc[c + 1] * txy)))
+                return rc;
+            CK(cudaEventRecord(s->ev_st[c], s->stream));
+        }
+        s->parity ^= 1;
+        const char* res = (const char*)D.U[s->parity];
+        for (int c = 0; c < nch; ++c)
+        {
+            CK(cudaStreamWaitEvent(s->down, s->ev_st[c], 0));
+            const size_t off = (size_t)zc[c] * plane * esz, bytes = (size_t)(zc[c + 1] - zc[c]) * plane * esz;
+            for (int q = 0; q < 7; ++q)
+                CK(cudaMemcpyAsync((char*)host7[q] + off, res + (size_t)q * D.fs * esz + off, bytes,
+                                   cudaMemcpyDeviceToHost, s->down));
+            CK(cudaEventRecord(s->ev_down[c], s->down));
+        }
+    }
+    // the device state equals the host result; the sound-speed accumulator
+    // was cleared by the last dt and holds nothing
+    s->sos_fresh = false;
+    s->sums_valid = false;
+    CK(cudaStreamSynchronize(s->down));
+    CK(cudaStreamSynchronize(s->up));
+    if (time_out) CK(cudaMemcpyAsync(time_out, s->time, sizeof(double), cudaMemcpyDeviceToHost, s->stream));
     CK(cudaStreamSynchronize(s->stream));
     return MPCF_OK;
 }

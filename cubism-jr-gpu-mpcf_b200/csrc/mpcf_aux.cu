@@ -37,7 +37,7 @@ __global__ void __launch_bounds__(256) sos_kernel(const SosArgs A)
 {
     typedef typename Pol::T T;
     __shared__ T wmax[8];
-    const int c = blockIdx.x;
+    const int c = A.chunk0 + blockIdx.x;
     int d = 0;
     while (d + 1 < A.ndom && A.doms[d + 1].sos_chunk_begin <= c) ++d;
     const DomDev& D = A.doms[d];

@@ -342,14 +342,15 @@ stage_kernel(const StageArgs A)
         __syncthreads();
     }
 
+    // tiles tile0 .. ntiles-1: from the work counter, or one per CTA
     int t;
     if (PERSIST)
     {
-        if (threadIdx.x == 0) *tile_bc = (int)atomicAdd(A.counter, 1u);
+        if (threadIdx.x == 0) *tile_bc = A.tile0 + (int)atomicAdd(A.counter, 1u);
         __syncthreads();
         t = *tile_bc;
     }
-    else t = blockIdx.x;
+    else t = A.tile0 + blockIdx.x;
 
     while (t < A.ntiles)
     {
@@ -865,7 +866,7 @@ stage_kernel(const StageArgs A)
         }
         if (!PERSIST) break;
         __syncthreads();
-        if (threadIdx.x == 0) *tile_bc = tma_late ? A.ntiles : (int)atomicAdd(A.counter, 1u);
+        if (threadIdx.x == 0) *tile_bc = tma_late ? A.ntiles : A.tile0 + (int)atomicAdd(A.counter, 1u);
         __syncthreads();
         t = *tile_bc;
     }

@@ -61,7 +61,8 @@ struct StageArgs
 {
     const DomDev* doms;
     int    ndom;
-    int    ntiles;      // total tiles over all domains
+    int    ntiles;      // end of the launch's tile range (all tiles: the total over all domains)
+    int    tile0;       // first tile of the launch's range (0: from the first tile)
     int    dz;          // z-chunk depth of a tile
     int    parity;      // read U[parity], write U[parity^1]
     double a, b;        // LSRK3 stage coefficients
@@ -88,8 +89,9 @@ struct SosArgs
 {
     const DomDev* doms;
     int    ndom;
-    int    nchunks;     // total chunks over all domains
+    int    nchunks;     // chunks of this launch (all domains: the total)
     int    chunk;       // cells per chunk
+    int    chunk0;      // first chunk of the launch (block b takes chunk chunk0 + b)
     int    parity;
     void*  sos_bits;    // per domain: unsigned (float bits) or unsigned long long (double bits)
 };

@@ -93,6 +93,7 @@ SIGNATURES = {
     "mpcf_compute_dt": (_I, [_P, _D, _D, _PD]),
     "mpcf_step": (_I, [_P, _D, _D, _PD]),
     "mpcf_run": (_I, [_P, _I, _D, _D, _I, _PD]),
+    "mpcf_run_host": (_I, [_P, _I, _D, _D, _PP, _I, _PD]),
     "mpcf_synchronize": (_I, [_P]),
     "mpcf_update": (_I, [_P, _D]),
     "mpcf_conserved_sums": (_I, [_P, _PD]),

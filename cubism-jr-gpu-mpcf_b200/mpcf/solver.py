@@ -132,6 +132,19 @@ class Solver:
         check(lib().mpcf_run(self._h, int(nsteps), float(cfl), float(dt_max), 1 if graph else 0, out))
         return list(out)
 
+    def run_host(self, host_state, nsteps, cfl=0.3, dt_max=1e30, nchunks=8):
+        """nsteps steps of a state held in host memory (mpcf_run_host):
+        `host_state` (7 contiguous arrays of the solver's dtype, pinned
+        memory for overlap) is every step's input and is overwritten with
+        every step's result.  Returns the time."""
+        for a in host_state:
+            if a.dtype != self.dtype or not a.flags["C_CONTIGUOUS"] or a.size != self.ncells(0):
+                raise ValueError("host fields must be contiguous arrays of the solver's dtype and size")
+        t = ctypes.c_double()
+        check(lib().mpcf_run_host(self._h, int(nsteps), float(cfl), float(dt_max), _ptr_array(host_state),
+                                  int(nchunks), ctypes.byref(t)))
+        return t.value
+
     def synchronize(self):
         check(lib().mpcf_synchronize(self._h))
 

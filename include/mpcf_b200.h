@@ -132,6 +132,25 @@ int mpcf_stage(mpcf_solver* s, double a, double b, const double* dtinvh);
 int mpcf_compute_dt(mpcf_solver* s, double cfl, double dt_max, double* dt_out);
 int mpcf_step(mpcf_solver* s, double cfl, double dt_max, double* dt_out);
 int mpcf_run(mpcf_solver* s, int nsteps, double cfl, double dt_max, int use_graph, double* time_out);
+/* nsteps LSRK3 steps of a state that lives in host memory: the reference's
+ * host-resident block streamed through the GPU (GPUlab::process_all's
+ * chunked, double-buffered PCIe transfers on three streams,
+ * GPUlab.cpp:202-372,703-793, under LSRK3_IntegratorMPI::operator(),
+ * LSRK3_IntegratorMPI.cpp:27-62).  host7: the 7 fields of the single domain
+ * (x fastest), read as every step's input and overwritten with every step's
+ * result; page-locked memory lets the copies overlap the kernels.  Every
+ * step uploads the state in z-chunks of whole tile layers on one copy
+ * stream, reduces each chunk's sound speed as it lands, computes dt and
+ * stages 1-2, then runs stage 3 chunk by chunk and downloads each chunk of
+ * the new state on a second copy stream as soon as it is written; the next
+ * step's upload of a chunk follows its download (copies in both directions
+ * overlap).  nchunks: requested chunks (at most the tile layers, nz/dz; one
+ * layer per chunk with the tiling's dz).  The register stays on the device
+ * (stage 1 multiplies it by a = 0).  Results are bit-identical to mpcf_run
+ * on the same state.  Single-domain solvers without halo faces;
+ * conservation tracking is not applied.  time_out (optional): the time. */
+int mpcf_run_host(mpcf_solver* s, int nsteps, double cfl, double dt_max, void* const* host7, int nchunks,
+                  double* time_out);
 int mpcf_synchronize(mpcf_solver* s);
 /* The state update alone, U <- U + b*R (Update_CUDA::compute ->
  * GPU::update -> _update, Update_CUDA.cpp:12-17, GPUkernels.cu:1142-1179),
