@@ -145,28 +145,49 @@ def all_state(s):
     return [np.concatenate([p[q] for p in parts]) for q in range(7)]
 
 
-def derived_fields(st, dtype=np.float64):
-    """(rho, p, G) in FP64 from a stored state; the state's arrays are
-    released as they are used (1024^3 states are tens of GB)."""
-    rho = st[0].astype(dtype)
-    ke = st[1].astype(dtype) ** 2
-    st[1] = None
-    ke += st[2].astype(dtype) ** 2
-    st[2] = None
-    ke += st[3].astype(dtype) ** 2
-    st[3] = None
-    ke *= 0.5
-    ke /= rho
-    p = st[4].astype(dtype)
-    st[4] = None
-    p -= ke
-    del ke
-    p -= st[6]
-    st[6] = None
-    G = st[5].astype(dtype)
-    st[5] = None
-    p /= G
+CHUNK = 1 << 24
+
+
+def derived_chunk(st, sl):
+    """(rho, p, G) in FP64 of cells `sl` of a stored state."""
+    rho = st[0][sl].astype(np.float64)
+    ke = st[1][sl].astype(np.float64) ** 2 + st[2][sl].astype(np.float64) ** 2 + st[3][sl].astype(np.float64) ** 2
+    G = st[5][sl].astype(np.float64)
+    p = (st[4][sl].astype(np.float64) - 0.5 * ke / rho - st[6][sl]) / G
     return rho, p, G
+
+
+def derived_fields(st):
+    """(rho, p, G) in FP64 of a stored state, computed in chunks of cells."""
+    n = st[0].size
+    out = [np.empty(n, np.float64) for _ in range(3)]
+    for i in range(0, n, CHUNK):
+        sl = slice(i, min(n, i + CHUNK))
+        for o, v in zip(out, derived_chunk(st, sl)):
+            o[sl] = v
+    return out
+
+
+def errors_against(st, ref):
+    """Relative L1 (mean |x - x64| / mean |x64|) and L-inf (max |x - x64| /
+    max |x64|) of rho, p and G of state `st` against the FP64 run's `ref`,
+    accumulated in chunks of cells."""
+    n = st[0].size
+    acc = np.zeros((3, 4))          # sum |d|, sum |ref|, max |d|, max |ref|
+    for i in range(0, n, CHUNK):
+        sl = slice(i, min(n, i + CHUNK))
+        for k, v in enumerate(derived_chunk(st, sl)):
+            r = ref[k][sl]
+            d = np.abs(v - r)
+            a = np.abs(r)
+            acc[k] += (d.sum(), a.sum(), 0, 0)
+            acc[k, 2] = max(acc[k, 2], d.max())
+            acc[k, 3] = max(acc[k, 3], a.max())
+    out = {}
+    for k, name in enumerate(("rho", "p", "G")):
+        out["L1_" + name] = float(acc[k, 0] / acc[k, 1])
+        out["Linf_" + name] = float(acc[k, 2] / acc[k, 3])
+    return out
 
 
 def time_steps(mpcf, s, steps, warmup, cfl, dist=None):
@@ -366,12 +387,6 @@ def main():
     K, W = args.steps, max(3, args.warmup)
     cfl = mpcf.configs.CFL
 
-    def l1(a, b):
-        return float(np.mean(np.abs(a - b)) / np.mean(np.abs(b)))
-
-    def linf(a, b):
-        return float(np.max(np.abs(a - b)) / np.max(np.abs(b)))
-
     # ---------------- mixed (headline): W warm-up + K timed graph replays
     s = make_solver(mpcf, cfg, args.precision)
     s.set_tiling(*pick_tiling(mpcf, s))
@@ -387,9 +402,11 @@ def main():
     # the device error word after the warm-up and timed steps (0: every
     # update stayed physical, every sound speed real and finite)
     err_word = s.error_word()
-    derived = {}
+    # states of the forms compared with the FP64 run, kept until it exists;
+    # the FP64 run's (rho, p, G)
+    states, ref64 = {}, None
     if rank == 0:
-        derived[args.precision] = derived_fields(all_state(s))
+        states[args.precision] = all_state(s)
     # roofline of the dominant kernel (the stage) on this same solver
     st_ms = stage_kernel_ms(mpcf, s)
     nt, grid, threads = s.launch_shape()
@@ -413,23 +430,23 @@ def main():
         others[prec] = {"value": world * ncell * 3.0 * K / (mso * 1e-3), "ms_per_step": mso / K,
                         "tiling": so.tiling()}
         if rank == 0:
-            derived[prec] = derived_fields(all_state(so))
+            if prec == "fp64":
+                ref64 = derived_fields(all_state(so))
+            else:
+                states[prec] = all_state(so)
         so.close()
-        if rank == 0 and "fp64" in derived:
-            # errors against the FP64 run as soon as both exist; the other
-            # forms' fields are then dropped
-            r64, p64, G64 = derived["fp64"]
-            for pr in [k for k in derived if k != "fp64"]:
-                r, p, G = derived.pop(pr)
-                err_by[pr] = {"L1_rho": l1(r, r64), "Linf_rho": linf(r, r64), "L1_p": l1(p, p64),
-                              "Linf_p": linf(p, p64), "L1_G": l1(G, G64), "Linf_G": linf(G, G64)}
-                del r, p, G
+        if rank == 0 and ref64 is not None:
+            # errors against the FP64 run as soon as both exist; the states
+            # are then dropped (1024^3 states are tens of GB)
+            for pr in list(states):
+                err_by[pr] = errors_against(states.pop(pr), ref64)
     err = None
     if err_by:
         err = dict(err_by)
         err["note"] = ("relative L1 (mean |x-x64| / mean |x64|) and L-inf (max |x-x64| / max |x64|) "
                        "against the all-FP64 GPU run after the same %d steps (W+K) from the same IC" % (W + K))
-    derived.clear()
+    states.clear()
+    ref64 = None
 
     # ---------------- e2e through the C ABI with host buffers
     e2e = None
