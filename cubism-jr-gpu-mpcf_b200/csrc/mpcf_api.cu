@@ -332,8 +332,6 @@ StageArgs stage_args(mpcf_solver* s, double a, double b, bool sums)
     A.tmaps = s->tmaps;
     A.sos_bits = nullptr;
     A.test_flags = s->test_flags;
-    A.one = 1.0f;
-    A.mzero = -0.0f;
     return A;
 }
 

@@ -446,76 +446,13 @@ __device__ __forceinline__ void hllc_face_packed(const FaceState<T>& S, const in
     o.Gm = S.Gm; o.Gp = S.Gp; o.Pm = S.Pm; o.Pp = S.Pp;
 }
 
-// ---------------------------------------------------------------------------
-// Exactly rounded FP32 pairs (reference-rounding policy).  A packed multiply
-// and a packed add are written as packed fused multiply-adds with an
-// identity operand, a*b + (-0) and a*1 + b (a - b as b*(-1) + a): each lane
-// rounds once, like the scalar operation.  The identities come from the
-// kernel's arguments, so the code generator cannot see their values and
-// merge a multiply with the add that consumes it into one fused operation
-// (which would round once for both).
-// ---------------------------------------------------------------------------
-struct ExactPair
-{
-    float2 one, mone, mzero;
-};
-__device__ __forceinline__ float2 xmul2(const float2 a, const float2 b, const ExactPair& E) { return __ffma2_rn(a, b, E.mzero); }
-__device__ __forceinline__ float2 xadd2(const float2 a, const float2 b, const ExactPair& E) { return __ffma2_rn(a, E.one, b); }
-__device__ __forceinline__ float2 xsub2(const float2 a, const float2 b, const ExactPair& E) { return __ffma2_rn(b, E.mone, a); }
-
-// weno_cell_ref for FP32 with the two edges (and the f / g indicator pair)
-// as exactly rounded pairs: every lane performs the scalar form's operations
-// in its order, so R and L are bit-identical to weno_cell_ref<PolRef32>.
-// Lane x is the minus side (right edge R), lane y the plus side (left edge L).
-__device__ __forceinline__ void weno_cell_ref_x2(const float y0, const float y1, const float y2, const float y3,
-                                                 const float y4, float& R, float& L, const ExactPair& E)
-{
-    typedef float T;
-    // beta_f(y0, y1, y2) in lane x, beta_g(y2, y3, y4) in lane y:
-    //   x*(x*c1 - y*c2 + z*c3) + y*(y*c4 - z*c5) + z*z*c6
-    const float2 X = f2(y0, y2), Y = f2(y1, y3), Z = f2(y2, y4);
-    const float2 t = xmul2(X, xadd2(xsub2(xmul2(X, f2((T)(4./3.), (T)(10./3.)), E), xmul2(Y, f2((T)(19./3.), (T)(31./3.)), E), E),
-                                    xmul2(Z, f2s((T)(11./3.)), E), E), E);
-    const float2 u = xmul2(Y, xsub2(xmul2(Y, f2s((T)(25./3.)), E), xmul2(Z, f2((T)(31./3.), (T)(19./3.)), E), E), E);
-    const float2 PFG = xadd2(xadd2(xadd2(t, u, E), xmul2(xmul2(Z, Z, E), f2((T)(10./3.), (T)(4./3.)), E), E),
-                             f2s((T)MPCF_WENOEPS), E);
-    const T ph = beta_h<T>(y1, y2, y3) + (T)MPCF_WENOEPS;
-    // the 10.0 literal promotes these to double (GPUonly.cuh:111-113)
-    const double qf = ((T)1)/(10.0*PFG.x*PFG.x);
-    const double qh = ((T)1)/(10.0*ph*ph);
-    const double qg = ((T)1)/(10.0*PFG.y*PFG.y);
-    const T a1 = (T)((T)(6)*qh);
-    const float2 A0 = f2((T)((T)(1)*qf), (T)((T)(1)*qg));     // minus a0, plus a0
-    const float2 A2 = f2((T)((T)(3)*qg), (T)((T)(3)*qf));     // minus a2, plus a2
-    const float2 A1 = f2s(a1);
-    const float2 S = xadd2(xadd2(A0, A1, E), A2, E);
-    const float2 INV = f2(((T)1)/S.x, ((T)1)/S.y);
-    const float2 W0 = xmul2(A0, INV, E), W1 = xmul2(A1, INV, E);
-    const float2 W2 = xsub2(xsub2(E.one, W0, E), W1, E);
-    // candidates: minus (y0..y4), plus mirrored (y4..y0)
-    const float2 c0 = xadd2(xsub2(xmul2(f2s((T)(1./3.)), f2(y0, y4), E), xmul2(f2s((T)(7./6.)), f2(y1, y3), E), E),
-                            xmul2(f2s((T)(11./6.)), f2s(y2), E), E);
-    const float2 c1 = xadd2(xadd2(xmul2(f2s(-(T)(1./6.)), f2(y1, y3), E), xmul2(f2s((T)(5./6.)), f2s(y2), E), E),
-                            xmul2(f2s((T)(1./3.)), f2(y3, y1), E), E);
-    const float2 c2 = xsub2(xadd2(xmul2(f2s((T)(1./3.)), f2s(y2), E), xmul2(f2s((T)(5./6.)), f2(y3, y1), E), E),
-                            xmul2(f2s((T)(1./6.)), f2(y4, y0), E), E);
-    const float2 r = xadd2(xadd2(xmul2(W0, c0, E), xmul2(W1, c1, E), E), xmul2(W2, c2, E), E);
-    const T lo = dmin(dmin(y1, y2), y3);
-    const T hi = dmax(dmax(y1, y2), y3);
-    R = dmin(dmax(r.x, lo), hi);
-    L = dmin(dmax(r.y, lo), hi);
-}
-
 // Both edge values of one cell in the policy's arithmetic.
 template <class Pol>
 __device__ __forceinline__ void weno_cell(const typename Pol::T y0, const typename Pol::T y1,
         const typename Pol::T y2, const typename Pol::T y3, const typename Pol::T y4,
-        typename Pol::T& R, typename Pol::T& L, const ExactPair& E)
+        typename Pol::T& R, typename Pol::T& L)
 {
     if constexpr (Pol::kFastWeno) weno_cell_packed<typename Pol::T>(y0, y1, y2, y3, y4, R, L);
-#ifdef MPCF_REF_PACKED
-    else if constexpr (sizeof(typename Pol::T) == 4) weno_cell_ref_x2(y0, y1, y2, y3, y4, R, L, E);
-#endif
     else                          weno_cell_ref<Pol>(y0, y1, y2, y3, y4, R, L);
 }
 

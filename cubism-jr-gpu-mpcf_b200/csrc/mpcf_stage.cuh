@@ -306,8 +306,6 @@ stage_kernel(const StageArgs A)
     const T a = (T)A.a;
     const T b = (T)A.b;
     const T factor6 = (T)1.0f / (T)6.0f;   // GPUkernels.cu:1103
-    // identity operands of the exactly rounded pairs (from the arguments)
-    const ExactPair EX = {make_float2(A.one, A.one), make_float2(-A.one, -A.one), make_float2(A.mzero, A.mzero)};
     bool ok = true;
     bool oob = false;                      // bounds-checking build: an index left its buffer
     uint32_t phA = 0, phB = 0;             // mbarrier phase parities
@@ -657,7 +655,7 @@ stage_kernel(const StageArgs A)
                         for (int q = 0; q < 7; ++q)
                         {
                             const T* pl = sm + q * L::kPP;
-                            weno_cell<Pol>(pl[ad[0]], pl[ad[1]], pl[ad[2]], pl[ad[3]], pl[ad[4]], Rv[q], Lv[q], EX);
+                            weno_cell<Pol>(pl[ad[0]], pl[ad[1]], pl[ad[2]], pl[ad[3]], pl[ad[4]], Rv[q], Lv[q]);
                         }
                         if (cz == k)
                         {
@@ -712,7 +710,7 @@ stage_kernel(const StageArgs A)
                         for (int q = 0; q < 7; ++q)
                         {
                             const T* pl = sm + q * L::kPP + base;
-                            weno_cell<Pol>(pl[-2 * step], pl[-step], pl[0], pl[step], pl[2 * step], Rv[q], Lv[q], EX);
+                            weno_cell<Pol>(pl[-2 * step], pl[-step], pl[0], pl[step], pl[2 * step], Rv[q], Lv[q]);
                         }
                         if (dR >= 0)
                         {
@@ -751,7 +749,7 @@ stage_kernel(const StageArgs A)
 #endif
                             const T* pl = sm + q * L::kPP + base;
                             T rv, lv;
-                            weno_cell<Pol>(pl[-2 * step], pl[-step], pl[0], pl[step], pl[2 * step], rv, lv, EX);
+                            weno_cell<Pol>(pl[-2 * step], pl[-step], pl[0], pl[step], pl[2 * step], rv, lv);
                             // the right / upper edge fills a minus slot, the
                             // left / lower edge a plus slot
                             if (dR >= 0) sm[dR + q * L::kFP] = rv;

@@ -73,7 +73,6 @@ struct StageArgs
     const void* tmaps;  // per domain 4 CUtensorMap (128 B each): [buffer 0, 1] x [halo box, interior box]
     void* sos_bits;     // per domain maximum sound speed of the new state (bits), or null
     unsigned test_flags; // TEST_* below; 0 outside the failure-detection tests
-    float  one, mzero;  // 1 and -0: identity operands of exactly rounded packed operations
 };
 
 // Failure-detection tests: with TEST_DROP_LAST_COPY a non-persistent stage
