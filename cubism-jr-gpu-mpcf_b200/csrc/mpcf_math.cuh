@@ -33,7 +33,6 @@
 
 #include <cuda_runtime.h>
 #include <stdint.h>
-#include "mpcf_ieee.cuh"
 
 namespace mpcf {
 
@@ -85,11 +84,6 @@ __device__ __forceinline__ float sqrt_approx(float x)
     return r;
 }
 
-// 1/x in the reference rounding: the correctly rounded reciprocal, without a
-// branch in single precision
-template <class T> __device__ __forceinline__ T rcp_ref(const T x) { return ((T)1) / x; }
-template <> __device__ __forceinline__ float rcp_ref<float>(const float x) { return rcp_rn_f32(x); }
-
 // ---------------------------------------------------------------------------
 // WENO5 smoothness indicators.  For a window of three consecutive cells
 // (x, y, z) left to right, the reference uses three polynomial forms:
@@ -140,26 +134,16 @@ __device__ __forceinline__ void weno_cell_ref(const typename Pol::T y0, const ty
     const T ph = beta_h<T>(y1, y2, y3) + (T)MPCF_WENOEPS;
     const T pg = beta_g<T>(y2, y3, y4) + (T)MPCF_WENOEPS;
     // the 10.0 literal promotes these to double (GPUonly.cuh:111-113)
-#if defined(MPCF_REF_BRANCHFREE) || defined(MPCF_REF_BF_W)
-    const double qf = sizeof(T) == 4 ? rcp_rn_f64_weight(10.0*pf*pf) : ((T)1)/(10.0*pf*pf);
-    const double qh = sizeof(T) == 4 ? rcp_rn_f64_weight(10.0*ph*ph) : ((T)1)/(10.0*ph*ph);
-    const double qg = sizeof(T) == 4 ? rcp_rn_f64_weight(10.0*pg*pg) : ((T)1)/(10.0*pg*pg);
-#else
     const double qf = ((T)1)/(10.0*pf*pf);
     const double qh = ((T)1)/(10.0*ph*ph);
     const double qg = ((T)1)/(10.0*pg*pg);
-#endif
     const T a1 = (T)((T)(6)*qh);
     const T lo = dmin(dmin(y1, y2), y3);
     const T hi = dmax(dmax(y1, y2), y3);
     {
         // minus side: indicators (f, h, g)
         const T a0 = (T)((T)(1)*qf), a2 = (T)((T)(3)*qg);
-#if defined(MPCF_REF_BRANCHFREE) || defined(MPCF_REF_BF_INV)
-        const T inv = rcp_ref<T>(a0 + a1 + a2);
-#else
         const T inv = ((T)1)/(a0 + a1 + a2);
-#endif
         const T w0 = a0 * inv, w1 = a1 * inv, w2 = 1 - w0 - w1;
         const T r = w0*((T)(1.0/3.)*y0-(T)(7./6.)*y1+(T)(11./6.)*y2) + w1*(-(T)(1./6.)*y1+(T)(5./6.)*y2+(T)(1./3.)*y3) + w2*((T)(1./3.)*y2+(T)(5./6.)*y3-(T)(1./6.)*y4);
         R = dmin(dmax(r, lo), hi);
@@ -167,11 +151,7 @@ __device__ __forceinline__ void weno_cell_ref(const typename Pol::T y0, const ty
     {
         // plus side: indicators (g, h, f)
         const T a0 = (T)((T)(1)*qg), a2 = (T)((T)(3)*qf);
-#if defined(MPCF_REF_BRANCHFREE) || defined(MPCF_REF_BF_INV)
-        const T inv = rcp_ref<T>(a0 + a1 + a2);
-#else
         const T inv = ((T)1)/(a0 + a1 + a2);
-#endif
         const T w0 = a0 * inv, w1 = a1 * inv, w2 = 1 - w0 - w1;
         const T r = w0*((T)(1./3.)*y4-(T)(7./6.)*y3+(T)(11./6.)*y2) + w1*(-(T)(1./6.)*y3+(T)(5./6.)*y2+(T)(1./3.)*y1) + w2*((T)(1./3.)*y2+(T)(5./6.)*y1-(T)(1./6.)*y0);
         L = dmin(dmax(r, lo), hi);

@@ -126,7 +126,6 @@ SIGNATURES = {
     "mpcf_set_tiling": (_I, [_P, _I, _I, _I]),
     "mpcf_set_test_flags": (_I, [_P, _c.c_uint]),
     "mpcf_test_copy_count": (_I, [_P, _c.POINTER(_c.c_uint), _I]),
-    "mpcf_selftest_ieee": (_I, [_I, _I, _c.POINTER(_c.c_ulonglong), _c.POINTER(_c.c_uint)]),
     "mpcf_get_tiling": (_I, [_P, _PI, _PI, _PI]),
     "mpcf_autotune": (_I, [_P, _I, _PI, _PD]),
     "mpcf_launch_shape": (_I, [_P, _c.POINTER(_c.c_longlong), _c.POINTER(_c.c_longlong), _PI]),

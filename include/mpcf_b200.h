@@ -384,15 +384,6 @@ int mpcf_autotune(mpcf_solver* s, int reps, int* best3, double* best_ms);
 #define MPCF_TEST_DROP_LAST_COPY 1u
 #define MPCF_TEST_DROP_MID_COPY  2u
 int mpcf_set_test_flags(mpcf_solver* s, unsigned flags);
-/* Self-test of the correctly rounded reciprocals that the FP32
- * reference-rounding stage kernel uses in place of division (no reference
- * counterpart): which = 0 checks the WENO weights' double reciprocal
- * 1/(10 x^2), which = 1 the float reciprocal 1/x, each against the IEEE
- * quotient for every one of the 2^32 float bit patterns x on `device`.
- * *mismatches receives the count (0: identical everywhere, NaNs compared as
- * NaN), first8 (optional) the first mismatching bit patterns.  About a
- * second on a B200. */
-int mpcf_selftest_ieee(int which, int device, unsigned long long* mismatches, unsigned* first8);
 /* Failure-detection tests only: bulk copies the stage kernel issued while a
  * test flag was set (clear != 0 resets the count).  No reference
  * counterpart. */

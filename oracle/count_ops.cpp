@@ -50,6 +50,8 @@ static inline CF cf_sqrt(const CF& a) { ++g_ops; return CF(std::sqrt(a.v)); }
 static inline CF cf_abs(const CF& a) { ++g_ops; return CF(std::fabs(a.v)); }
 
 #define ORACLE_WENOEPS 1e-6
+/* the operation count is the WENO5 build's */
+static int g_oracle_weno3 = 0;
 #define REAL CF
 #define SFX(name) name##_cnt
 #define RMIN cf_min

@@ -18,6 +18,11 @@
 /* WENOEPS: Makefile.config:15,252 (weps ?= 1e-6) */
 #define ORACLE_WENOEPS 1e-6
 
+/* reconstruction order: 0 WENO5 (the default build), 1 the reference's
+ * compile-time _WENO3_ build (GPUonly.cuh:102,141) */
+static int g_oracle_weno3 = 0;
+void oracle_set_weno3(int on) { g_oracle_weno3 = on != 0; }
+
 /* ---- single precision ---- */
 #define REAL float
 #define SFX(name) name##_f32

@@ -33,6 +33,18 @@
 /* ---------------------------------------------------------------------- */
 static REAL SFX(weno_pluss)(const REAL b, const REAL c, const REAL d, const REAL e, const REAL f)
 {
+    if (g_oracle_weno3)
+    {
+        /* the reference's _WENO3_ build (GPUonly.cuh:125-137): the WENOEPS
+         * and fraction literals promote the weights and the result to double */
+        const REAL is0 = (d-e)*(d-e);
+        const REAL is1 = (d-c)*(d-c);
+        const REAL alpha0 = (1./3.)/((is0+ORACLE_WENOEPS)*(is0+ORACLE_WENOEPS));
+        const REAL alpha1 = (2./3.)/((is1+ORACLE_WENOEPS)*(is1+ORACLE_WENOEPS));
+        const REAL omega0 = alpha0/(alpha0+alpha1);
+        const REAL omega1 = 1.-omega0;
+        return omega0*(1.5*d-.5*e) + omega1*(.5*d+.5*c);
+    }
     const REAL is0 = d*(d*(REAL)(10./3.)- e*(REAL)(31./3.) + f*(REAL)(11./3.)) + e*(e*(REAL)(25./3.) - f*(REAL)(19./3.)) +    f*f*(REAL)(4./3.);
     const REAL is1 = c*(c*(REAL)(4./3.) - d*(REAL)(13./3.) + e*(REAL)(5./3.)) + d*(d*(REAL)(13./3.)  - e*(REAL)(13./3.)) +    e*e*(REAL)(4./3.);
     const REAL is2 = b*(b*(REAL)(4./3.) - c*(REAL)(19./3.) + d*(REAL)(11./3.)) + c*(c*(REAL)(25./3.) - d*(REAL)(31./3.)) +    d*d*(REAL)(10./3.);
@@ -56,6 +68,18 @@ static REAL SFX(weno_pluss)(const REAL b, const REAL c, const REAL d, const REAL
 
 static REAL SFX(weno_minus)(const REAL a, const REAL b, const REAL c, const REAL d, const REAL e)
 {
+    if (g_oracle_weno3)
+    {
+        /* _WENO3_ (GPUonly.cuh:164-176); note 1./(3.*x*x) here against
+         * (1./3.)/(x*x) on the plus side */
+        const REAL is0 = (c-b)*(c-b);
+        const REAL is1 = (d-c)*(d-c);
+        const REAL alpha0 = 1./(3.*(is0+ORACLE_WENOEPS)*(is0+ORACLE_WENOEPS));
+        const REAL alpha1 = 2./(3.*(is1+ORACLE_WENOEPS)*(is1+ORACLE_WENOEPS));
+        const REAL omega0=alpha0/(alpha0+alpha1);
+        const REAL omega1=1.-omega0;
+        return omega0*(1.5*c-.5*b) + omega1*(.5*c+.5*d);
+    }
     const REAL is0 = a*(a*(REAL)(4./3.)  - b*(REAL)(19./3.)  + c*(REAL)(11./3.)) + b*(b*(REAL)(25./3.)  - c*(REAL)(31./3.)) + c*c*(REAL)(10./3.);
     const REAL is1 = b*(b*(REAL)(4./3.)  - c*(REAL)(13./3.)  + d*(REAL)(5./3.))  + c*(c*(REAL)(13./3.)  - d*(REAL)(13./3.)) + d*d*(REAL)(4./3.);
     const REAL is2 = c*(c*(REAL)(10./3.) - d*(REAL)(31./3.)  + e*(REAL)(11./3.)) + d*(d*(REAL)(25./3.)  - e*(REAL)(19./3.)) + e*e*(REAL)(4./3.);
