@@ -7,6 +7,7 @@ Run where the reference tree is present, after `make -C oracle ref`:
 It calls the reference's own code compiled from its sources (oracle/_ref):
   * source/GPU/GPUonly.cuh device math (WENO5 +/- with clipping, Einfeldt,
     Batten s*, HLLC rho/vel/pvel/e, extra-term velocity, stencil reads),
+    and its WENO3 reconstruction (the -D_WENO3_ build),
   * source/BoundaryConditions.h absorbing/reflecting ghost fills,
   * source/MaxSpeedOfSound.cpp (MaxSpeedOfSound_CPP::compute),
   * source/Sim/Sim_SICCloudMPI.cpp (the shock-induced cloud-collapse IC,
@@ -100,6 +101,17 @@ def make_devmath(L, rng):
     np.savez_compressed(os.path.join(HERE, "ref_devmath.npz"), weno_in=W, weno_minus_clipped=wm,
                         weno_pluss_clipped=wp, weno_minus=wmu, weno_pluss=wpu, states=S, sm=sm, sp=sp,
                         ss=ss, hllc_rho=hr, hllc_vel=hv, hllc_pvel=hpv, hllc_e=he, extraterm=hx)
+
+
+def make_devmath_w3(rng):
+    """The reference's compile-time WENO3 build (-D_WENO3_) of the same
+    reconstruction functions."""
+    L = O.ref_lib("libref_devmath_w3_8x7x6")
+    W = weno_inputs(rng, 3000)
+    wm = np.array([L.ref_weno_minus_clipped(*map(float, w[:5])) for w in W], np.float32)
+    wp = np.array([L.ref_weno_pluss_clipped(*map(float, w[1:])) for w in W], np.float32)
+    np.savez_compressed(os.path.join(HERE, "ref_devmath_w3.npz"), weno_in=W, weno_minus_clipped=wm,
+                        weno_pluss_clipped=wp)
 
 
 def cloud(dims, seed):
@@ -241,6 +253,7 @@ def main():
     make_sic(np.random.default_rng(20261204))
     make_dump()
     make_cases()
+    make_devmath_w3(np.random.default_rng(20261205))
     print("wrote", sorted(f for f in os.listdir(HERE) if f.endswith(".npz")))
 
 

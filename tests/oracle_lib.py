@@ -66,6 +66,7 @@ def oracle():
         L.oracle_stencil_f32.argtypes = [_I, _I, _I, _PPF, _PF, _PF, _PF, _I, _I, _I, _I, _I, _PF]
         L.oracle_sic_cloud_f32.argtypes = [_I, _I, _I, _PD, _I, _PD, _D, _PPF, _PD]
         L.oracle_sic_cloud_f64.argtypes = [_I, _I, _I, _PD, _I, _PD, _D, _PPD, _PD]
+        L.oracle_set_weno3.argtypes = [_I]
         L.oracle_bubbles.restype = _I
         L.oracle_bubbles.argtypes = [_c.c_ulonglong, _I, _D, _D, _PD, _PD, _D, _I, _PD]
         L.oracle_ic_cloud_f32.argtypes = [_I, _I, _I, _PI, _PI, _PD, _c.c_ulonglong, _I, _PD, _PPF]
@@ -96,7 +97,7 @@ def ref_lib(name):
     if name == "libref_sic_ic":
         L.ref_sic_dims.argtypes = [_PI]
         L.ref_sic_ic.argtypes = [_c.c_char_p, _I, _c.POINTER(_c.c_char_p), _D, _PPF, _PD]
-    if name.startswith("libref_devmath"):
+    if name.startswith("libref_devmath"):   # the WENO5 and the WENO3 build
         L.ref_devmath_dims.argtypes = [_PI]
         for n in ("ref_weno_pluss", "ref_weno_minus", "ref_weno_pluss_clipped", "ref_weno_minus_clipped"):
             getattr(L, n).restype = _F
@@ -443,3 +444,16 @@ def ic_cloud(dims, params, bub, dtype=np.float32, origin=None, glob=None):
     f(nx, ny, nz, o3, g3, prm.ctypes.data_as(_PD), _c.c_ulonglong(seed), b.size // 4,
       b.ctypes.data_as(_PD) if b.size else None, fptrs(out))
     return out
+
+
+class weno3:
+    """Context manager: the oracle's reconstruction is the reference's
+    compile-time WENO3 build while inside (GPUonly.cuh:102,141)."""
+
+    def __enter__(self):
+        oracle().oracle_set_weno3(1)
+        return self
+
+    def __exit__(self, *exc):
+        oracle().oracle_set_weno3(0)
+        return False

@@ -46,6 +46,22 @@ def test_golden_weno():
     assert eq(wp, g["weno_pluss_clipped"])
 
 
+def test_golden_weno3():
+    """The reference's compile-time WENO3 build (GPUonly.cuh:102,141)."""
+    g = np.load(os.path.join(GOLD, "ref_devmath_w3.npz"))
+    L = O.oracle()
+    W = g["weno_in"]
+    with O.weno3():
+        wm = np.array([L.oracle_weno_minus_clipped_f32(*map(float, w[:5])) for w in W], np.float32)
+        wp = np.array([L.oracle_weno_pluss_clipped_f32(*map(float, w[1:])) for w in W], np.float32)
+    assert eq(wm, g["weno_minus_clipped"])
+    assert eq(wp, g["weno_pluss_clipped"])
+    # WENO5 again once the context is left
+    g5 = np.load(os.path.join(GOLD, "ref_devmath.npz"))
+    w = g5["weno_in"][1]
+    assert eq(L.oracle_weno_minus_clipped_f32(*map(float, w[:5])), g5["weno_minus_clipped"][1])
+
+
 def test_golden_wave_speeds_and_hllc():
     g = np.load(os.path.join(GOLD, "ref_devmath.npz"))
     L = O.oracle()
@@ -106,6 +122,19 @@ def test_live_weno_random(refdev):
         w = (rng.normal(0, 1, 6) * 10 ** rng.uniform(-5, 4)).astype(np.float32)
         assert eq(L.oracle_weno_minus_clipped_f32(*map(float, w[:5])), refdev.ref_weno_minus_clipped(*map(float, w[:5])))
         assert eq(L.oracle_weno_pluss_clipped_f32(*map(float, w[1:])), refdev.ref_weno_pluss_clipped(*map(float, w[1:])))
+
+
+def test_live_weno3_random():
+    L3 = O.ref_lib("libref_devmath_w3_8x7x6")
+    if L3 is None:
+        pytest.skip("oracle/_ref not built (the reference tree is absent)")
+    rng = np.random.default_rng(98)
+    L = O.oracle()
+    with O.weno3():
+        for _ in range(2000):
+            w = (rng.normal(0, 1, 6) * 10 ** rng.uniform(-5, 4)).astype(np.float32)
+            assert eq(L.oracle_weno_minus_clipped_f32(*map(float, w[:5])), L3.ref_weno_minus_clipped(*map(float, w[:5])))
+            assert eq(L.oracle_weno_pluss_clipped_f32(*map(float, w[1:])), L3.ref_weno_pluss_clipped(*map(float, w[1:])))
 
 
 def test_live_stencil_reads(refdev):
