@@ -133,6 +133,7 @@ struct mpcf_solver
     bool graph_cons = false;
 
     unsigned test_flags = 0;        // MPCF_TEST_* (failure-detection tests only)
+    bool weno3 = false;             // the reference's compile-time WENO3 reconstruction
 
     // runs over host-resident state (mpcf_run_host): two copy streams and
     // per-chunk events, made on first use
@@ -158,6 +159,7 @@ bool valid_ty(const mpcf_solver* s, int ty)
 
 StageKernelInfo stage_info(const mpcf_solver* s, int ty, bool persist, bool sums, bool tma)
 {
+    if (s->weno3) return s->pol == 0 ? stage_info_ref_w3(ty, persist, sums, tma) : stage_info_fp64_w3(ty, persist, sums, tma);
     switch (s->pol)
     {
         case 0: return stage_info_ref(ty, persist, sums, tma);
@@ -170,6 +172,9 @@ StageKernelInfo stage_info(const mpcf_solver* s, int ty, bool persist, bool sums
 
 cudaError_t launch_stage(const mpcf_solver* s, const StageArgs& A, int grid, cudaStream_t st)
 {
+    if (s->weno3)
+        return s->pol == 0 ? launch_stage_ref_w3(s->ty, s->persist != 0, s->tma != 0, A, grid, st)
+                           : launch_stage_fp64_w3(s->ty, s->persist != 0, s->tma != 0, A, grid, st);
     switch (s->pol)
     {
         case 0: return launch_stage_ref(s->ty, s->persist != 0, s->tma != 0, A, grid, st);
@@ -1541,6 +1546,25 @@ int mpcf_test_copy_count(mpcf_solver* s, unsigned* count, int clear)
     CK(cudaStreamSynchronize(s->stream));
     *count = *(unsigned*)s->host_stage;
     return MPCF_OK;
+}
+
+int mpcf_set_weno_order(mpcf_solver* s, int order)
+{
+    if (!s) return fail(MPCF_ERR_ARG, "null solver");
+    if (order != 5 && order != 3) return fail(MPCF_ERR_ARG, "reconstruction order %d: 5 or 3", order);
+    if (order == 3 && s->pol != MPCF_PREC_FP32_REF && s->pol != MPCF_PREC_FP64)
+        return fail(MPCF_ERR_ARG, "WENO3 is built for the reference-rounding forms (MPCF_PREC_FP32_REF, MPCF_PREC_FP64)");
+    DeviceGuard g(s->device);
+    CK(cudaStreamSynchronize(s->stream));
+    s->weno3 = order == 3;
+    destroy_graphs(s);    // captured launches are of the other kernel
+    return MPCF_OK;
+}
+
+int mpcf_get_weno_order(const mpcf_solver* s)
+{
+    if (!s) return fail(MPCF_ERR_ARG, "null solver");
+    return s->weno3 ? 3 : 5;
 }
 
 int mpcf_get_tiling(const mpcf_solver* s, int* ty, int* dz, int* flags)

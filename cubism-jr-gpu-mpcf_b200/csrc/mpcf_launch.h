@@ -24,11 +24,16 @@ cudaError_t launch_stage_fast32(int ty, bool persist, bool tma, const StageArgs&
 cudaError_t launch_stage_mixed(int ty, bool persist, bool tma, const StageArgs& A, int grid, cudaStream_t st);
 cudaError_t launch_stage_fp64(int ty, bool persist, bool tma, const StageArgs& A, int grid, cudaStream_t st);
 cudaError_t launch_stage_fast64(int ty, bool persist, bool tma, const StageArgs& A, int grid, cudaStream_t st);
+// the reference's compile-time WENO3 build of the reference-rounding forms
+cudaError_t launch_stage_ref_w3(int ty, bool persist, bool tma, const StageArgs& A, int grid, cudaStream_t st);
+cudaError_t launch_stage_fp64_w3(int ty, bool persist, bool tma, const StageArgs& A, int grid, cudaStream_t st);
 StageKernelInfo stage_info_ref(int ty, bool persist, bool sums, bool tma);
 StageKernelInfo stage_info_fast32(int ty, bool persist, bool sums, bool tma);
 StageKernelInfo stage_info_mixed(int ty, bool persist, bool sums, bool tma);
 StageKernelInfo stage_info_fp64(int ty, bool persist, bool sums, bool tma);
 StageKernelInfo stage_info_fast64(int ty, bool persist, bool sums, bool tma);
+StageKernelInfo stage_info_ref_w3(int ty, bool persist, bool sums, bool tma);
+StageKernelInfo stage_info_fp64_w3(int ty, bool persist, bool sums, bool tma);
 
 // mpcf_aux.cu
 cudaError_t launch_sos(int pol, const SosArgs& A, cudaStream_t st);

@@ -24,6 +24,8 @@
 //   PolFast64  double storage and arithmetic with the fast forms' algebra
 //              (factored indicators and fluxes, refined double reciprocals):
 //              the tuned FP64 yardstick of the mixed form.
+//   PolRef32W3, PolFP64W3  the two reference-rounding forms with the
+//              reference's compile-time WENO3 reconstruction.
 //
 // Primitive index convention used throughout the device code:
 //   0 rho, 1 u, 2 v, 3 w, 4 p, 5 G = 1/(gamma-1), 6 P = gamma*pc/(gamma-1)
@@ -40,11 +42,15 @@ namespace mpcf {
 #define MPCF_WENOEPS 1e-6   // Makefile.config:15 (weps ?= 1e-6)
 #endif
 
-struct PolRef32  { typedef float  T; static constexpr bool kFastWeno = false; static constexpr bool kP64 = false; static constexpr bool kRefRounding = true;  static constexpr int id = 0; };
-struct PolFast32 { typedef float  T; static constexpr bool kFastWeno = true;  static constexpr bool kP64 = false; static constexpr bool kRefRounding = false; static constexpr int id = 1; };
-struct PolMixed  { typedef float  T; static constexpr bool kFastWeno = true;  static constexpr bool kP64 = true;  static constexpr bool kRefRounding = false; static constexpr int id = 2; };
-struct PolFP64   { typedef double T; static constexpr bool kFastWeno = false; static constexpr bool kP64 = false; static constexpr bool kRefRounding = true;  static constexpr int id = 3; };
-struct PolFast64 { typedef double T; static constexpr bool kFastWeno = true;  static constexpr bool kP64 = false; static constexpr bool kRefRounding = false; static constexpr int id = 4; };
+struct PolRef32  { typedef float  T; static constexpr bool kFastWeno = false; static constexpr bool kP64 = false; static constexpr bool kRefRounding = true;  static constexpr bool kWeno3 = false; static constexpr int id = 0; };
+struct PolFast32 { typedef float  T; static constexpr bool kFastWeno = true;  static constexpr bool kP64 = false; static constexpr bool kRefRounding = false; static constexpr bool kWeno3 = false; static constexpr int id = 1; };
+struct PolMixed  { typedef float  T; static constexpr bool kFastWeno = true;  static constexpr bool kP64 = true;  static constexpr bool kRefRounding = false; static constexpr bool kWeno3 = false; static constexpr int id = 2; };
+struct PolFP64   { typedef double T; static constexpr bool kFastWeno = false; static constexpr bool kP64 = false; static constexpr bool kRefRounding = true;  static constexpr bool kWeno3 = false; static constexpr int id = 3; };
+struct PolFast64 { typedef double T; static constexpr bool kFastWeno = true;  static constexpr bool kP64 = false; static constexpr bool kRefRounding = false; static constexpr bool kWeno3 = false; static constexpr int id = 4; };
+// The reference's compile-time WENO3 build (-D_WENO3_, GPUonly.cuh:102,141)
+// of the two reference-rounding forms.
+struct PolRef32W3 { typedef float  T; static constexpr bool kFastWeno = false; static constexpr bool kP64 = false; static constexpr bool kRefRounding = true; static constexpr bool kWeno3 = true; static constexpr int id = 0; };
+struct PolFP64W3  { typedef double T; static constexpr bool kFastWeno = false; static constexpr bool kP64 = false; static constexpr bool kRefRounding = true; static constexpr bool kWeno3 = true; static constexpr int id = 3; };
 
 __device__ __forceinline__ float  dmin(float a, float b)   { return fminf(a, b); }
 __device__ __forceinline__ float  dmax(float a, float b)   { return fmaxf(a, b); }
@@ -446,14 +452,52 @@ __device__ __forceinline__ void hllc_face_packed(const FaceState<T>& S, const in
     o.Gm = S.Gm; o.Gp = S.Gp; o.Pm = S.Pm; o.Pp = S.Pp;
 }
 
+// Both edge values of one cell with the reference's WENO3 reconstruction
+// (the -D_WENO3_ build, GPUonly.cuh:124-137 for the plus side, 163-176 for
+// the minus side), from the cells y1, y2, y3 = l-1, l, l+1:
+//   R, the minus side of face l+1/2 (_weno_minus with b, c, d = y1, y2, y3):
+//     is0 = (c-b)^2, is1 = (d-c)^2, alpha0 = 1./(3.(is0+eps)^2),
+//     alpha1 = 2./(3.(is1+eps)^2), w0 = alpha0/(alpha0+alpha1), w1 = 1.-w0,
+//     R = w0 (1.5c - .5b) + w1 (.5c + .5d);
+//   L, the plus side of face l-1/2 (_weno_pluss with c, d, e = y1, y2, y3):
+//     is0 = (d-e)^2, is1 = (d-c)^2, alpha0 = (1./3.)/(is0+eps)^2,
+//     alpha1 = (2./3.)/(is1+eps)^2, w0 = alpha0/(alpha0+alpha1), w1 = 1.-w0,
+//     L = w0 (1.5d - .5e) + w1 (.5d + .5c);
+// both clipped to [min, max] of y1, y2, y3.  The double literals promote the
+// weights' arithmetic and the final combination to double, as in the
+// reference.  The squared differences are shared: (y2-y3)^2 is (y3-y2)^2
+// bit for bit (rounding to nearest is symmetric under negation).
+template <class Pol>
+__device__ __forceinline__ void weno3_cell_ref(const typename Pol::T y1, const typename Pol::T y2,
+        const typename Pol::T y3, typename Pol::T& R, typename Pol::T& L)
+{
+    typedef typename Pol::T T;
+    const T dl = y2 - y1, dr = y3 - y2;
+    const T sl = dl*dl, sr = dr*dr;
+    const double el = sl + MPCF_WENOEPS, er = sr + MPCF_WENOEPS;
+    const T am0 = (T)(1./(3.*el*el)), am1 = (T)(2./(3.*er*er));
+    const T wm0 = am0/(am0 + am1);
+    const T wm1 = (T)(1. - wm0);
+    const T rm = (T)(wm0*(1.5*y2 - .5*y1) + wm1*(.5*y2 + .5*y3));
+    const T ap0 = (T)((1./3.)/(er*er)), ap1 = (T)((2./3.)/(el*el));
+    const T wp0 = ap0/(ap0 + ap1);
+    const T wp1 = (T)(1. - wp0);
+    const T rp = (T)(wp0*(1.5*y2 - .5*y3) + wp1*(.5*y2 + .5*y1));
+    const T lo = dmin(dmin(y1, y2), y3);
+    const T hi = dmax(dmax(y1, y2), y3);
+    R = dmin(dmax(rm, lo), hi);
+    L = dmin(dmax(rp, lo), hi);
+}
+
 // Both edge values of one cell in the policy's arithmetic.
 template <class Pol>
 __device__ __forceinline__ void weno_cell(const typename Pol::T y0, const typename Pol::T y1,
         const typename Pol::T y2, const typename Pol::T y3, const typename Pol::T y4,
         typename Pol::T& R, typename Pol::T& L)
 {
-    if constexpr (Pol::kFastWeno) weno_cell_packed<typename Pol::T>(y0, y1, y2, y3, y4, R, L);
-    else                          weno_cell_ref<Pol>(y0, y1, y2, y3, y4, R, L);
+    if constexpr (Pol::kWeno3)         weno3_cell_ref<Pol>(y1, y2, y3, R, L);
+    else if constexpr (Pol::kFastWeno) weno_cell_packed<typename Pol::T>(y0, y1, y2, y3, y4, R, L);
+    else                               weno_cell_ref<Pol>(y0, y1, y2, y3, y4, R, L);
 }
 
 // Wave speeds and fluxes of one face in the policy's arithmetic.

@@ -124,6 +124,8 @@ SIGNATURES = {
     "mpcf_set_time": (_I, [_P, _I, _D]),
     "mpcf_get_time": (_I, [_P, _I, _PD]),
     "mpcf_set_tiling": (_I, [_P, _I, _I, _I]),
+    "mpcf_set_weno_order": (_I, [_P, _I]),
+    "mpcf_get_weno_order": (_I, [_P]),
     "mpcf_set_test_flags": (_I, [_P, _c.c_uint]),
     "mpcf_test_copy_count": (_I, [_P, _c.POINTER(_c.c_uint), _I]),
     "mpcf_get_tiling": (_I, [_P, _PI, _PI, _PI]),

@@ -267,6 +267,14 @@ class Solver:
         return t.value
 
     # -- launch configuration ----------------------------------------------
+    def set_weno_order(self, order):
+        """5 (WENO5) or 3 (the reference's compile-time WENO3 build; the
+        reference-rounding forms only)."""
+        check(lib().mpcf_set_weno_order(self._h, int(order)))
+
+    def weno_order(self):
+        return check(lib().mpcf_get_weno_order(self._h))
+
     def set_tiling(self, ty, dz, persistent=False, tma=True):
         flags = (_lib.TILE_PERSISTENT if persistent else 0) | (_lib.TILE_TMA if tma else 0)
         check(lib().mpcf_set_tiling(self._h, int(ty), int(dz), flags))

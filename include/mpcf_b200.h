@@ -365,6 +365,15 @@ int mpcf_get_time(mpcf_solver* s, int dom, double* t);
  * candidates on the solver's own state (which it leaves unchanged) and
  * keeps the fastest; best3 (optional) = {ty, dz, flags}, best_ms (optional)
  * = stage time. */
+/* Reconstruction order of the stage: 5 (WENO5, the default) or 3, the
+ * reference's compile-time WENO3 build (-D_WENO3_, GPUonly.cuh:102-137,
+ * 141-176: two-stencil weights (1/3, 2/3) on the squared neighbour
+ * differences, the same clipping).  WENO3 is provided for the two
+ * reference-rounding forms, MPCF_PREC_FP32_REF (bit-identical to the
+ * reference's WENO3 arithmetic) and MPCF_PREC_FP64; other forms are
+ * rejected with MPCF_ERR_ARG.  mpcf_get_weno_order returns 5 or 3. */
+int mpcf_set_weno_order(mpcf_solver* s, int order);
+int mpcf_get_weno_order(const mpcf_solver* s);
 int mpcf_set_tiling(mpcf_solver* s, int ty, int dz, int flags);
 int mpcf_get_tiling(const mpcf_solver* s, int* ty, int* dz, int* flags);
 int mpcf_autotune(mpcf_solver* s, int reps, int* best3, double* best_ms);
