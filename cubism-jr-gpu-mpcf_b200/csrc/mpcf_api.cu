@@ -307,6 +307,28 @@ int apply_tiling(mpcf_solver* s)
     return MPCF_OK;
 }
 
+// Allow the large shared-memory footprints of every tiling variant of the
+// solver's stage kernel (its precision form and reconstruction order).
+int grant_shared_memory(const mpcf_solver* s)
+{
+    const int tys[4] = {3, 7, 8, 15};
+    for (int i = 0; i < 4; ++i)
+    {
+        if (!valid_ty(s, tys[i])) continue;
+        for (int p = 0; p < 8; ++p)
+        {
+            StageKernelInfo I = stage_info(s, tys[i], (p & 1) != 0, (p & 2) != 0, (p & 4) != 0);
+            if (!I.fn) continue;
+            if (cudaFuncSetAttribute(I.fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)I.smem) != cudaSuccess)
+            {
+                cudaGetLastError();
+                return fail(MPCF_ERR_CUDA, "cannot grant %zu B shared memory to the stage kernel (ty=%d)", I.smem, tys[i]);
+            }
+        }
+    }
+    return MPCF_OK;
+}
+
 int persistent_grid(mpcf_solver* s, int ty)
 {
     StageKernelInfo I = stage_info(s, ty, true, false, s->tma != 0);
@@ -553,19 +575,7 @@ int mpcf_create(mpcf_solver** out, int ndomains, const int* dims, const int* bc,
     if (cudaMallocHost(&s->host_stage, 8 * (size_t)ndomains * 8) != cudaSuccess)
     { cudaGetLastError(); return bail(fail(MPCF_ERR_NOMEM, "cudaMallocHost failed")); }
 
-    // allow the large shared-memory footprints of every tiling variant
-    const int tys[4] = {3, 7, 8, 15};
-    for (int i = 0; i < 4; ++i)
-    {
-        if (!valid_ty(s, tys[i])) continue;
-        for (int p = 0; p < 8; ++p)
-        {
-            StageKernelInfo I = stage_info(s, tys[i], (p & 1) != 0, (p & 2) != 0, (p & 4) != 0);
-            if (!I.fn) continue;
-            if (cudaFuncSetAttribute(I.fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)I.smem) != cudaSuccess)
-            { cudaGetLastError(); return bail(fail(MPCF_ERR_CUDA, "cannot grant %zu B shared memory to the stage kernel (ty=%d)", I.smem, tys[i])); }
-        }
-    }
+    if ((rc = grant_shared_memory(s))) return bail(rc);
     s->ty = 7;
     s->dz = 64;
     s->persist = 0;
@@ -1556,7 +1566,10 @@ int mpcf_set_weno_order(mpcf_solver* s, int order)
         return fail(MPCF_ERR_ARG, "WENO3 is built for the reference-rounding forms (MPCF_PREC_FP32_REF, MPCF_PREC_FP64)");
     DeviceGuard g(s->device);
     CK(cudaStreamSynchronize(s->stream));
+    const bool was = s->weno3;
     s->weno3 = order == 3;
+    int rc = grant_shared_memory(s);
+    if (rc) { s->weno3 = was; return rc; }
     destroy_graphs(s);    // captured launches are of the other kernel
     return MPCF_OK;
 }

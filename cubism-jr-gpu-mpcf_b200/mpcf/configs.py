@@ -48,6 +48,14 @@ def config(name, seed=1234, placer=None):
         bub = [_bubbles(seed, 200, 0.02, 0.06)]
         return dict(name=name, dims=dims, bubbles=bub, params=ic_params(1000.0, seed), steps=20,
                     precision="mixed", desc="512^3, 200 bubbles R~U[0.02,0.06], liquid p=1000, 20 steps")
+    if name == "c3_slab128":
+        # the lower quarter of configuration 3's domain (512 x 512 x 128
+        # cells, its cloud and liquid): a few-GB case of the same kernel and
+        # tiling for hardware-counter captures
+        dims = [(512, 512, 128)]
+        bub = [_bubbles(seed, 200, 0.02, 0.06)]
+        return dict(name=name, dims=dims, bubbles=bub, params=ic_params(1000.0, seed), steps=20,
+                    precision="mixed", desc="512x512x128, the lower quarter of the 512^3 200-bubble cloud, liquid p=1000")
     if name == "c4_ensemble":
         rng = np.random.default_rng(seed)
         edges = (32, 48, 64, 96, 128)
