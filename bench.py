@@ -42,16 +42,17 @@ METRIC = "cell-stage updates/s on 1 B200: mixed vs plain FP64 at stated L1 error
 UNIT = "cell-stage updates/s"
 BYTES_PER_CELL_STAGE = {"fp32_ref": 112, "fp32": 112, "mixed": 112, "fp64": 224, "fp64_fast": 224}
 # DRAM bytes per cell-stage of the mixed stage kernel measured by ncu
-# (dram__bytes_read.sum + dram__bytes_write.sum = 8.98 + 7.48 GB for one
-# full-size launch over the 512^3 cloud, 134.2 M cells, 32 x 8 tiles over
-# whole columns, persistent, bulk-copy staging: a one-pass capture).  The
-# per-launch figure of the bench line is this times the workload's cells.
+# (dram__bytes_read.sum + dram__bytes_write.sum = 2.145 + 1.831 GB for one
+# launch over the 512 x 512 x 128 lower quarter of the 512^3 cloud, 33.55 M
+# cells, 32 x 8 tiles over whole columns, persistent, bulk-copy staging: a
+# few-GB case of the bench's kernel and tiling).  The per-launch figure of the
+# bench line is this times the workload's cells.
 # the arithmetic each precision form computes in, and its name in the workload
 DTYPE_OF = {"mixed": "f32+f64 (mixed)", "fp32": "f32", "fp32_ref": "f32 (reference rounding)", "fp64": "f64",
             "fp64_fast": "f64 (fast form)"}
 FORM_OF = {"mixed": "mixed form", "fp32": "fast FP32 form", "fp32_ref": "FP32 reference-rounding form",
            "fp64": "FP64 form", "fp64_fast": "fast FP64 form (factored algebra, refined reciprocals)"}
-MEASURED_DRAM_BYTES_PER_CELL_STAGE = {"mixed": 16.39e9 / 512 ** 3}
+MEASURED_DRAM_BYTES_PER_CELL_STAGE = {"mixed": (2.144534528e9 + 1.830834432e9) / (512 * 512 * 128)}
 
 
 # Algorithmic floating-point operations of one cell-stage, counted by
@@ -489,7 +490,8 @@ def main():
                          "frac": achieved / hbm,
                          "traffic": (MEASURED_DRAM_BYTES_PER_CELL_STAGE[args.precision] * ncell
                                      if args.precision in MEASURED_DRAM_BYTES_PER_CELL_STAGE else None),
-                         "traffic_note": "ncu DRAM bytes of one 512^3 launch (32x8 tiles, whole columns, persistent, TMA)",
+                         "traffic_note": "ncu DRAM bytes of one launch over the 512x512x128 lower quarter of the cloud "
+                                         "(32x8 tiles, whole columns, persistent, TMA), scaled by the cells of a launch",
                          "kernel": "stage_kernel<Pol%s>" % {"mixed": "Mixed", "fp32": "Fast32", "fp32_ref": "Ref32", "fp64": "FP64",
                                                              "fp64_fast": "Fast64"}[args.precision],
                          "ms_per_launch": st_ms,

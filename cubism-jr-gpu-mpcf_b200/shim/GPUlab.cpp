@@ -113,6 +113,10 @@ GPUlab::GPUlab(GridMPI& G, const uint_t nslices_, const int verbosity)
     const int dims[3] = {(int)sizeX, (int)sizeY, (int)sizeZ};
     const int dev = getenv("MPCF_DEVICE") ? atoi(getenv("MPCF_DEVICE")) : 0;
     GPU::check(mpcf_create(&m_solver, 1, dims, m_bc, precision_for_real(), dev), "GPUlab: mpcf_create");
+#ifdef _WENO3_
+    // the reference's compile-time WENO3 build (GPUonly.cuh:102,141)
+    GPU::check(mpcf_set_weno_order(m_solver, 3), "GPUlab: WENO3");
+#endif
     GPU::set_current_solver(m_solver);
     {
         std::lock_guard<std::mutex> lk(g_mu);
