@@ -8,6 +8,8 @@ It calls the reference's own code compiled from its sources (oracle/_ref):
   * source/GPU/GPUonly.cuh device math (WENO5 +/- with clipping, Einfeldt,
     Batten s*, HLLC rho/vel/pvel/e, extra-term velocity, stencil reads),
     and its WENO3 reconstruction (the -D_WENO3_ build),
+  * source/GPU/GPUkernels.cu stage kernels (flux assembly, extra terms,
+    divergence, update), run on the host in the WENO5 and WENO3 builds,
   * source/BoundaryConditions.h absorbing/reflecting ghost fills,
   * source/MaxSpeedOfSound.cpp (MaxSpeedOfSound_CPP::compute),
   * source/Sim/Sim_SICCloudMPI.cpp (the shock-induced cloud-collapse IC,
@@ -112,6 +114,36 @@ def make_devmath_w3(rng):
     wp = np.array([L.ref_weno_pluss_clipped(*map(float, w[1:])) for w in W], np.float32)
     np.savez_compressed(os.path.join(HERE, "ref_devmath_w3.npz"), weno_in=W, weno_minus_clipped=wm,
                         weno_pluss_clipped=wp)
+
+
+STAGE_CASES = (   # (reconstruction order, boundary conditions, stages (a, b, dt/h))
+    (5, (0, 0, 0, 0, 0, 0), ((0.0, 0.25, 0.05),)),
+    (5, (0, 1, 1, 0, 0, 1), ((0.0, 0.25, 0.04), (-17.0 / 32, 8.0 / 9, 0.04), (-32.0 / 27, 0.75, 0.04))),
+    (5, (1, 1, 1, 1, 1, 1), ((-17.0 / 32, 8.0 / 9, 0.06),)),
+    (3, (1, 0, 0, 1, 1, 0), ((0.0, 0.25, 0.05), (-17.0 / 32, 8.0 / 9, 0.05), (-32.0 / 27, 0.75, 0.05))),
+)
+
+
+def make_stage():
+    """The reference's own stage kernels (GPUkernels.cu:35-1179, run on the
+    host by oracle/ref_kernels.cpp) on seeded states: the SHA-256 of the
+    state and register after the stages, and the first cells of rho."""
+    rec = {}
+    for i, (order, bc, stages) in enumerate(STAGE_CASES):
+        L = O.ref_kernels(order)
+        dims = O.ref_kernels_dims(L)
+        U, R = O.stage_input(dims, 40 + i)
+        gxyz = None
+        for a, b, dtinvh in stages:
+            gxyz = O.fill_ghosts(dims, bc, U)
+            O.ref_kernels_stage(L, U, R, gxyz, a, b, dtinvh)
+        rec[f"order{i}"] = np.array(order)
+        rec[f"bc{i}"] = np.array(bc)
+        rec[f"stages{i}"] = np.array(stages, np.float64)
+        rec[f"dims{i}"] = np.array(dims)
+        rec[f"digest{i}"] = np.array(O.state_digest(U, R))
+        rec[f"rho{i}"] = U[0][:64].copy()
+    np.savez_compressed(os.path.join(HERE, "ref_stage.npz"), **rec)
 
 
 def cloud(dims, seed):
@@ -254,6 +286,7 @@ def main():
     make_dump()
     make_cases()
     make_devmath_w3(np.random.default_rng(20261205))
+    make_stage()
     print("wrote", sorted(f for f in os.listdir(HERE) if f.endswith(".npz")))
 
 

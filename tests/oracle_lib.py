@@ -457,3 +457,50 @@ class weno3:
     def __exit__(self, *exc):
         oracle().oracle_set_weno3(0)
         return False
+
+
+def ref_kernels(order=5):
+    """oracle/_ref/libref_kernels[_w3]_20x16x12.so: the reference's own stage
+    kernels run on the host (WENO5 or the -D_WENO3_ build), or None."""
+    L = ref_lib("libref_kernels_20x16x12" if order == 5 else "libref_kernels_w3_20x16x12")
+    if L is not None:
+        L.ref_kernels_dims.argtypes = [_PI]
+        L.ref_kernels_stage.argtypes = [_PPF, _PPF, _PF, _PF, _PF, _F, _F, _F]
+    return L
+
+
+def ref_kernels_dims(L):
+    d = (_I * 3)()
+    L.ref_kernels_dims(d)
+    return d[0], d[1], d[2]
+
+
+def ref_kernels_stage(L, U, R, ghosts, a, b, dtinvh):
+    """One stage of the reference's kernels, in place on U and R (FP32)."""
+    gx, gy, gz = ghosts
+    L.ref_kernels_stage(fptrs(U), fptrs(R), gx.ctypes.data_as(_PF), gy.ctypes.data_as(_PF), gz.ctypes.data_as(_PF),
+                        float(np.float32(a)), float(np.float32(b)), float(np.float32(dtinvh)))
+
+
+def stage_input(dims, seed):
+    """The state (the oracle's cloud set-up with its seeded placement: two
+    bubbles) and a seeded register of a stage case of the reference-kernel
+    checks."""
+    from mpcf import configs
+    params = configs.ic_params(100.0, seed)
+    ext = configs.extents(dims)
+    edge = min(ext)
+    bub = bubbles(seed, 2, 0.08 * edge, 0.2 * edge, tuple(0.2 * e for e in ext), tuple(0.8 * e for e in ext))
+    U = ic_cloud(dims, params, bub, np.float32)
+    rng = np.random.default_rng(seed)
+    R = [rng.normal(0, 1e-2, U[0].size).astype(np.float32) for _ in range(7)]
+    return U, R
+
+
+def state_digest(U, R):
+    """SHA-256 of the FP32 bytes of the 7 state and 7 register fields."""
+    import hashlib
+    h = hashlib.sha256()
+    for a in list(U) + list(R):
+        h.update(np.ascontiguousarray(a, np.float32).tobytes())
+    return h.hexdigest()

@@ -62,6 +62,29 @@ def test_golden_weno3():
     assert eq(L.oracle_weno_minus_clipped_f32(*map(float, w[:5])), g5["weno_minus_clipped"][1])
 
 
+def test_golden_reference_stage_kernels():
+    """The oracle's stage (flux assembly, extra terms, divergence, update)
+    against the reference's own stage kernels (GPUkernels.cu:35-1179, run on
+    the host by oracle/ref_kernels.cpp, WENO5 and WENO3 builds): the SHA-256
+    of state and register after the recorded stages."""
+    g = np.load(os.path.join(GOLD, "ref_stage.npz"))
+    n = len([k for k in g.files if k.startswith("digest")])
+    assert n == 4
+    for i in range(n):
+        dims = tuple(int(v) for v in g[f"dims{i}"])
+        bc = tuple(int(v) for v in g[f"bc{i}"])
+        U, R = O.stage_input(dims, 40 + i)
+        if int(g[f"order{i}"]) == 3:
+            O.oracle().oracle_set_weno3(1)
+        try:
+            for a, b, dtinvh in g[f"stages{i}"]:
+                O.stage(dims, bc, U, R, float(a), float(b), float(dtinvh))
+        finally:
+            O.oracle().oracle_set_weno3(0)
+        assert eq(U[0][:64], g[f"rho{i}"]), i
+        assert O.state_digest(U, R) == str(g[f"digest{i}"]), i
+
+
 def test_golden_wave_speeds_and_hllc():
     g = np.load(os.path.join(GOLD, "ref_devmath.npz"))
     L = O.oracle()
@@ -135,6 +158,30 @@ def test_live_weno3_random():
             w = (rng.normal(0, 1, 6) * 10 ** rng.uniform(-5, 4)).astype(np.float32)
             assert eq(L.oracle_weno_minus_clipped_f32(*map(float, w[:5])), L3.ref_weno_minus_clipped(*map(float, w[:5])))
             assert eq(L.oracle_weno_pluss_clipped_f32(*map(float, w[1:])), L3.ref_weno_pluss_clipped(*map(float, w[1:])))
+
+
+@pytest.mark.parametrize("order", [5, 3])
+def test_live_reference_stage_kernels(order):
+    """The oracle's stage against the reference's own stage kernels run on
+    the host, bit for bit: every boundary mix, the three LSRK3 stages."""
+    L = O.ref_kernels(order)
+    if L is None:
+        pytest.skip("oracle/_ref not built (the reference tree is absent)")
+    dims = O.ref_kernels_dims(L)
+    for k, bc in enumerate([(0,) * 6, (1,) * 6, (0, 1, 1, 0, 0, 1), (1, 0, 1, 0, 0, 1)]):
+        U, R = O.stage_input(dims, 60 + k)
+        Uo, Ro = [a.copy() for a in U], [a.copy() for a in R]
+        for a, b in ((0.0, 0.25), (-17.0 / 32, 8.0 / 9), (-32.0 / 27, 0.75)):
+            O.ref_kernels_stage(L, U, R, O.fill_ghosts(dims, bc, U), a, b, 0.05)
+            if order == 3:
+                O.oracle().oracle_set_weno3(1)
+            try:
+                O.stage(dims, bc, Uo, Ro, a, b, 0.05)
+            finally:
+                O.oracle().oracle_set_weno3(0)
+            for q in range(7):
+                assert eq(U[q], Uo[q]), (bc, a, "state", q)
+                assert eq(R[q], Ro[q]), (bc, a, "register", q)
 
 
 def test_live_stencil_reads(refdev):
