@@ -229,7 +229,7 @@ def stage_kernel_ms(mpcf, s, reps=6):
 # its first domain (its whole first domain when that is thinner), with the
 # domain's cell spacing, bubbles and material data; one LSRK3 step of it per
 # timed step.
-CPU_SAMPLE_PLANES = int(os.environ.get("MPCF_CPU_SAMPLE_PLANES", "64"))
+CPU_SAMPLE_PLANES = int(os.environ.get("MPCF_CPU_SAMPLE_PLANES", "32"))
 
 
 def cpu_sample_block(cfg):
