@@ -154,9 +154,6 @@ int stage_block_threads(int ty) { return ((ty + 1) & ty) == 0 ? 32 * (ty + 1) : 
 bool valid_ty(const mpcf_solver* s, int ty)
 {
     if (ty == 3 || ty == 7 || ty == 8) return true;
-#ifdef MPCF_FAST_TY15
-    if (ty == 15 && s->pol == 2) return true;
-#endif
     return ty == 15 && s->pol == 0;
 }
 

@@ -7,20 +7,14 @@
 
 namespace mpcf {
 
-#ifdef MPCF_FAST_TY15
-constexpr bool kMixedTY15 = true;
-#else
-constexpr bool kMixedTY15 = false;
-#endif
-
 cudaError_t launch_stage_mixed(int ty, bool persist, bool tma, const StageArgs& A, int grid, cudaStream_t st)
 {
-    return StageDispatch<PolMixed, kMixedTY15>::launch(ty, persist, tma, A, grid, st);
+    return StageDispatch<PolMixed, false>::launch(ty, persist, tma, A, grid, st);
 }
 
 StageKernelInfo stage_info_mixed(int ty, bool persist, bool sums, bool tma)
 {
-    return StageDispatch<PolMixed, kMixedTY15>::info(ty, persist, sums, tma);
+    return StageDispatch<PolMixed, false>::info(ty, persist, sums, tma);
 }
 
 } // namespace mpcf
