@@ -692,6 +692,48 @@ int mpcf_stage(mpcf_solver* s, double a, double b, const double* dtinvh)
     return MPCF_OK;
 }
 
+int mpcf_stream(mpcf_solver* s, void** stream)
+{
+    if (!s || !stream) return fail(MPCF_ERR_ARG, "null argument");
+    *stream = (void*)s->stream;
+    return MPCF_OK;
+}
+
+int mpcf_sos_accumulator(mpcf_solver* s, void** dev_ptr)
+{
+    if (!s || !dev_ptr) return fail(MPCF_ERR_ARG, "null argument");
+    *dev_ptr = s->sos_bits;
+    return MPCF_OK;
+}
+
+int mpcf_enqueue_sos(mpcf_solver* s)
+{
+    Range nvtx("mpcf_enqueue_sos");
+    if (!s) return fail(MPCF_ERR_ARG, "null solver");
+    DeviceGuard g(s->device);
+    s->sos_fresh = false;
+    return enqueue_sos(s);
+}
+
+int mpcf_enqueue_dt(mpcf_solver* s, double cfl, double dt_max)
+{
+    Range nvtx("mpcf_enqueue_dt");
+    if (!s) return fail(MPCF_ERR_ARG, "null solver");
+    if (!(cfl > 0) || !(dt_max > 0)) return fail(MPCF_ERR_ARG, "cfl and dt_max must be positive");
+    DeviceGuard g(s->device);
+    s->sos_fresh = false;
+    return enqueue_dt(s, cfl, dt_max);
+}
+
+int mpcf_enqueue_stage(mpcf_solver* s, double a, double b)
+{
+    Range nvtx("mpcf_enqueue_stage");
+    if (!s) return fail(MPCF_ERR_ARG, "null solver");
+    DeviceGuard g(s->device);
+    s->sos_fresh = false;
+    return enqueue_stage(s, a, b, false);
+}
+
 int mpcf_compute_dt(mpcf_solver* s, double cfl, double dt_max, double* dt_out)
 {
     Range nvtx("mpcf_compute_dt");

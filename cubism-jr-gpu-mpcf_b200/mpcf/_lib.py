@@ -95,6 +95,11 @@ SIGNATURES = {
     "mpcf_run": (_I, [_P, _I, _D, _D, _I, _PD]),
     "mpcf_run_host": (_I, [_P, _I, _D, _D, _PP, _I, _PD]),
     "mpcf_synchronize": (_I, [_P]),
+    "mpcf_stream": (_I, [_P, _PP]),
+    "mpcf_sos_accumulator": (_I, [_P, _PP]),
+    "mpcf_enqueue_sos": (_I, [_P]),
+    "mpcf_enqueue_dt": (_I, [_P, _D, _D]),
+    "mpcf_enqueue_stage": (_I, [_P, _D, _D]),
     "mpcf_update": (_I, [_P, _D]),
     "mpcf_conserved_sums": (_I, [_P, _PD]),
     "mpcf_conserved_sums_noalloc": (_I, [_PP, _c.c_longlong, _I, _PD, _I, _I, _P]),

@@ -262,7 +262,39 @@ class SlabRank:
         self.time += dt
         return dt
 
-    def run(self, nsteps, cfl=0.3, dt_max=1e30):
+    def enqueue_step(self, cfl=0.3, dt_max=1e30):
+        """One LSRK3 step ordered on the solver's stream, with no host round
+        trip: the sound speed into the solver's device accumulator, an
+        all-reduce MAX of it over the ranks, the device dt, and per stage the
+        exchange of the ghost planes (NCCL point-to-point copies that start
+        after the stage that wrote the planes; the next stage waits for them
+        on the stream, not on the host) and the stage.  Bit-identical to
+        step(), which synchronises four times per step.  A state without a
+        real sound speed is flagged in the error word of the rank that holds
+        it (the device dt kernel's check)."""
+        import torch
+        dev = torch.device("cuda", self.device)
+        stream = torch.cuda.ExternalStream(self.solver.stream_handle(), device=dev)
+        with torch.cuda.stream(stream):
+            self.solver.enqueue_sos()
+            acc = torch.as_tensor(_DeviceBlock(self.solver.sos_accumulator(), 1, self._typestr), device=dev)
+            self.dist.all_reduce(acc, op=self.dist.ReduceOp.MAX, group=self.group)
+            self.solver.enqueue_dt(cfl, dt_max)
+            for a, b in LSRK3:
+                if self.nranks > 1:
+                    exchange_planes(self.dist, self.rank, self.nranks, *self.plane_blocks(), group=self.group)
+                self.solver.enqueue_stage(a, b)
+
+    def run(self, nsteps, cfl=0.3, dt_max=1e30, ordered=False):
+        """nsteps steps; ordered: every step stream-ordered (enqueue_step),
+        with one synchronisation at the end.  Returns the time."""
+        if not ordered:
+            for _ in range(int(nsteps)):
+                self.step(cfl, dt_max)
+            return self.time
+        t0 = self.solver.get_time()
         for _ in range(int(nsteps)):
-            self.step(cfl, dt_max)
+            self.enqueue_step(cfl, dt_max)
+        self.solver.synchronize()
+        self.time += self.solver.get_time() - t0
         return self.time

@@ -145,6 +145,28 @@ class Solver:
                                   int(nchunks), ctypes.byref(t)))
         return t.value
 
+    # -- stream-ordered building blocks (nothing synchronises) -------------
+    def stream_handle(self):
+        """The solver's cudaStream_t as an integer (mpcf_stream)."""
+        p = ctypes.c_void_p()
+        check(lib().mpcf_stream(self._h, ctypes.byref(p)))
+        return p.value or 0
+
+    def sos_accumulator(self):
+        """Device address of the per-domain sound-speed accumulator."""
+        p = ctypes.c_void_p()
+        check(lib().mpcf_sos_accumulator(self._h, ctypes.byref(p)))
+        return p.value
+
+    def enqueue_sos(self):
+        check(lib().mpcf_enqueue_sos(self._h))
+
+    def enqueue_dt(self, cfl=0.3, dt_max=1e30):
+        check(lib().mpcf_enqueue_dt(self._h, float(cfl), float(dt_max)))
+
+    def enqueue_stage(self, a, b):
+        check(lib().mpcf_enqueue_stage(self._h, float(a), float(b)))
+
     def synchronize(self):
         check(lib().mpcf_synchronize(self._h))
 

@@ -152,6 +152,30 @@ int mpcf_run(mpcf_solver* s, int nsteps, double cfl, double dt_max, int use_grap
 int mpcf_run_host(mpcf_solver* s, int nsteps, double cfl, double dt_max, void* const* host7, int nchunks,
                   double* time_out);
 int mpcf_synchronize(mpcf_solver* s);
+/* Stream-ordered building blocks of a step, for a driver that orders its
+ * own work with the solver's kernels: the reference's per-rank step with
+ * its MPI MIN of dt (LSRK3_IntegratorMPI.cpp:27-62, :40) and its halo
+ * exchange before every stage (GPUlab::load_ghosts, GPUlab.cpp:622-644),
+ * run without host round trips (an NCCL all-reduce and point-to-point
+ * copies on the solver's stream between these calls).  None of them
+ * synchronises.
+ * mpcf_stream: the solver's cudaStream_t (every kernel of the solver runs
+ *   on it).
+ * mpcf_sos_accumulator: device address of the per-domain sound-speed
+ *   accumulator, ndom values of the state's type (float, or double for the
+ *   FP64 forms); it holds non-negative values, so a caller may reduce it
+ *   further in place (an all-reduce MAX over ranks) before mpcf_enqueue_dt.
+ * mpcf_enqueue_sos: the maximum sound speed of every domain's current state
+ *   into the accumulator (cleared first).
+ * mpcf_enqueue_dt: dt = min(cfl h/sos, dt_max) and dt/h per domain on the
+ *   device from the accumulator, which it clears.
+ * mpcf_enqueue_stage: one stage with the device dt/h: mpcf_stage without
+ *   its final synchronisation. */
+int mpcf_stream(mpcf_solver* s, void** stream);
+int mpcf_sos_accumulator(mpcf_solver* s, void** dev_ptr);
+int mpcf_enqueue_sos(mpcf_solver* s);
+int mpcf_enqueue_dt(mpcf_solver* s, double cfl, double dt_max);
+int mpcf_enqueue_stage(mpcf_solver* s, double a, double b);
 /* The state update alone, U <- U + b*R (Update_CUDA::compute ->
  * GPU::update -> _update, Update_CUDA.cpp:12-17, GPUkernels.cu:1142-1179),
  * for callers that split a stage into Convection_CUDA (mpcf_stage with

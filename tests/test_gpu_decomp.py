@@ -158,6 +158,40 @@ def test_single_rank_driver_matches_step(mpcf):
 
 
 @pytest.mark.parametrize("prec", ["fp32_ref", "fp64"])
+def test_single_rank_driver_stream_ordered_matches_step(mpcf, prec):
+    """The stream-ordered rank driver (sound speed, its NCCL all-reduce, the
+    device dt and the stages all on the solver's stream, no host round trip)
+    reproduces mpcf_step bit for bit, the time included."""
+    import datetime
+    import os
+    import socket
+    import torch.distributed as dist
+    sk = socket.socket()
+    sk.bind(("127.0.0.1", 0))
+    port = sk.getsockname()[1]
+    sk.close()
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("nccl", rank=0, world_size=1, timeout=datetime.timedelta(seconds=60))
+    try:
+        U0 = _state(prec, mpcf)
+        with dc.SlabRank(DIMS, bc=BC, precision=prec, dist=dist) as r:
+            r.set_global_state(U0)
+            t = r.run(3, 0.3, ordered=True)
+            U, R = r.get_state()
+            assert r.solver.error_word() == 0
+        with mpcf.Solver([DIMS], bc=[BC], precision=prec) as s:
+            s.set_state(U0)
+            t_ref = s.run(3, cfl=0.3, graph=False)[0]
+            U_ref, R_ref = s.get_state()
+        assert t == t_ref, (t, t_ref)
+        assert_bitwise(U, U_ref, "state")
+        assert_bitwise(R, R_ref, "register")
+    finally:
+        dist.destroy_process_group()
+
+
+@pytest.mark.parametrize("prec", ["fp32_ref", "fp64"])
 def test_slab_initial_conditions_match_undivided_domain(mpcf, prec):
     """Each slab carries its place in the global grid (mpcf_set_origin), so
     the device generators write the undivided domain's initial condition,
