@@ -75,6 +75,24 @@ def oracle():
     return _oracle
 
 
+def contracted():
+    """oracle/liboracle_contracted.so: the oracle's stage source built with
+    fused multiply-add contraction, or None when it is not built or this CPU
+    has no FMA instructions."""
+    p = os.path.join(ORACLE_DIR, "liboracle_contracted.so")
+    try:
+        with open("/proc/cpuinfo") as f:
+            has_fma = " fma " in f.read()
+    except OSError:
+        has_fma = False
+    if not (has_fma and os.path.exists(p)):
+        return None
+    L = _c.CDLL(p)
+    L.oracle_step_f32.restype = _D
+    L.oracle_step_f32.argtypes = [_I, _I, _I, _PI, _PPF, _PPF, _D, _D, _D, _PD]
+    return L
+
+
 def ref_lib(name):
     """Load oracle/_ref/<name>.so or return None when it was not built."""
     p = os.path.join(REF_DIR, name + ".so")

@@ -12,6 +12,8 @@
    energy are conserved between reflecting walls, and the two sound-speed
    formulas agree.
 4. The FP32 roofline constant of bench.py equals the operation counter.
+5. How far one changed rounding (contraction) moves the reference's FP32
+   step, against the FP64 step.
 """
 import ctypes
 import os
@@ -373,6 +375,49 @@ def test_fp32_weno_indicator_cancellation_documented():
         p = L.oracle_weno_pluss_clipped_f32(*map(float, w[::-1][1:]))
         worst = max(worst, abs(m - p) / abs(m))
     assert 1e-6 < worst < 1e-4
+
+
+def test_fp32_step_depends_on_contraction():
+    """The same FP32 step compiled with and without fused multiply-add
+    contraction, one step of the 64^3 single-bubble cloud (configuration 1).
+    The reference's own build keeps nvcc's default contraction
+    (makefiles/Makefile:59 passes no --fmad flag), so the rounding of its
+    FP32 results depends on the compiler's choices.  The momenta move by
+    1e-4..1e-3 of their maximum, as far as either rounding is from the FP64
+    step (the expanded indicators amplify one changed rounding); density,
+    energy, G and P agree within 2e-6.  A momentum bar of 1e-5 against the
+    reference's FP32 step is therefore met only by one fixed rounding
+    reproduced bit for bit: the oracle's, the literal C semantics."""
+    Lc = O.contracted()
+    if Lc is None:
+        pytest.skip("contracted oracle not built or no FMA on this CPU")
+    import mpcf
+    cfg = mpcf.configs.config("c1_64")
+    dims = cfg["dims"][0]
+    U0 = O.ic_cloud(dims, cfg["params"], cfg["bubbles"][0], np.float32)
+    h = 1.0 / max(dims)
+
+    def step(f, dtype):
+        U = [a.astype(dtype) for a in U0]
+        R = [np.zeros_like(a) for a in U]
+        sos = ctypes.c_double()
+        dt = f(*dims, O.bc_arr((0,) * 6), O.fptrs(U), O.fptrs(R), 0.3, 1e30, h, ctypes.byref(sos))
+        assert dt > 0
+        return U
+
+    Ua = step(O.oracle().oracle_step_f32, np.float32)
+    Ub = step(Lc.oracle_step_f32, np.float32)
+    U64 = step(O.oracle().oracle_step_f64, np.float64)
+
+    def rel(a, b):
+        return float(np.abs(a.astype(np.float64) - b).max() / np.abs(b).max())
+
+    for q in (1, 2, 3):
+        d, ea, eb = rel(Ub[q], Ua[q]), rel(Ua[q], U64[q]), rel(Ub[q], U64[q])
+        assert 1e-4 < d < 1e-3, (q, d)
+        assert 0.5 * ea < eb < 2.0 * ea, (q, ea, eb)
+    for q in (0, 4, 5, 6):
+        assert rel(Ub[q], Ua[q]) < 2e-6, (q, rel(Ub[q], Ua[q]))
 
 
 def test_fp64_conservation_between_reflecting_walls():
