@@ -536,9 +536,10 @@ def e2e_measure(mpcf, cfg, K, W, cfl, dist, precision="mixed", tiling=None, nchu
     """Same metric through the C ABI with the state in page-locked host
     memory, as the reference keeps it: every step reads its input state from
     the host buffers and writes its result back to them (mpcf_run_host: z-chunk
-    uploads, stage 3 chunk by chunk with each chunk downloaded as soon as it
-    is written, the next step's upload of a chunk after its download, copies
-    in both directions overlapping the kernels).  The register stays on the
+    uploads, the three stages as a wavefront over the chunks, each chunk
+    downloaded as soon as stage 3 has written it, the next step's upload of
+    a chunk after its download, copies in both directions overlapping the
+    kernels).  The register stays on the
     device (stage 1 multiplies it by a = 0), so the state is the step's whole
     input and result.  Host wall clock over the K timed steps.  Also the
     serial form: mpcf_set_state + mpcf_step + mpcf_get_state per step."""

@@ -858,6 +858,16 @@ int mpcf_run_host(mpcf_solver* s, int nsteps, double cfl, double dt_max, void* c
             CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
             v->push_back(e);
         }
+    // hi[c]: the last chunk within 3 planes above chunk c (a stage reads 3
+    // planes beyond its cells); a stage of chunk c may run once the stage
+    // before it (or the upload) has covered chunks 0..hi[c]
+    std::vector<int> hi(nch);
+    for (int c = 0; c < nch; ++c)
+    {
+        int j = c;
+        while (j + 1 < nch && zc[j + 1] < zc[c + 1] + 3) ++j;
+        hi[c] = j;
+    }
     // the first upload overwrites the state only after the work already
     // queued on the solver's stream
     CK(cudaEventRecord(s->ev_start, s->stream));
@@ -865,9 +875,10 @@ int mpcf_run_host(mpcf_solver* s, int nsteps, double cfl, double dt_max, void* c
     int rc;
     for (int n = 0; n < nsteps; ++n)
     {
+        const int p = s->parity;
         // (1) the step's input: chunk c of the host state into the state
         // buffer, once the previous step's result of chunk c is on the host
-        char* dev = (char*)D.U[s->parity];
+        char* dev = (char*)D.U[p];
         for (int c = 0; c < nch; ++c)
         {
             if (n > 0) CK(cudaStreamWaitEvent(s->up, s->ev_down[c], 0));
@@ -877,39 +888,56 @@ int mpcf_run_host(mpcf_solver* s, int nsteps, double cfl, double dt_max, void* c
                                    cudaMemcpyHostToDevice, s->up));
             CK(cudaEventRecord(s->ev_up[c], s->up));
         }
-        // (2) its maximum sound speed, chunk by chunk as the chunks land
-        CK(cudaMemsetAsync(s->sos_bits, 0, esz, s->stream));
-        int done = 0;
-        for (int c = 0; c < nch; ++c)
+        // (2) the maximum sound speed of the input.  First step: reduced
+        // chunk by chunk as the chunks land.  Later steps: the input is the
+        // previous step's result, whose sound speed stage 3 accumulated as
+        // it wrote it (as in a resident run), so dt needs no whole upload.
+        if (n == 0)
         {
-            CK(cudaStreamWaitEvent(s->stream, s->ev_up[c], 0));
-            const int upto = c == nch - 1 ? s->nchunks : (int)((long long)zc[c + 1] * plane / s->sos_chunk);
-            if (upto <= done) continue;
-            SosArgs A;
-            A.doms = s->ddoms;
-            A.ndom = 1;
-            A.nchunks = upto - done;
-            A.chunk = s->sos_chunk;
-            A.chunk0 = done;
-            A.parity = s->parity;
-            A.sos_bits = s->sos_bits;
-            CK(launch_sos(s->pol, A, s->stream));
-            done = upto;
+            CK(cudaMemsetAsync(s->sos_bits, 0, esz, s->stream));
+            int done = 0;
+            for (int c = 0; c < nch; ++c)
+            {
+                CK(cudaStreamWaitEvent(s->stream, s->ev_up[c], 0));
+                const int upto = c == nch - 1 ? s->nchunks : (int)((long long)zc[c + 1] * plane / s->sos_chunk);
+                if (upto <= done) continue;
+                SosArgs A;
+                A.doms = s->ddoms;
+                A.ndom = 1;
+                A.nchunks = upto - done;
+                A.chunk = s->sos_chunk;
+                A.chunk0 = done;
+                A.parity = p;
+                A.sos_bits = s->sos_bits;
+                CK(launch_sos(s->pol, A, s->stream));
+                done = upto;
+            }
         }
-        // (3) dt, stages 1 and 2 over the whole domain
         if ((rc = enqueue_dt(s, cfl, dt_max))) return rc;
-        for (int k = 0; k < 2; ++k)
-            if ((rc = enqueue_stage(s, kLSRK3[k][0], kLSRK3[k][1], false))) return rc;
-        // (4) stage 3 chunk by chunk; each chunk of the new state goes to the
-        // host as soon as it is written
-        for (int c = 0; c < nch; ++c)
+        // (3) the three stages as a wavefront over the chunks: stage k of
+        // chunk c follows stage k-1 (stage 1: the upload) of chunks
+        // 0..hi[c].  Stage k reads buffer p ^ (k & 1) and writes the other;
+        // a chunk's stage overwrites planes that only the previous stage of
+        // chunks up to hi[c] read, so these read-after-write orders also
+        // cover the buffers' reuse.  Stage 3 accumulates the sound speed of
+        // the state it writes (the next step's dt) and hands each chunk to
+        // the download stream.
+        int d[3] = {0, 0, 0};
+        while (d[2] < nch)
         {
-            if ((rc = enqueue_stage_tiles(s, kLSRK3[2][0], kLSRK3[2][1], false, false, lc[c] * txy, lc[c + 1] * txy)))
-                return rc;
-            CK(cudaEventRecord(s->ev_st[c], s->stream));
+            int k = 0;
+            if (d[1] > hi[d[2]]) k = 2;
+            else if (d[1] < nch && d[0] > hi[d[1]]) k = 1;
+            const int c = d[k]++;
+            if (k == 0) CK(cudaStreamWaitEvent(s->stream, s->ev_up[hi[c]], 0));
+            s->parity = p ^ (k & 1);
+            rc = enqueue_stage_tiles(s, kLSRK3[k][0], kLSRK3[k][1], false, k == 2, lc[c] * txy, lc[c + 1] * txy);
+            s->parity = p;
+            if (rc) return rc;
+            if (k == 2) CK(cudaEventRecord(s->ev_st[c], s->stream));
         }
-        s->parity ^= 1;
-        const char* res = (const char*)D.U[s->parity];
+        s->parity = p ^ 1;
+        const char* res = (const char*)D.U[p ^ 1];
         for (int c = 0; c < nch; ++c)
         {
             CK(cudaStreamWaitEvent(s->down, s->ev_st[c], 0));
@@ -920,9 +948,9 @@ int mpcf_run_host(mpcf_solver* s, int nsteps, double cfl, double dt_max, void* c
             CK(cudaEventRecord(s->ev_down[c], s->down));
         }
     }
-    // the device state equals the host result; the sound-speed accumulator
-    // was cleared by the last dt and holds nothing
-    s->sos_fresh = false;
+    // the device state equals the host result, and the sound-speed
+    // accumulator holds its maximum (from the last stage 3)
+    if (nsteps > 0) s->sos_fresh = true;
     s->sums_valid = false;
     CK(cudaStreamSynchronize(s->down));
     CK(cudaStreamSynchronize(s->up));

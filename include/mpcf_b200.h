@@ -140,15 +140,20 @@ int mpcf_run(mpcf_solver* s, int nsteps, double cfl, double dt_max, int use_grap
  * (x fastest), read as every step's input and overwritten with every step's
  * result; page-locked memory lets the copies overlap the kernels.  Every
  * step uploads the state in z-chunks of whole tile layers on one copy
- * stream, reduces each chunk's sound speed as it lands, computes dt and
- * stages 1-2, then runs stage 3 chunk by chunk and downloads each chunk of
- * the new state on a second copy stream as soon as it is written; the next
- * step's upload of a chunk follows its download (copies in both directions
- * overlap).  nchunks: requested chunks (at most the tile layers, nz/dz; one
- * layer per chunk with the tiling's dz).  The register stays on the device
- * (stage 1 multiplies it by a = 0).  Results are bit-identical to mpcf_run
- * on the same state.  Single-domain solvers without halo faces;
- * conservation tracking is not applied.  time_out (optional): the time. */
+ * stream and runs the three stages as a wavefront over the chunks: a stage
+ * of a chunk runs once the stage before it (stage 1: the upload) has
+ * covered every chunk within 3 planes above, and each chunk of the new
+ * state goes back on a second copy stream as soon as stage 3 has written
+ * it; the next step's upload of a chunk follows its download (copies in
+ * both directions overlap each other and the kernels).  The first step's dt
+ * comes from the sound speed reduced chunk by chunk as the chunks land;
+ * later steps take the sound speed that stage 3 accumulated over the state
+ * it wrote (the values the host receives and sends back), as mpcf_run does.
+ * nchunks: requested chunks (at most the tile layers, nz/dz; one layer per
+ * chunk with the tiling's dz).  The register stays on the device (stage 1
+ * multiplies it by a = 0).  Results are bit-identical to mpcf_run on the
+ * same state.  Single-domain solvers without halo faces; conservation
+ * tracking is not applied.  time_out (optional): the time. */
 int mpcf_run_host(mpcf_solver* s, int nsteps, double cfl, double dt_max, void* const* host7, int nchunks,
                   double* time_out);
 int mpcf_synchronize(mpcf_solver* s);

@@ -1,11 +1,15 @@
 """Runs over a host-resident state (mpcf_run_host): the reference's
 host-resident block streamed through the GPU (GPUlab.cpp:202-372,703-793).
 
-Every step uploads the state from host memory in z-chunks, reduces the sound
-speed chunk by chunk, runs stages 1-2, then stage 3 chunk by chunk with each
-chunk downloaded as soon as it is written; the next step's upload of a chunk
-follows its download.  The result must be bit-identical to the same steps of
-a device-resident run (mpcf_run), for any chunking."""
+Every step uploads the state from host memory in z-chunks and runs the three
+stages as a wavefront over the chunks: a stage of a chunk follows the stage
+before it (stage 1: the upload) on every chunk within 3 planes above, and each
+chunk of the new state is downloaded as soon as stage 3 has written it; the
+next step's upload of a chunk follows its download.  The first step reduces
+the sound speed chunk by chunk as the chunks land, later steps take the one
+stage 3 accumulated.  The result must be bit-identical to the same steps of a
+device-resident run (mpcf_run), for any chunking, chunks thinner than the
+3-plane stencil reach included."""
 import numpy as np
 import pytest
 
@@ -29,6 +33,8 @@ def resident(mpcf, dims, prec, U0, tiling, steps):
     ("mixed", (8, 32, False, True), 2),
     ("fp64", (3, 16, False, False), 3),
     ("fp32", (8, 96, True, True), 4),          # one layer: a single chunk
+    ("mixed", (8, 2, True, True), 48),         # 2-plane chunks: a stage waits for 2 above
+    ("fp32_ref", (3, 1, True, True), 32),      # 3-plane chunks of 1-plane layers
 ])
 def test_streamed_run_equals_resident_run(mpcf, prec, tiling, nchunks):
     dims = (64, 48, 96)
