@@ -454,6 +454,12 @@ def main():
     if not args.no_e2e:
         e2e = e2e_measure(mpcf, cfg, K=K, W=W, cfl=cfl, dist=dist, precision=args.precision, tiling=tiling,
                           nchunks=args.e2e_chunks)
+    # the same for the drop-in form (FP32 reference rounding, bit-identical
+    # to the reference's arithmetic), on its own tiling
+    e2e_drop_in = None
+    if not args.no_e2e and args.precision != "fp32_ref" and "fp32_ref" in others:
+        e2e_drop_in = e2e_measure(mpcf, cfg, K=K, W=W, cfl=cfl, dist=dist, precision="fp32_ref",
+                                  tiling=others["fp32_ref"]["tiling"], nchunks=args.e2e_chunks, serial_form=False)
 
     # ---------------- CPU baseline (rank 0, N=1 only): the oracle on the
     # workload's CPU sample, its state from the oracle's cloud set-up
@@ -507,6 +513,7 @@ def main():
             "device_error_word": err_word,
             "clocks": clk,
             "e2e": e2e,
+            "e2e_drop_in": e2e_drop_in,
             "cpu_baseline": cpu,
         }
         print(json.dumps(line), flush=True)
@@ -532,7 +539,51 @@ def pick_tiling(mpcf, s):
     return best
 
 
-def e2e_measure(mpcf, cfg, K, W, cfl, dist, precision="mixed", tiling=None, nchunks=16):
+def pcie_peak(nbytes=1 << 30, chunks=16, reps=5):
+    """Measured host-device copy rates (GB/s, 1e9 B): page-locked host
+    buffer to device, device to host, and both directions at once on two
+    streams (the rate each direction keeps while the other runs), in
+    `chunks` copies of nbytes/chunks each way per repetition."""
+    import torch
+    n = nbytes // 4
+    cs = n // chunks
+    host_a = torch.empty(n, dtype=torch.float32, pin_memory=True)
+    host_b = torch.empty(n, dtype=torch.float32, pin_memory=True)
+    dev_a = torch.empty(n, dtype=torch.float32, device="cuda")
+    dev_b = torch.empty(n, dtype=torch.float32, device="cuda")
+    host_a.fill_(1.0)
+    dev_b.fill_(1.0)
+    up, down = torch.cuda.Stream(), torch.cuda.Stream()
+
+    def h2d():
+        with torch.cuda.stream(up):
+            for c in range(chunks):
+                dev_a[c * cs:(c + 1) * cs].copy_(host_a[c * cs:(c + 1) * cs], non_blocking=True)
+
+    def d2h():
+        with torch.cuda.stream(down):
+            for c in range(chunks):
+                host_b[c * cs:(c + 1) * cs].copy_(dev_b[c * cs:(c + 1) * cs], non_blocking=True)
+
+    def rate(*fns):
+        for f in fns:
+            f()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for _ in range(reps):
+            for f in fns:
+                f()
+        torch.cuda.synchronize()
+        return reps * cs * chunks * 4 / (time.perf_counter() - t0) / 1e9
+
+    out = {"h2d_gbs": rate(h2d), "d2h_gbs": rate(d2h), "both_gbs_per_direction": rate(h2d, d2h),
+           "sample": f"{chunks} copies of {cs * 4 >> 20} MiB each way, {reps} repetitions"}
+    del host_a, host_b, dev_a, dev_b
+    torch.cuda.empty_cache()
+    return out
+
+
+def e2e_measure(mpcf, cfg, K, W, cfl, dist, precision="mixed", tiling=None, nchunks=16, serial_form=True):
     """Same metric through the C ABI with the state in page-locked host
     memory, as the reference keeps it: every step reads its input state from
     the host buffers and writes its result back to them (mpcf_run_host: z-chunk
@@ -582,6 +633,15 @@ def e2e_measure(mpcf, cfg, K, W, cfl, dist, precision="mixed", tiling=None, nchu
         out["value"], _ = rp.throughput(dist, ncell, 3.0 * K, sec * 1e3, device="cuda" if dist is not None else None)
         out["path"] = (f"mpcf_run_host: state in pinned host memory read and written every step, {nchunks} z-chunks, "
                        f"tiling {list(s.tiling())}, host wall clock over {K} steps")
+        # the bound of a streamed step: its bytes each way at the measured
+        # rate of concurrent host-to-device and device-to-host copies
+        pk = pcie_peak()
+        bound_ms = out["h2d_bytes_per_step"] / (pk["both_gbs_per_direction"] * 1e9) * 1e3
+        step_ms = sec * 1e3 / K
+        out["roofline"] = {"bound": "pcie", "achieved": out["h2d_bytes_per_step"] / step_ms / 1e6,
+                           "peak": pk["both_gbs_per_direction"], "unit": "GB/s per direction",
+                           "frac": bound_ms / step_ms, "bound_ms_per_step": bound_ms, "ms_per_step": step_ms,
+                           "copies": pk}
 
     def serial(k):
         for _ in range(k):
@@ -591,6 +651,9 @@ def e2e_measure(mpcf, cfg, K, W, cfl, dist, precision="mixed", tiling=None, nchu
             for d, (_, up) in enumerate(bufs):
                 mpcf._lib.check(L.mpcf_get_state(s._h, d, up, None, 0))
 
+    if streamed and not serial_form:
+        s.close()
+        return out
     ks = max(2, min(K, 4))
     serial(1)
     sec = timed(serial, ks)
