@@ -1,7 +1,8 @@
 """Full-size GPU checks (the benchmark configurations' sizes) through
 size-independent properties: invariance of a uniform state, axis
 permutations, conservation between reflecting walls, graph replay against
-plain steps, ensembles against separate solvers.  Parity against the CPU
+plain steps, ensembles against separate solvers, the host-resident streamed
+run (the e2e path) against the device-resident run.  Parity against the CPU
 oracle at these sizes and tilings is in test_gpu_parity_bench.py."""
 import numpy as np
 import pytest
@@ -139,3 +140,33 @@ def test_graph_replay_equals_plain_steps_512cube(mpcf):
             out.append((t, st[0][::997].copy(), st[4][::997].copy()))
     assert out[0][0] == out[1][0]
     assert np.array_equal(out[0][1], out[1][1]) and np.array_equal(out[0][2], out[1][2])
+
+
+def test_streamed_run_equals_resident_run_512cube(mpcf):
+    """The e2e path at the bench's size and settings: configuration 3's
+    cloud held in page-locked host memory and streamed through the GPU in 16
+    z-chunks (32 x 8 tiles, 32-plane layers, persistent, bulk-copy staging),
+    three steps, against the same steps of the device-resident run: the
+    host state and the time bit for bit."""
+    import torch
+    cfg = mpcf.configs.config("c3_512")
+    dims = cfg["dims"][0]
+    tiling = (8, 32, True, True)
+    with mpcf.Solver([dims], precision="mixed") as s:
+        s.set_tiling(*tiling)
+        s.ic_cloud(cfg["params"], cfg["bubbles"][0])
+        U0 = s.get_state(with_reg=False)
+        t_res = s.run(3, cfl=0.3, graph=True)[0]
+        U_res = s.get_state(with_reg=False)
+    host = [torch.empty(U0[0].size, dtype=torch.float32, pin_memory=True) for _ in range(7)]
+    for q in range(7):
+        host[q].numpy()[:] = U0[q]
+    del U0
+    arrs = [h.numpy() for h in host]
+    with mpcf.Solver([dims], precision="mixed") as s:
+        s.set_tiling(*tiling)
+        t = s.run_host(arrs, 3, cfl=0.3, nchunks=16)
+        assert s.error_word() == 0
+    assert t == t_res, (t, t_res)
+    for q in range(7):
+        assert np.array_equal(arrs[q], U_res[q]), q
