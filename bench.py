@@ -11,7 +11,7 @@ Synthetic inputs of that shape (no dataset is involved).
 One step = max speed of sound + on-device dt + three LSRK3 stages, replayed
 as a CUDA graph over device-resident state (inputs 11 GB > L2, so no flush
 is needed between steps).  The headline `value` is the MIXED form
-(FP32 bulk, FP64 pressure recovery and conservation sums); the line also
+(FP32 bulk, compensated FP32 pressure recovery, FP64 conservation sums); the line also
 carries the all-FP64 throughput on the same workload and the L1 / L-inf
 error of rho, p and G of the mixed run against the FP64 run.
 

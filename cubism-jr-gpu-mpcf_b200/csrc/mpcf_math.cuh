@@ -18,8 +18,8 @@
 //   PolFast32  float everywhere; WENO smoothness indicators in factored
 //              (cancellation-free, shared-curvature) form, weights from
 //              single-precision reciprocals, fused multiply-adds allowed.
-//   PolMixed   PolFast32 plus the stiffened-gas pressure recovery in FP64
-//              and FP64 conservation sums.
+//   PolMixed   PolFast32 plus the stiffened-gas pressure recovery in
+//              compensated FP32 (two-sum) and FP64 conservation sums.
 //   PolFP64    double storage and arithmetic (the all-FP64 GPU oracle run).
 //   PolFast64  double storage and arithmetic with the fast forms' algebra
 //              (factored indicators and fluxes, refined double reciprocals):
@@ -42,15 +42,15 @@ namespace mpcf {
 #define MPCF_WENOEPS 1e-6   // Makefile.config:15 (weps ?= 1e-6)
 #endif
 
-struct PolRef32  { typedef float  T; static constexpr bool kFastWeno = false; static constexpr bool kP64 = false; static constexpr bool kRefRounding = true;  static constexpr bool kWeno3 = false; static constexpr int id = 0; };
-struct PolFast32 { typedef float  T; static constexpr bool kFastWeno = true;  static constexpr bool kP64 = false; static constexpr bool kRefRounding = false; static constexpr bool kWeno3 = false; static constexpr int id = 1; };
-struct PolMixed  { typedef float  T; static constexpr bool kFastWeno = true;  static constexpr bool kP64 = true;  static constexpr bool kRefRounding = false; static constexpr bool kWeno3 = false; static constexpr int id = 2; };
-struct PolFP64   { typedef double T; static constexpr bool kFastWeno = false; static constexpr bool kP64 = false; static constexpr bool kRefRounding = true;  static constexpr bool kWeno3 = false; static constexpr int id = 3; };
-struct PolFast64 { typedef double T; static constexpr bool kFastWeno = true;  static constexpr bool kP64 = false; static constexpr bool kRefRounding = false; static constexpr bool kWeno3 = false; static constexpr int id = 4; };
+struct PolRef32  { typedef float  T; static constexpr bool kFastWeno = false; static constexpr bool kCompP = false; static constexpr bool kRefRounding = true;  static constexpr bool kWeno3 = false; static constexpr int id = 0; };
+struct PolFast32 { typedef float  T; static constexpr bool kFastWeno = true;  static constexpr bool kCompP = false; static constexpr bool kRefRounding = false; static constexpr bool kWeno3 = false; static constexpr int id = 1; };
+struct PolMixed  { typedef float  T; static constexpr bool kFastWeno = true;  static constexpr bool kCompP = true;  static constexpr bool kRefRounding = false; static constexpr bool kWeno3 = false; static constexpr int id = 2; };
+struct PolFP64   { typedef double T; static constexpr bool kFastWeno = false; static constexpr bool kCompP = false; static constexpr bool kRefRounding = true;  static constexpr bool kWeno3 = false; static constexpr int id = 3; };
+struct PolFast64 { typedef double T; static constexpr bool kFastWeno = true;  static constexpr bool kCompP = false; static constexpr bool kRefRounding = false; static constexpr bool kWeno3 = false; static constexpr int id = 4; };
 // The reference's compile-time WENO3 build (-D_WENO3_, GPUonly.cuh:102,141)
 // of the two reference-rounding forms.
-struct PolRef32W3 { typedef float  T; static constexpr bool kFastWeno = false; static constexpr bool kP64 = false; static constexpr bool kRefRounding = true; static constexpr bool kWeno3 = true; static constexpr int id = 0; };
-struct PolFP64W3  { typedef double T; static constexpr bool kFastWeno = false; static constexpr bool kP64 = false; static constexpr bool kRefRounding = true; static constexpr bool kWeno3 = true; static constexpr int id = 3; };
+struct PolRef32W3 { typedef float  T; static constexpr bool kFastWeno = false; static constexpr bool kCompP = false; static constexpr bool kRefRounding = true; static constexpr bool kWeno3 = true; static constexpr int id = 0; };
+struct PolFP64W3  { typedef double T; static constexpr bool kFastWeno = false; static constexpr bool kCompP = false; static constexpr bool kRefRounding = true; static constexpr bool kWeno3 = true; static constexpr int id = 3; };
 
 __device__ __forceinline__ float  dmin(float a, float b)   { return fminf(a, b); }
 __device__ __forceinline__ float  dmax(float a, float b)   { return fmaxf(a, b); }
@@ -512,9 +512,28 @@ __device__ __forceinline__ void face_hllc(const FaceState<typename Pol::T>& S, c
 // p, G, P).  Reference form (GPUkernels.cu:209-244):
 //   u = (rho u)/rho, ...;  p = (E - 0.5f*rho*(u*u + v*v + w*w) - P) / G
 // in the reference-rounding and FP64 policies.  The fast policies multiply
-// by reciprocals; the mixed policy evaluates the pressure recovery in FP64
-// from the stored conserved values:
-//   p = (E - 0.5*((rho u)^2+(rho v)^2+(rho w)^2)/rho - P)/G.
+// by reciprocals.  In the liquid E and P are ~50x the internal energy G p,
+// so E - ke - P cancels catastrophically in FP32; the mixed policy recovers
+// the pressure in compensated FP32 (comp_pressure below).
+// Compensated FP32 pressure recovery p = ((E - P) - ke) / G.  E - P is
+// formed as the unevaluated sum s + e of the two-sum algorithm (Knuth; s the
+// rounded difference, e its exact rounding error), so the cancellation of E
+// against P loses nothing; ke (small against E) is subtracted from s and e
+// added back; the quotient is a product with the approximate reciprocal of
+// G, corrected once by its residual (num - G q) / G.  Every operation is an
+// explicit round-to-nearest instruction, so the result does not depend on
+// the translation unit's contraction flags.
+__device__ __forceinline__ float comp_pressure(const float E, const float P, const float G, const float ke)
+{
+    const float s = __fsub_rn(E, P);
+    const float z = __fsub_rn(s, E);
+    const float e = __fadd_rn(__fsub_rn(E, __fsub_rn(s, z)), __fsub_rn(-P, z));
+    const float num = __fadd_rn(__fsub_rn(s, ke), e);
+    const float iG = rcp_approx(G);
+    const float q = __fmul_rn(num, iG);
+    return __fmaf_rn(__fmaf_rn(-G, q, num), iG, q);
+}
+
 template <class Pol>
 __device__ __forceinline__ void to_primitive(const typename Pol::T c[7], typename Pol::T q[7])
 {
@@ -526,12 +545,9 @@ __device__ __forceinline__ void to_primitive(const typename Pol::T c[7], typenam
         q[1] = c[1] * ir;
         q[2] = c[2] * ir;
         q[3] = c[3] * ir;
-        if constexpr (Pol::kP64)
-        {
-            const double m2 = (double)c[1]*(double)c[1] + (double)c[2]*(double)c[2] + (double)c[3]*(double)c[3];
-            const double ke = 0.5 * m2 * rcp_f64((double)c[0]);
-            q[4] = (T)(((double)c[4] - ke - (double)c[6]) * rcp_f64((double)c[5]));
-        }
+        if constexpr (Pol::kCompP)
+            q[4] = comp_pressure(c[4], c[6], c[5],
+                                 __fmul_rn(__fmaf_rn(c[3], q[3], __fmaf_rn(c[2], q[2], __fmul_rn(c[1], q[1]))), 0.5f));
         else
             q[4] = (c[4] - (T)0.5*c[0]*(q[1]*q[1] + q[2]*q[2] + q[3]*q[3]) - c[6]) * rcp_approx(c[5]);
     }
@@ -561,7 +577,7 @@ __device__ __forceinline__ double shfl_max(double v) { for (int o = 16; o > 0; o
 
 // Maximum characteristic speed of one cell, |u|max + c with
 //   p = (E - (ru^2+rv^2+rw^2)*(0.5/rho) - P)/G,  c = sqrt(((p+P)/G + p)/rho)
-// (GPUkernels.cu:1182-1222; the mixed policy recovers p in FP64).  Every
+// (GPUkernels.cu:1182-1222; the mixed policy recovers p in compensated FP32).  Every
 // operation is an explicit instruction -- round-to-nearest intrinsics, and
 // in the fast policies the approximate reciprocal and square root -- so the
 // result is the same whatever the translation unit's contraction and
@@ -583,40 +599,26 @@ __device__ __forceinline__ typename Pol::T cell_sos_rn(const typename Pol::T r, 
     else if constexpr (Pol::kFastWeno)
     {
         // the fast policies: reciprocals and square root of the special-
-        // function unit, refined in FP64 for the mixed pressure, every
-        // operation an explicit instruction (so the two reductions still
-        // agree bit for bit)
+        // function unit, the compensated pressure in the mixed policy,
+        // every operation an explicit instruction (so the two reductions
+        // still agree bit for bit)
         const float ir = rcp_approx(r), iG = rcp_approx(G);
+        const float sq = __fmaf_rn(w, w, __fmaf_rn(v, v, __fmul_rn(u, u)));
+        const float ke = __fmul_rn(sq, __fmul_rn(0.5f, ir));
         float p;
-        if constexpr (Pol::kP64)
-        {
-            const double du = u, dv = v, dw = w;
-            const double sq = __fma_rn(dw, dw, __fma_rn(dv, dv, __dmul_rn(du, du)));
-            const double ke = __dmul_rn(sq, __dmul_rn(0.5, rcp_f64((double)r)));
-            p = (float)__dmul_rn(__dsub_rn(__dsub_rn((double)e, ke), (double)P), rcp_f64((double)G));
-        }
+        if constexpr (Pol::kCompP)
+            p = comp_pressure(e, P, G, ke);
         else
-        {
-            const float sq = __fmaf_rn(w, w, __fmaf_rn(v, v, __fmul_rn(u, u)));
-            p = __fmul_rn(__fsub_rn(__fsub_rn(e, __fmul_rn(sq, __fmul_rn(0.5f, ir))), P), iG);
-        }
+            p = __fmul_rn(__fsub_rn(__fsub_rn(e, ke), P), iG);
         const float c = sqrt_approx(__fmul_rn(__fmaf_rn(__fadd_rn(p, P), iG, p), ir));
         return __fmaf_rn(fmaxf(fmaxf(fabsf(u), fabsf(v)), fabsf(w)), ir, c);
     }
     else
     {
-        float p;
-        if constexpr (Pol::kP64)
-        {
-            const double du = u, dv = v, dw = w;
-            const double sq = __dadd_rn(__dadd_rn(__dmul_rn(du, du), __dmul_rn(dv, dv)), __dmul_rn(dw, dw));
-            p = (float)__ddiv_rn(__dsub_rn(__dsub_rn((double)e, __dmul_rn(sq, __ddiv_rn(0.5, (double)r))), (double)P), (double)G);
-        }
-        else
-        {
-            const float sq = __fadd_rn(__fadd_rn(__fmul_rn(u, u), __fmul_rn(v, v)), __fmul_rn(w, w));
-            p = __fdiv_rn(__fsub_rn(__fsub_rn(e, __fmul_rn(sq, __fdiv_rn(0.5f, r))), P), G);
-        }
+        // the reference-rounding policy: IEEE division and square root
+        static_assert(!Pol::kCompP, "compensated pressure: fast policies only");
+        const float sq = __fadd_rn(__fadd_rn(__fmul_rn(u, u), __fmul_rn(v, v)), __fmul_rn(w, w));
+        const float p = __fdiv_rn(__fsub_rn(__fsub_rn(e, __fmul_rn(sq, __fdiv_rn(0.5f, r))), P), G);
         const float c = __fsqrt_rn(__fdiv_rn(__fadd_rn(__fdiv_rn(__fadd_rn(p, P), G), p), r));
         return __fadd_rn(c, __fdiv_rn(fmaxf(fmaxf(fabsf(u), fabsf(v)), fabsf(w)), r));
     }

@@ -37,7 +37,7 @@ typedef struct mpcf_solver mpcf_solver;
 /* precisions */
 #define MPCF_PREC_FP32_REF 0  /* FP32, rounding of the reference source (bit-exact to the CPU restatement) */
 #define MPCF_PREC_FP32     1  /* FP32, fast weights / division, fused multiply-add */
-#define MPCF_PREC_MIXED    2  /* fast FP32 + FP64 pressure recovery + FP64 conservation sums */
+#define MPCF_PREC_MIXED    2  /* fast FP32 + compensated (two-sum) FP32 pressure recovery + FP64 conservation sums */
 #define MPCF_PREC_FP64     3  /* all FP64, rounding order of the reference source */
 #define MPCF_PREC_FP64_FAST 4 /* all FP64 with the fast forms' factored algebra and refined reciprocals */
 

@@ -208,7 +208,7 @@ def test_fast_forms_every_tiling_tracks_fp64_oracle(mpcf, prec, dims):
         # FP32 pressure recovery cancels on liquid cells (p ~ 1e2 against
         # E, P ~ 1e4): the fast FP32 form's state is ~1e-4 off FP64 there,
         # below the reference rounding's own ~3e-4; the mixed form recovers
-        # the pressure in FP64 and stays at FP32 rounding
+        # the pressure in compensated FP32 and stays at FP32 rounding
         tol_u = 2e-4 if prec == "fp32" else 2e-6
         for q in range(7):
             assert rel_linf(Ug[q], U[q]) <= tol_u, (tiling, q, rel_linf(Ug[q], U[q]))
@@ -257,7 +257,7 @@ def rel_l1(a, b):
 def test_fast_forms_at_least_as_accurate_as_reference_rounding(mpcf, prec):
     """The fast FP32 and mixed forms are not bit-exact to the reference by
     design (factored smoothness indicators, single-precision weights, fused
-    multiply-adds, FP64 pressure in the mixed form).  The reference's own
+    multiply-adds, compensated pressure in the mixed form).  The reference's own
     FP32 indicators cancel ~1e4-sized products down to ~epsilon on smooth
     liquid stencils, so its results carry rounding noise of O(local
     variation); the right yardstick is the FP64 oracle.  After one LSRK3
