@@ -52,7 +52,7 @@ DTYPE_OF = {"mixed": "f32+f64 (mixed)", "fp32": "f32", "fp32_ref": "f32 (referen
             "fp64_fast": "f64 (fast form)"}
 FORM_OF = {"mixed": "mixed form", "fp32": "fast FP32 form", "fp32_ref": "FP32 reference-rounding form",
            "fp64": "FP64 form", "fp64_fast": "fast FP64 form (factored algebra, refined reciprocals)"}
-MEASURED_DRAM_BYTES_PER_CELL_STAGE = {"mixed": (2.144534528e9 + 1.830834432e9) / (512 * 512 * 128)}
+MEASURED_DRAM_BYTES_PER_CELL_STAGE = {"mixed": (2.135219968e9 + 1.831107072e9) / (512 * 512 * 128)}
 
 
 # Algorithmic floating-point operations of one cell-stage, counted by
