@@ -140,6 +140,14 @@ struct mpcf_solver
     cudaStream_t up = nullptr, down = nullptr;
     std::vector<cudaEvent_t> ev_up, ev_st, ev_down;
     cudaEvent_t ev_start = nullptr;
+
+    // windowed runs (mpcf_create_window / mpcf_run_window): the domains are
+    // slots of win_nslices planes that z-chunks of a win_nz-plane domain
+    // held in host memory pass through; win_bc: its z faces.  Per slot, the
+    // events that free it for the next chunk (compute stream, download).
+    int win_nz = 0, win_nslices = 0, win_nch = 0;
+    int win_bc[2] = {0, 0};
+    std::vector<cudaEvent_t> ev_free_c, ev_free_d;
 };
 
 namespace {
@@ -428,7 +436,7 @@ int enqueue_dt(mpcf_solver* s, double cfl, double dt_max)
     A.dt = s->dt;
     A.time = s->time;
     A.err = s->err;
-    A.grouped = s->links.empty() ? 0 : 1;
+    A.grouped = (s->links.empty() && !s->win_nch) ? 0 : 1;
     CK(launch_dt(s->pol, A, s->stream));
     return MPCF_OK;
 }
@@ -445,6 +453,14 @@ int enqueue_step(mpcf_solver* s, double cfl, double dt_max, bool standalone_sos)
     for (int k = 0; k < 3; ++k)
         if ((rc = enqueue_stage(s, kLSRK3[k][0], kLSRK3[k][1], s->track_cons && k == 2, k == 2))) return rc;
     return MPCF_OK;
+}
+
+// A windowed solver's domains are slots that z-chunks pass through; only
+// mpcf_run_window advances them.
+int window_only(const mpcf_solver* s, const char* what)
+{
+    return fail(MPCF_ERR_STATE, "%s: a windowed solver (%d slots of %d planes) is advanced by mpcf_run_window",
+                what, s->ndom, s->win_nslices);
 }
 
 int check_dom(const mpcf_solver* s, int dom)
@@ -592,7 +608,7 @@ int mpcf_destroy(mpcf_solver* s)
     if (s->stream) cudaStreamSynchronize(s->stream);
     for (cudaStream_t c : {s->up, s->down})
         if (c) { cudaStreamSynchronize(c); cudaStreamDestroy(c); }
-    for (auto* v : {&s->ev_up, &s->ev_st, &s->ev_down})
+    for (auto* v : {&s->ev_up, &s->ev_st, &s->ev_down, &s->ev_free_c, &s->ev_free_d})
         for (cudaEvent_t e : *v) cudaEventDestroy(e);
     if (s->ev_start) cudaEventDestroy(s->ev_start);
     destroy_graphs(s);
@@ -674,6 +690,7 @@ int mpcf_stage(mpcf_solver* s, double a, double b, const double* dtinvh)
 {
     Range nvtx("mpcf_stage");
     if (!s) return fail(MPCF_ERR_ARG, "null solver");
+    if (s->win_nch) return window_only(s, "mpcf_stage");
     DeviceGuard g(s->device);
     s->sos_fresh = false;                   // the state (or the accumulator) changes
     if (dtinvh)
@@ -729,6 +746,7 @@ int mpcf_enqueue_stage(mpcf_solver* s, double a, double b)
 {
     Range nvtx("mpcf_enqueue_stage");
     if (!s) return fail(MPCF_ERR_ARG, "null solver");
+    if (s->win_nch) return window_only(s, "mpcf_enqueue_stage");
     DeviceGuard g(s->device);
     s->sos_fresh = false;
     return enqueue_stage(s, a, b, false);
@@ -753,6 +771,7 @@ int mpcf_step(mpcf_solver* s, double cfl, double dt_max, double* dt_out)
 {
     Range nvtx("mpcf_step");
     if (!s) return fail(MPCF_ERR_ARG, "null solver");
+    if (s->win_nch) return window_only(s, "mpcf_step");
     if (!(cfl > 0) || !(dt_max > 0)) return fail(MPCF_ERR_ARG, "cfl and dt_max must be positive");
     DeviceGuard g(s->device);
     int rc = enqueue_step(s, cfl, dt_max, !s->sos_fresh);
@@ -770,6 +789,7 @@ int mpcf_run(mpcf_solver* s, int nsteps, double cfl, double dt_max, int use_grap
 {
     Range nvtx("mpcf_run");
     if (!s) return fail(MPCF_ERR_ARG, "null solver");
+    if (s->win_nch) return window_only(s, "mpcf_run");
     if (nsteps < 0) return fail(MPCF_ERR_ARG, "nsteps < 0");
     if (!(cfl > 0) || !(dt_max > 0)) return fail(MPCF_ERR_ARG, "cfl and dt_max must be positive");
     DeviceGuard g(s->device);
@@ -823,6 +843,7 @@ int mpcf_run_host(mpcf_solver* s, int nsteps, double cfl, double dt_max, void* c
 {
     Range nvtx("mpcf_run_host");
     if (!s) return fail(MPCF_ERR_ARG, "null solver");
+    if (s->win_nch) return window_only(s, "mpcf_run_host");
     if (nsteps < 0 || nchunks < 1) return fail(MPCF_ERR_ARG, "nsteps < 0 or nchunks < 1");
     if (!(cfl > 0) || !(dt_max > 0)) return fail(MPCF_ERR_ARG, "cfl and dt_max must be positive");
     if (!host7) return fail(MPCF_ERR_ARG, "null host state");
@@ -951,6 +972,312 @@ int mpcf_run_host(mpcf_solver* s, int nsteps, double cfl, double dt_max, void* c
     // the device state equals the host result, and the sound-speed
     // accumulator holds its maximum (from the last stage 3)
     if (nsteps > 0) s->sos_fresh = true;
+    s->sums_valid = false;
+    CK(cudaStreamSynchronize(s->down));
+    CK(cudaStreamSynchronize(s->up));
+    if (time_out) CK(cudaMemcpyAsync(time_out, s->time, sizeof(double), cudaMemcpyDeviceToHost, s->stream));
+    CK(cudaStreamSynchronize(s->stream));
+    return MPCF_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Windowed runs: a domain held in host memory that may exceed device memory
+// (GPUlab's z-chunks of nslices planes streamed through the GPU,
+// GPUlab.cpp:202-372,703-793).  The solver's domains are slots of nslices
+// planes with 3 stored ghost planes on each z side; chunk c of a step passes
+// through slot c % nslots.
+// ---------------------------------------------------------------------------
+namespace {
+
+// One operation of a windowed run in the order the host enqueues it.  step
+// -1: the sound-speed pass of the first step's input.
+struct WinOp { int op, step, stage, chunk; };
+enum { WOP_UPLOAD = 0, WOP_SOS = 1, WOP_DT = 2, WOP_STAGE = 3, WOP_DOWNLOAD = 4 };
+
+// The plan of nsteps steps of nch chunks through ns slots.  Stage k of chunk
+// c needs stage k-1 (stage 1: the upload) of chunks up to c+1, whose planes
+// its upper ghost planes copy; a slot is free for its next chunk once that
+// chunk's stage 3 has been downloaded and the stage 3 of the chunk above
+// (which copies its top planes) is queued.  Each step's dt needs the sound
+// speed of all of its input: the first from a pass that streams every chunk
+// through the slots and reduces it, later ones from what stage 3 of the
+// step before accumulated.  Operations are taken greedily, downloads and the
+// later stages first; false if nothing can proceed (too few slots).
+bool window_plan(const int nch, const int ns, const int nsteps, std::vector<WinOp>& plan)
+{
+    plan.clear();
+    if (nsteps <= 0) return true;
+    if (nch < 1 || ns < 1) return false;
+    auto hi = [&](const int c) { return std::min(c + 1, nch - 1); };
+    // the sound-speed pass: chunk u into slot u % ns once chunk u - ns has
+    // been reduced
+    for (int u = 0, q = 0; q < nch;)
+    {
+        if (u < nch && u - q < ns) plan.push_back({WOP_UPLOAD, -1, 0, u++});
+        else plan.push_back({WOP_SOS, -1, 0, q++});
+    }
+    plan.push_back({WOP_DT, 0, 0, 0});
+    int dts = 1;                                   // steps whose dt is queued
+    const long long total = (long long)nsteps * nch;
+    long long up = 0, dn = 0, st[3] = {0, 0, 0};   // next operation of each kind (step * nch + chunk)
+    std::vector<long long> occ(ns, -1);
+    std::vector<char> busy(ns, 0);
+    auto released = [&](const long long j)
+    {
+        const long long above = (j % nch == nch - 1) ? j : j + 1;
+        return st[2] > above && dn > j;
+    };
+    while (dn < total)
+    {
+        for (int k = 0; k < ns; ++k)
+            if (busy[k] && released(occ[k])) busy[k] = 0;
+        if (st[2] > dn)
+        {
+            plan.push_back({WOP_DOWNLOAD, (int)(dn / nch), 0, (int)(dn % nch)});
+            ++dn;
+            continue;
+        }
+        if (dts < nsteps && st[2] >= (long long)dts * nch)
+        {
+            plan.push_back({WOP_DT, dts, 0, 0});
+            ++dts;
+            continue;
+        }
+        bool did = false;
+        for (int k = 2; k >= 0 && !did; --k)
+        {
+            const long long j = st[k];
+            if (j >= total) continue;
+            const int n = (int)(j / nch), c = (int)(j % nch);
+            if (n >= dts) continue;
+            const long long need = (long long)n * nch + hi(c);
+            if ((k == 0 ? up : st[k - 1]) > need)
+            {
+                plan.push_back({WOP_STAGE, n, k, c});
+                ++st[k];
+                did = true;
+            }
+        }
+        if (did) continue;
+        if (up < total)
+        {
+            const int slot = (int)((up % nch) % ns);
+            if (!busy[slot])
+            {
+                busy[slot] = 1;
+                occ[slot] = up;
+                plan.push_back({WOP_UPLOAD, (int)(up / nch), 0, (int)(up % nch)});
+                ++up;
+                continue;
+            }
+        }
+        return false;
+    }
+    return true;
+}
+
+} // namespace
+
+int mpcf_window_plan(int nchunks, int nslots, int nsteps, int* ops4, int cap)
+{
+    std::vector<WinOp> plan;
+    if (nchunks < 1 || nslots < 1 || nsteps < 0) return fail(MPCF_ERR_ARG, "nchunks, nslots >= 1 and nsteps >= 0");
+    if (!window_plan(nchunks, nslots, nsteps, plan))
+        return fail(MPCF_ERR_ARG, "%d slots are too few for %d chunks", nslots, nchunks);
+    if (ops4)
+        for (int i = 0; i < (int)plan.size() && i < cap; ++i)
+        {
+            ops4[4 * i] = plan[i].op;
+            ops4[4 * i + 1] = plan[i].step;
+            ops4[4 * i + 2] = plan[i].stage;
+            ops4[4 * i + 3] = plan[i].chunk;
+        }
+    return (int)plan.size();
+}
+
+int mpcf_create_window(mpcf_solver** out, int nx, int ny, int nz, int nslices, int nslots, int precision,
+                       const int* bc6, int device)
+{
+    if (!out) return fail(MPCF_ERR_ARG, "null output handle");
+    *out = nullptr;
+    if (nslices < kHaloPlanes || nz < nslices || nz % nslices)
+        return fail(MPCF_ERR_ARG, "nslices (%d) must be at least %d and divide nz (%d)", nslices, kHaloPlanes, nz);
+    const int nch = nz / nslices;
+    const int ns = std::min(nslots, nch);
+    std::vector<WinOp> plan;
+    if (nslots < 1 || !window_plan(nch, ns, 2, plan))
+        return fail(MPCF_ERR_ARG, "%d slots are too few for %d chunks (at least %d)", nslots, nch, std::min(5, nch));
+    int bc[6] = {MPCF_BC_ABSORBING, MPCF_BC_ABSORBING, MPCF_BC_ABSORBING, MPCF_BC_ABSORBING,
+                 MPCF_BC_ABSORBING, MPCF_BC_ABSORBING};
+    if (bc6)
+        for (int f = 0; f < 6; ++f)
+        {
+            if (bc6[f] != MPCF_BC_ABSORBING && bc6[f] != MPCF_BC_REFLECTING)
+                return fail(MPCF_ERR_ARG, "boundary condition %d on face %d: absorbing or reflecting", bc6[f], f);
+            bc[f] = bc6[f];
+        }
+    std::vector<int> dims(3 * ns), bcs(6 * ns);
+    for (int d = 0; d < ns; ++d)
+    {
+        dims[3 * d] = nx; dims[3 * d + 1] = ny; dims[3 * d + 2] = nslices;
+        for (int f = 0; f < 4; ++f) bcs[6 * d + f] = bc[f];
+        bcs[6 * d + 4] = bcs[6 * d + 5] = MPCF_BC_HALO;
+    }
+    mpcf_solver* s = nullptr;
+    int rc = mpcf_create(&s, ns, dims.data(), bcs.data(), precision, device);
+    if (rc) return rc;
+    s->win_nz = nz;
+    s->win_nslices = nslices;
+    s->win_nch = nch;
+    s->win_bc[0] = bc[4];
+    s->win_bc[1] = bc[5];
+    // the domain's spacing and geometry; all slots advance with one dt
+    const double h = 1.0 / (double)std::max(nx, std::max(ny, nz));
+    for (int d = 0; d < ns; ++d)
+    {
+        DomDev& D = s->hdoms[d];
+        D.h = h;
+        D.group = 0;
+        D.gdim[0] = nx; D.gdim[1] = ny; D.gdim[2] = nz;
+    }
+    DeviceGuard g(s->device);
+    if (cudaMemcpyAsync(s->ddoms, s->hdoms.data(), sizeof(DomDev) * s->ndom, cudaMemcpyHostToDevice, s->stream) != cudaSuccess ||
+        cudaStreamSynchronize(s->stream) != cudaSuccess)
+    {
+        cudaGetLastError();
+        mpcf_destroy(s);
+        return fail(MPCF_ERR_CUDA, "window set-up copy failed");
+    }
+    *out = s;
+    return MPCF_OK;
+}
+
+int mpcf_window_info(const mpcf_solver* s, int* info4)
+{
+    if (!s || !info4) return fail(MPCF_ERR_ARG, "null argument");
+    if (!s->win_nch) return fail(MPCF_ERR_STATE, "not a windowed solver");
+    info4[0] = s->win_nz;
+    info4[1] = s->win_nslices;
+    info4[2] = s->win_nch;
+    info4[3] = s->ndom;
+    return MPCF_OK;
+}
+
+int mpcf_run_window(mpcf_solver* s, int nsteps, double cfl, double dt_max, void* const* host7, double* time_out)
+{
+    Range nvtx("mpcf_run_window");
+    if (!s) return fail(MPCF_ERR_ARG, "null solver");
+    if (!s->win_nch) return fail(MPCF_ERR_STATE, "mpcf_run_window needs a windowed solver (mpcf_create_window)");
+    if (nsteps < 0) return fail(MPCF_ERR_ARG, "nsteps < 0");
+    if (!(cfl > 0) || !(dt_max > 0)) return fail(MPCF_ERR_ARG, "cfl and dt_max must be positive");
+    if (!host7) return fail(MPCF_ERR_ARG, "null host state");
+    for (int q = 0; q < 7; ++q) if (!host7[q]) return fail(MPCF_ERR_ARG, "host field %d is null", q);
+    const int nch = s->win_nch, ns = s->ndom, nsl = s->win_nslices;
+    std::vector<WinOp> plan;
+    if (!window_plan(nch, ns, nsteps, plan)) return fail(MPCF_ERR_STATE, "window plan stalled (%d slots, %d chunks)", ns, nch);
+    DeviceGuard g(s->device);
+    const long long plane = (long long)s->hdoms[0].nx * s->hdoms[0].ny;
+    const size_t esz = s->esz;
+    const size_t cbytes = (size_t)nsl * plane * esz;        // one field of one chunk
+    const long long fs = s->hdoms[0].fs;
+    if (!s->up)
+    {
+        CK(cudaStreamCreateWithFlags(&s->up, cudaStreamNonBlocking));
+        CK(cudaStreamCreateWithFlags(&s->down, cudaStreamNonBlocking));
+        CK(cudaEventCreateWithFlags(&s->ev_start, cudaEventDisableTiming));
+    }
+    auto grow = [&](std::vector<cudaEvent_t>& v, const int n)
+    {
+        while ((int)v.size() < n)
+        {
+            cudaEvent_t e;
+            if (cudaEventCreateWithFlags(&e, cudaEventDisableTiming) != cudaSuccess) return false;
+            v.push_back(e);
+        }
+        return true;
+    };
+    if (!grow(s->ev_up, nch) || !grow(s->ev_st, nch) || !grow(s->ev_free_c, ns) || !grow(s->ev_free_d, ns))
+    { cudaGetLastError(); return fail(MPCF_ERR_CUDA, "cudaEventCreate failed"); }
+    // the slots' last use by earlier work on the solver's stream frees them
+    CK(cudaEventRecord(s->ev_start, s->stream));
+    CK(cudaStreamWaitEvent(s->up, s->ev_start, 0));
+    CK(cudaStreamWaitEvent(s->down, s->ev_start, 0));
+    for (int k = 0; k < ns; ++k)
+    {
+        CK(cudaEventRecord(s->ev_free_c[k], s->stream));
+        CK(cudaEventRecord(s->ev_free_d[k], s->down));
+    }
+    CK(cudaMemsetAsync(s->sos_bits, 0, esz * ns, s->stream));
+    const int p0 = s->parity;
+    int rc = MPCF_OK;
+    for (const WinOp& o : plan)
+    {
+        const int c = o.chunk, slot = c % ns;
+        const int p = o.step < 0 ? p0 : (p0 ^ (o.step & 1));      // the step's input buffer
+        DomDev& D = s->hdoms[slot];
+        const size_t off = (size_t)c * cbytes;
+        switch (o.op)
+        {
+            case WOP_UPLOAD:
+                CK(cudaStreamWaitEvent(s->up, s->ev_free_c[slot], 0));
+                CK(cudaStreamWaitEvent(s->up, s->ev_free_d[slot], 0));
+                for (int q = 0; q < 7; ++q)
+                    CK(cudaMemcpyAsync((char*)D.U[p] + (size_t)q * fs * esz, (const char*)host7[q] + off, cbytes,
+                                       cudaMemcpyHostToDevice, s->up));
+                CK(cudaEventRecord(s->ev_up[c], s->up));
+                break;
+            case WOP_SOS:
+            {
+                CK(cudaStreamWaitEvent(s->stream, s->ev_up[c], 0));
+                SosArgs A;
+                A.doms = s->ddoms;
+                A.ndom = ns;
+                A.nchunks = D.sos_chunks;
+                A.chunk = s->sos_chunk;
+                A.chunk0 = D.sos_chunk_begin;
+                A.parity = p;
+                A.sos_bits = s->sos_bits;
+                CK(launch_sos(s->pol, A, s->stream));
+                CK(cudaEventRecord(s->ev_free_c[slot], s->stream));
+                break;
+            }
+            case WOP_DT:
+                if ((rc = enqueue_dt(s, cfl, dt_max))) return rc;
+                break;
+            case WOP_STAGE:
+            {
+                const int k = o.stage, b = p ^ (k & 1);
+                if (k == 0) CK(cudaStreamWaitEvent(s->stream, s->ev_up[std::min(c + 1, nch - 1)], 0));
+                const void* lo = c > 0 ? s->hdoms[(c - 1) % ns].U[b] : nullptr;
+                const void* hi = c < nch - 1 ? s->hdoms[(c + 1) % ns].U[b] : nullptr;
+                CK(launch_window_ghosts((int)esz, D.U[b], lo, hi, fs, plane, nsl, s->win_bc[0], s->win_bc[1], s->stream));
+                s->parity = b;
+                rc = enqueue_stage_tiles(s, kLSRK3[k][0], kLSRK3[k][1], false, k == 2, D.tile_begin,
+                                         D.tile_begin + D.tiles_x * D.tiles_y * D.tiles_z);
+                s->parity = p0;
+                if (rc) return rc;
+                if (k == 2)
+                {
+                    CK(cudaEventRecord(s->ev_st[c], s->stream));
+                    // the chunk below is no longer read (its top planes were
+                    // this stage's lower ghost planes); the last chunk frees
+                    // its own slot
+                    if (c > 0) CK(cudaEventRecord(s->ev_free_c[(c - 1) % ns], s->stream));
+                    if (c == nch - 1) CK(cudaEventRecord(s->ev_free_c[slot], s->stream));
+                }
+                break;
+            }
+            case WOP_DOWNLOAD:
+                CK(cudaStreamWaitEvent(s->down, s->ev_st[c], 0));
+                for (int q = 0; q < 7; ++q)
+                    CK(cudaMemcpyAsync((char*)host7[q] + off, (const char*)D.U[p ^ 1] + (size_t)q * fs * esz, cbytes,
+                                       cudaMemcpyDeviceToHost, s->down));
+                CK(cudaEventRecord(s->ev_free_d[slot], s->down));
+                break;
+        }
+    }
+    s->parity = p0 ^ (nsteps & 1);
+    s->sos_fresh = false;
     s->sums_valid = false;
     CK(cudaStreamSynchronize(s->down));
     CK(cudaStreamSynchronize(s->up));
@@ -1741,6 +2068,7 @@ int mpcf_autotune(mpcf_solver* s, int reps, int* best3, double* best_ms)
 {
     Range nvtx("mpcf_autotune");
     if (!s) return fail(MPCF_ERR_ARG, "null solver");
+    if (s->win_nch) return window_only(s, "mpcf_autotune");
     if (reps < 1) reps = 3;
     DeviceGuard g(s->device);
     s->sos_fresh = false;                   // the state (or the accumulator) changes

@@ -793,6 +793,61 @@ cudaError_t launch_halo(int esz, const DomDev* doms, const int* links, int nlink
     return cudaGetLastError();
 }
 
+// Ghost planes of one slot of a windowed run (mpcf_run_window): the slot
+// holds nz planes of a z-chunk of a larger domain at dst (plane 0), with 3
+// stored ghost planes on each side.  Block row blockIdx.y = 7 side + q fills
+// field q's 3 planes below (side 0) or above (side 1) the slot: from the top 3
+// planes of the slot below (lo) or the bottom 3 of the slot above (hi), or,
+// at the domain's own z faces (lo / hi null), by its boundary condition as
+// the stage kernel's own mapping gives it (BoundaryConditions.h:60-109):
+// absorbing repeats the face plane, reflecting mirrors the planes and negates
+// the normal momentum (a flip of the sign bit, as the negation in the
+// kernel's load).  The copies move bit patterns.
+template <class E>
+__global__ void window_ghosts_kernel(E* dst, const E* lo, const E* hi, long long fs, long long plane, int nz,
+                                     int bc_lo, int bc_hi)
+{
+    const int side = blockIdx.y / 7, q = blockIdx.y % 7;
+    const E sign = (E)1 << (sizeof(E) * 8 - 1);
+    const long long n = kHaloPlanes * plane;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+    {
+        const int g = (int)(i / plane) + 1;            // planes away from the slot's own planes, 1..3
+        const long long xy = i - (long long)(g - 1) * plane;
+        const E* src;
+        long long sp, dp;
+        bool flip = false;
+        if (side == 0)
+        {
+            dp = -(long long)g;
+            if (lo) { src = lo; sp = nz - g; }
+            else    { src = dst; const bool refl = bc_lo == BC_REFLECTING; sp = refl ? g - 1 : 0; flip = refl && q == 3; }
+        }
+        else
+        {
+            dp = nz - 1 + g;
+            if (hi) { src = hi; sp = g - 1; }
+            else    { src = dst; const bool refl = bc_hi == BC_REFLECTING; sp = refl ? nz - g : nz - 1; flip = refl && q == 3; }
+        }
+        const E v = src[q * fs + sp * plane + xy];
+        dst[q * fs + dp * plane + xy] = flip ? (v ^ sign) : v;
+    }
+}
+
+cudaError_t launch_window_ghosts(int esz, void* dst, const void* lo, const void* hi, long long fs, long long plane,
+                                 int nz, int bc_lo, int bc_hi, cudaStream_t st)
+{
+    const long long n = kHaloPlanes * plane;
+    const dim3 grid((unsigned)std::min<long long>((n + 255) / 256, 64), 14u);
+    if (esz == 8)
+        window_ghosts_kernel<unsigned long long><<<grid, 256, 0, st>>>((unsigned long long*)dst, (const unsigned long long*)lo,
+                                                                        (const unsigned long long*)hi, fs, plane, nz, bc_lo, bc_hi);
+    else
+        window_ghosts_kernel<unsigned><<<grid, 256, 0, st>>>((unsigned*)dst, (const unsigned*)lo, (const unsigned*)hi,
+                                                             fs, plane, nz, bc_lo, bc_hi);
+    return cudaGetLastError();
+}
+
 __global__ void zero_kernel(unsigned* p, size_t n)
 {
     for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) p[i] = 0u;

@@ -65,6 +65,10 @@ cudaError_t launch_zero(void* p, size_t bytes, cudaStream_t st);
 // device, max_plane = the largest nx*ny among the linked domains
 cudaError_t launch_halo(int esz, const DomDev* doms, const int* links, int nlinks, long long max_plane,
                         int parity, cudaStream_t st);
+// ghost planes of one slot of a windowed run: from the neighbouring slots'
+// planes (lo / hi) or, where they are null, the domain's z boundary condition
+cudaError_t launch_window_ghosts(int esz, void* dst, const void* lo, const void* hi, long long fs, long long plane,
+                                 int nz, int bc_lo, int bc_hi, cudaStream_t st);
 cudaError_t launch_update(int is_double, const DomDev* doms, int ndom, int parity, double b, cudaStream_t st);
 cudaError_t launch_fma_probe(int blocks, int iters, float* out, cudaStream_t st);
 cudaError_t launch_sum_state(const DomDev* doms, int ndom, int parity, int nchunks, int chunk, int is_double,

@@ -94,6 +94,10 @@ SIGNATURES = {
     "mpcf_step": (_I, [_P, _D, _D, _PD]),
     "mpcf_run": (_I, [_P, _I, _D, _D, _I, _PD]),
     "mpcf_run_host": (_I, [_P, _I, _D, _D, _PP, _I, _PD]),
+    "mpcf_create_window": (_I, [_PP, _I, _I, _I, _I, _I, _I, _PI, _I]),
+    "mpcf_run_window": (_I, [_P, _I, _D, _D, _PP, _PD]),
+    "mpcf_window_info": (_I, [_P, _PI]),
+    "mpcf_window_plan": (_I, [_I, _I, _I, _PI, _I]),
     "mpcf_synchronize": (_I, [_P]),
     "mpcf_stream": (_I, [_P, _PP]),
     "mpcf_sos_accumulator": (_I, [_P, _PP]),

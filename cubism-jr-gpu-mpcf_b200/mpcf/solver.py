@@ -422,6 +422,57 @@ def bubbles(seed, n, rmin, rmax, lo=(0.2, 0.2, 0.2), hi=(0.8, 0.8, 0.8), gap=0.0
 LSRK3 = ((0.0, 1.0 / 4), (-17.0 / 32, 8.0 / 9), (-32.0 / 27, 3.0 / 4))
 
 
+class WindowSolver(Solver):
+    """A domain of nx*ny*nz cells held in host memory, possibly larger than
+    the device's, advanced by streaming z-chunks of `nslices` planes through
+    `nslots` device slots (mpcf_create_window / mpcf_run_window; the
+    reference's GPUlab with nslices < sizeZ, GPUlab.cpp:37-41,202-372).
+    nslices >= 3 divides nz; nslots >= min(5, nz / nslices).  Only `run`
+    advances it."""
+
+    def __init__(self, dims, nslices, nslots=8, bc=None, precision="fp32_ref", device=0):
+        if isinstance(precision, str):
+            precision = _lib.PRECISIONS[precision]
+        nx, ny, nz = (int(v) for v in dims)
+        bcarr = None if bc is None else (ctypes.c_int * 6)(*[int(v) for v in bc])
+        h = ctypes.c_void_p()
+        check(lib().mpcf_create_window(ctypes.byref(h), nx, ny, nz, int(nslices), int(nslots), precision, bcarr, device))
+        self._h = h
+        self.device = int(device)
+        self.precision = precision
+        self.dtype = dtype_of(precision)
+        info = (ctypes.c_int * 4)()
+        check(lib().mpcf_window_info(self._h, info))
+        self.global_dims = (nx, ny, nz)
+        self.nslices, self.nchunks, self.nslots = info[1], info[2], info[3]
+        self.dims = [(nx, ny, self.nslices)] * self.nslots
+        self.ndom = self.nslots
+
+    def run(self, host_state, nsteps, cfl=0.3, dt_max=1e30):
+        """nsteps steps of `host_state` (7 contiguous arrays of nx*ny*nz of
+        the solver's dtype, page-locked for overlap), overwritten with each
+        step's result.  Returns the time."""
+        n = self.global_dims[0] * self.global_dims[1] * self.global_dims[2]
+        for a in host_state:
+            if a.dtype != self.dtype or not a.flags["C_CONTIGUOUS"] or a.size != n:
+                raise ValueError("host fields must be contiguous arrays of the solver's dtype and the domain's size")
+        t = ctypes.c_double()
+        check(lib().mpcf_run_window(self._h, int(nsteps), float(cfl), float(dt_max), _ptr_array(host_state),
+                                    ctypes.byref(t)))
+        return t.value
+
+
+def window_plan(nchunks, nslots, nsteps):
+    """The operations of a windowed run in enqueue order (mpcf_window_plan,
+    no device work): an int array of rows (kind, step, stage, chunk), kind 0
+    upload, 1 sound speed of the first step's input, 2 dt, 3 stage, 4
+    download; step -1 is the sound-speed pass."""
+    n = check(lib().mpcf_window_plan(int(nchunks), int(nslots), int(nsteps), None, 0))
+    buf = (ctypes.c_int * (4 * max(n, 1)))()
+    check(lib().mpcf_window_plan(int(nchunks), int(nslots), int(nsteps), buf, n))
+    return np.frombuffer(buf, dtype=np.int32)[:4 * n].reshape(n, 4).copy()
+
+
 class GPUlab:
     """Reference-shaped lab over a single-domain Solver (GPUlab.h:250-258).
 

@@ -156,6 +156,43 @@ int mpcf_run(mpcf_solver* s, int nsteps, double cfl, double dt_max, int use_grap
  * tracking is not applied.  time_out (optional): the time. */
 int mpcf_run_host(mpcf_solver* s, int nsteps, double cfl, double dt_max, void* const* host7, int nchunks,
                   double* time_out);
+/* Windowed runs: a domain held in host memory that may be larger than the
+ * device's, streamed through a few device slots in z-chunks of nslices
+ * planes (the reference's GPUlab with nslices < sizeZ: chunks of nslices
+ * planes with 3-plane overlaps streamed through the GPU every stage,
+ * GPUlab.cpp:37-41 (nslices must divide sizeZ), 202-372, 703-793).
+ * mpcf_create_window: a solver of min(nslots, nz/nslices) slots, each an
+ *   nx*ny*nslices domain with 3 stored ghost planes on each z side (device
+ *   memory of a slot: 3 buffers of nx*ny*(nslices+6) cells of 7 fields);
+ *   bc6: the domain's faces (absorbing or reflecting; null: absorbing).
+ *   nslices >= 3 must divide nz; nslots >= min(5, nz/nslices): a stage 3 of
+ *   chunk c needs chunks c-1 .. c+3 resident.  Only mpcf_run_window advances
+ *   it (the stepping calls return MPCF_ERR_STATE); set_tiling applies to the
+ *   slots.
+ * mpcf_run_window: nsteps LSRK3 steps of host7 (7 fields of nx*ny*nz, x
+ *   fastest; page-locked memory lets copies overlap), overwritten with each
+ *   step's result.  Chunk c goes through slot c % nslots: its upload, the
+ *   three stages as a wavefront over the chunks (a stage of chunk c runs once
+ *   the stage before it covers chunk c+1; before each stage a kernel fills
+ *   the slot's ghost planes from the neighbouring slots, or by the boundary
+ *   condition at the domain's z faces), and its download, on two copy
+ *   streams and the solver's stream.  The first step's dt comes from a pass
+ *   that streams every chunk through the slots and reduces its sound speed;
+ *   later steps take what stage 3 accumulated.  Results are bit-identical
+ *   to mpcf_run of the whole domain on one device.  time_out (optional): the
+ *   time.
+ * mpcf_window_info: {nz, nslices, chunks, slots} of a windowed solver.
+ * mpcf_window_plan: the operations of a windowed run in enqueue order (no
+ *   device work): ops4[4 i .. 4 i + 3] = {kind (0 upload, 1 sound speed of
+ *   the first step's input, 2 dt, 3 stage, 4 download), step (-1: the
+ *   sound-speed pass), stage (0..2), chunk}, at most cap entries written;
+ *   returns the number of operations, or MPCF_ERR_ARG when the slots are
+ *   too few. */
+int mpcf_create_window(mpcf_solver** out, int nx, int ny, int nz, int nslices, int nslots, int precision,
+                       const int* bc6, int device);
+int mpcf_run_window(mpcf_solver* s, int nsteps, double cfl, double dt_max, void* const* host7, double* time_out);
+int mpcf_window_info(const mpcf_solver* s, int* info4);
+int mpcf_window_plan(int nchunks, int nslots, int nsteps, int* ops4, int cap);
 int mpcf_synchronize(mpcf_solver* s);
 /* Stream-ordered building blocks of a step, for a driver that orders its
  * own work with the solver's kernels: the reference's per-rank step with
