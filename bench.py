@@ -368,6 +368,8 @@ def main():
                     help="precision of the headline run (profiling of the other forms)")
     ap.add_argument("--workload", default=WORKLOAD)
     ap.add_argument("--e2e-chunks", type=int, default=16, help="z-chunks of the streamed e2e run")
+    ap.add_argument("--window-slots", type=int, default=6,
+                    help="device slots of the windowed e2e run (0: skip it)")
     args = ap.parse_args()
     if args.impl == "reference":
         return reference_arm(args)
@@ -453,7 +455,7 @@ def main():
     e2e = None
     if not args.no_e2e:
         e2e = e2e_measure(mpcf, cfg, K=K, W=W, cfl=cfl, dist=dist, precision=args.precision, tiling=tiling,
-                          nchunks=args.e2e_chunks)
+                          nchunks=args.e2e_chunks, window_slots=args.window_slots)
     # the same for the drop-in form (FP32 reference rounding, bit-identical
     # to the reference's arithmetic), on its own tiling
     e2e_drop_in = None
@@ -583,7 +585,37 @@ def pcie_peak(nbytes=1 << 30, chunks=16, reps=5):
     return out
 
 
-def e2e_measure(mpcf, cfg, K, W, cfl, dist, precision="mixed", tiling=None, nchunks=16, serial_form=True):
+def window_measure(mpcf, cfg, K, W, cfl, dist, precision, tiling, host, nslots, nslices=32):
+    """The same steps through a windowed solver (mpcf_run_window): the
+    domain streamed through `nslots` device slots of `nslices` planes, as a
+    domain larger than device memory runs; each call's first step adds a
+    pass that streams the state once more for its sound speed."""
+    import mpcf.replicas as rp
+    dims = cfg["dims"][0]
+    ncell = dims[0] * dims[1] * dims[2]
+    with mpcf.WindowSolver(dims, nslices, nslots, precision=precision) as w:
+        if tiling is not None:
+            w.set_tiling(tiling[0], nslices, tiling[2], tiling[3])
+        w.run(host, W, cfl=cfl)
+        import torch
+        if dist is not None:
+            dist.barrier()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        w.run(host, K, cfl=cfl)
+        torch.cuda.synchronize()
+        sec = time.perf_counter() - t0
+        esz = 8 if precision in ("fp64", "fp64_fast") else 4
+        slot_bytes = 3 * 7 * esz * dims[0] * dims[1] * (nslices + 6)
+        v, _ = rp.throughput(dist, ncell, 3.0 * K, sec * 1e3, device="cuda" if dist is not None else None)
+        return {"value": v, "unit": UNIT, "ms_per_step": sec * 1e3 / K, "nslices": nslices, "slots": w.nslots,
+                "device_bytes": w.nslots * slot_bytes, "resident_bytes": 3 * 7 * esz * ncell,
+                "path": f"mpcf_run_window: {w.nchunks} chunks of {nslices} planes through {w.nslots} device slots, "
+                        f"host wall clock over one call of {K} steps"}
+
+
+def e2e_measure(mpcf, cfg, K, W, cfl, dist, precision="mixed", tiling=None, nchunks=16, serial_form=True,
+                window_slots=0):
     """Same metric through the C ABI with the state in page-locked host
     memory, as the reference keeps it: every step reads its input state from
     the host buffers and writes its result back to them (mpcf_run_host: z-chunk
@@ -642,6 +674,11 @@ def e2e_measure(mpcf, cfg, K, W, cfl, dist, precision="mixed", tiling=None, nchu
                            "peak": pk["both_gbs_per_direction"], "unit": "GB/s per direction",
                            "frac": bound_ms / step_ms, "bound_ms_per_step": bound_ms, "ms_per_step": step_ms,
                            "copies": pk}
+        if window_slots:
+            try:
+                out["window"] = window_measure(mpcf, cfg, K, W, cfl, dist, precision, tiling, host, window_slots)
+            except mpcf.MpcfError as e:
+                out["window"] = {"error": str(e)}
 
     def serial(k):
         for _ in range(k):

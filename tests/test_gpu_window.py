@@ -110,3 +110,57 @@ def test_window_run_512cube(mpcf):
     assert t == t_res, (t, t_res)
     for q in range(7):
         assert np.array_equal(arrs[q], U_res[q]), q
+
+
+def test_window_run_larger_than_device_memory(mpcf):
+    """A 1344^3 FP32 cloud (2.43e9 cells): its two state buffers and the
+    register would take 204 GB on the device, more than the B200's 192 GB;
+    the windowed run streams it in 42 chunks of 32 planes through 6 slots
+    (34.6 GB).  One step of the 200-bubble cloud (generated chunk by chunk
+    in the global domain's coordinates); the planes of three z-windows (at
+    the bottom face, across a chunk boundary in the middle, at the top face)
+    are compared bit for bit with a resident run of each window and the 9
+    planes beside it (a stage reads 3 planes beyond a cell), advanced with
+    the windowed run's dt."""
+    import psutil
+    import torch
+    n1 = 1344
+    dims = (n1, n1, n1)
+    N = n1 ** 3
+    plane = n1 * n1
+    if psutil.virtual_memory().available < 120e9:
+        pytest.skip("needs 120 GB of free host memory")
+    if 3 * 7 * 4 * N <= torch.cuda.mem_get_info()[1]:
+        pytest.skip("the domain would fit on this device")
+    cfg = mpcf.configs.config("c3_512")
+    host = [torch.empty(N, dtype=torch.float32, pin_memory=True) for _ in range(7)]
+    arrs = [h.numpy() for h in host]
+    T = 32
+    with mpcf.Solver([(n1, n1, T)], precision="mixed") as g:
+        for z0 in range(0, n1, T):
+            g.set_origin((0, 0, z0), dims)
+            g.ic_cloud(cfg["params"], cfg["bubbles"][0])
+            st = g.get_state(with_reg=False)
+            for q in range(7):
+                arrs[q][z0 * plane:(z0 + T) * plane] = st[q]
+    margin = 9
+    slabs = []
+    for z0, z1 in ((0, 32), (656, 688), (n1 - 32, n1)):
+        lo, hi = max(0, z0 - margin), min(n1, z1 + margin)
+        slabs.append((z0, z1, lo, hi, [a[lo * plane:hi * plane].copy() for a in arrs]))
+    with mpcf.WindowSolver(dims, T, 6, precision="mixed") as w:
+        w.set_tiling(8, 32, True, True)
+        t = w.run(arrs, 1, cfl=0.3)
+        assert w.error_word() == 0
+    dtinvh = float(np.float32(t / (1.0 / n1)))
+    for z0, z1, lo, hi, U0 in slabs:
+        with mpcf.Solver([(n1, n1, hi - lo)], precision="mixed") as s:
+            s.set_tiling(8, 32, True, True)
+            s.set_state(U0)
+            for a, b in mpcf.LSRK3:
+                s.stage(a, b, dtinvh)
+            U = s.get_state(with_reg=False)
+            assert s.error_word() == 0
+        sl = slice((z0 - lo) * plane, (z1 - lo) * plane)
+        for q in range(7):
+            assert np.array_equal(U[q][sl], arrs[q][z0 * plane:z1 * plane]), (z0, q)
