@@ -367,7 +367,7 @@ def main():
     ap.add_argument("--precision", default="mixed", choices=["mixed", "fp32", "fp32_ref", "fp64", "fp64_fast"],
                     help="precision of the headline run (profiling of the other forms)")
     ap.add_argument("--workload", default=WORKLOAD)
-    ap.add_argument("--e2e-chunks", type=int, default=16, help="z-chunks of the streamed e2e run")
+    ap.add_argument("--e2e-chunks", type=int, default=8, help="z-chunks of the streamed e2e run")
     ap.add_argument("--window-slots", type=int, default=6,
                     help="device slots of the windowed e2e run (0: skip it)")
     args = ap.parse_args()
@@ -614,7 +614,7 @@ def window_measure(mpcf, cfg, K, W, cfl, dist, precision, tiling, host, nslots, 
                         f"host wall clock over one call of {K} steps"}
 
 
-def e2e_measure(mpcf, cfg, K, W, cfl, dist, precision="mixed", tiling=None, nchunks=16, serial_form=True,
+def e2e_measure(mpcf, cfg, K, W, cfl, dist, precision="mixed", tiling=None, nchunks=8, serial_form=True,
                 window_slots=0):
     """Same metric through the C ABI with the state in page-locked host
     memory, as the reference keeps it: every step reads its input state from
