@@ -1353,6 +1353,7 @@ int mpcf_link_z(mpcf_solver* s, int lower, int upper)
     Range nvtx("mpcf_link_z");
     int rc = check_dom(s, lower);
     if (rc) return rc;
+    if (s->win_nch) return window_only(s, "mpcf_link_z");
     if ((rc = check_dom(s, upper))) return rc;
     if (lower == upper) return fail(MPCF_ERR_ARG, "a domain cannot be linked to itself");
     const DomDev& L = s->hdoms[lower];

@@ -167,8 +167,8 @@ int mpcf_run_host(mpcf_solver* s, int nsteps, double cfl, double dt_max, void* c
  *   bc6: the domain's faces (absorbing or reflecting; null: absorbing).
  *   nslices >= 3 must divide nz; nslots >= min(5, nz/nslices): a stage 3 of
  *   chunk c needs chunks c-1 .. c+3 resident.  Only mpcf_run_window advances
- *   it (the stepping calls return MPCF_ERR_STATE); set_tiling applies to the
- *   slots.
+ *   it (the stepping calls and mpcf_link_z return MPCF_ERR_STATE);
+ *   set_tiling applies to the slots.
  * mpcf_run_window: nsteps LSRK3 steps of host7 (7 fields of nx*ny*nz, x
  *   fastest; page-locked memory lets copies overlap), overwritten with each
  *   step's result.  Chunk c goes through slot c % nslots: its upload, the

@@ -78,7 +78,8 @@ def test_window_rejects_what_it_cannot_run(mpcf):
     with pytest.raises(mpcf.MpcfError, match="boundary condition"):
         mpcf.WindowSolver(dims, 8, 5, bc=(0, 0, 0, 0, 2, 0))
     with mpcf.WindowSolver(dims, 8, 5) as w:
-        for call in (lambda: w.step(cfl=0.3), lambda: w.stage(0.0, 0.25, 0.01), lambda: mpcf.Solver.run(w, 1)):
+        for call in (lambda: w.step(cfl=0.3), lambda: w.stage(0.0, 0.25, 0.01), lambda: mpcf.Solver.run(w, 1),
+                     lambda: w.link_z(0, 1)):
             with pytest.raises(mpcf.MpcfError, match="windowed"):
                 call()
         with pytest.raises(ValueError):
