@@ -20,6 +20,7 @@
 #include <random>
 #include <string>
 #include <vector>
+#include <limits>
 
 #include "../../include/mpcf_b200.h"
 #include "mpcf_types.h"
@@ -672,6 +673,7 @@ int mpcf_max_sos(mpcf_solver* s, double* sos)
 {
     Range nvtx("mpcf_max_sos");
     if (!s) return fail(MPCF_ERR_ARG, "null solver");
+    if (s->win_nch) return window_only(s, "mpcf_max_sos");
     DeviceGuard g(s->device);
     s->sos_fresh = false;                   // the state (or the accumulator) changes
     int rc = enqueue_sos(s);
@@ -1076,6 +1078,82 @@ bool window_plan(const int nch, const int ns, const int nsteps, std::vector<WinO
     return true;
 }
 
+// The plan of one stage of a block whose state and register live in host
+// memory (mpcf_window_stage, the reference's process_all over nslices
+// chunks): chunk c's state and register go into slot c % ns, its stage runs
+// once chunk c+1 is there (its upper ghost planes), then both come back; a
+// slot takes its next chunk once its chunk was downloaded and the stage of
+// the chunk above, which reads its top planes, is queued.
+bool window_stage_plan(const int nch, const int ns, std::vector<WinOp>& plan)
+{
+    plan.clear();
+    if (nch < 1 || ns < 1) return false;
+    int up = 0, st = 0, dn = 0;
+    std::vector<int> occ(ns, -1);
+    std::vector<char> busy(ns, 0);
+    auto released = [&](const int j) { return st > (j == nch - 1 ? j : j + 1) && dn > j; };
+    while (dn < nch)
+    {
+        for (int k = 0; k < ns; ++k)
+            if (busy[k] && released(occ[k])) busy[k] = 0;
+        if (st > dn) { plan.push_back({WOP_DOWNLOAD, 0, 0, dn++}); continue; }
+        if (st < nch && up > std::min(st + 1, nch - 1)) { plan.push_back({WOP_STAGE, 0, 0, st++}); continue; }
+        if (up < nch && !busy[up % ns])
+        {
+            busy[up % ns] = 1;
+            occ[up % ns] = up;
+            plan.push_back({WOP_UPLOAD, 0, 0, up++});
+            continue;
+        }
+        return false;
+    }
+    return true;
+}
+
+// Streams and events of a windowed call, made on first use; the slots'
+// last use by work already queued on the solver's stream frees them.
+int window_begin(mpcf_solver* s)
+{
+    const int nch = s->win_nch, ns = s->ndom;
+    if (!s->up)
+    {
+        CK(cudaStreamCreateWithFlags(&s->up, cudaStreamNonBlocking));
+        CK(cudaStreamCreateWithFlags(&s->down, cudaStreamNonBlocking));
+        CK(cudaEventCreateWithFlags(&s->ev_start, cudaEventDisableTiming));
+    }
+    auto grow = [&](std::vector<cudaEvent_t>& v, const int n)
+    {
+        while ((int)v.size() < n)
+        {
+            cudaEvent_t e;
+            if (cudaEventCreateWithFlags(&e, cudaEventDisableTiming) != cudaSuccess) return false;
+            v.push_back(e);
+        }
+        return true;
+    };
+    if (!grow(s->ev_up, nch) || !grow(s->ev_st, nch) || !grow(s->ev_free_c, ns) || !grow(s->ev_free_d, ns))
+    { cudaGetLastError(); return fail(MPCF_ERR_CUDA, "cudaEventCreate failed"); }
+    CK(cudaEventRecord(s->ev_start, s->stream));
+    CK(cudaStreamWaitEvent(s->up, s->ev_start, 0));
+    CK(cudaStreamWaitEvent(s->down, s->ev_start, 0));
+    for (int k = 0; k < ns; ++k)
+    {
+        CK(cudaEventRecord(s->ev_free_c[k], s->stream));
+        CK(cudaEventRecord(s->ev_free_d[k], s->down));
+    }
+    return MPCF_OK;
+}
+
+int window_end(mpcf_solver* s)
+{
+    s->sos_fresh = false;
+    s->sums_valid = false;
+    CK(cudaStreamSynchronize(s->down));
+    CK(cudaStreamSynchronize(s->up));
+    CK(cudaStreamSynchronize(s->stream));
+    return MPCF_OK;
+}
+
 } // namespace
 
 int mpcf_window_plan(int nchunks, int nslots, int nsteps, int* ops4, int cap)
@@ -1286,6 +1364,135 @@ int mpcf_run_window(mpcf_solver* s, int nsteps, double cfl, double dt_max, void*
     return MPCF_OK;
 }
 
+int mpcf_window_stage(mpcf_solver* s, double a, double b, double dtinvh, void* const* state7, void* const* reg7)
+{
+    Range nvtx("mpcf_window_stage");
+    if (!s) return fail(MPCF_ERR_ARG, "null solver");
+    if (!s->win_nch) return fail(MPCF_ERR_STATE, "mpcf_window_stage needs a windowed solver (mpcf_create_window)");
+    if (!state7 || !reg7) return fail(MPCF_ERR_ARG, "null host state or register");
+    for (int q = 0; q < 7; ++q)
+        if (!state7[q] || !reg7[q]) return fail(MPCF_ERR_ARG, "host field %d is null", q);
+    const int nch = s->win_nch, ns = s->ndom, nsl = s->win_nslices;
+    std::vector<WinOp> plan;
+    if (!window_stage_plan(nch, ns, plan)) return fail(MPCF_ERR_STATE, "window stage plan stalled (%d slots, %d chunks)", ns, nch);
+    DeviceGuard g(s->device);
+    int rc;
+    // dt/h of the stage for every slot
+    CK(cudaStreamSynchronize(s->stream));   // host staging buffer reuse
+    for (int d = 0; d < ns; ++d)
+    {
+        if (s->esz == 8) ((double*)s->host_stage)[d] = dtinvh;
+        else ((float*)s->host_stage)[d] = (float)dtinvh;
+    }
+    CK(cudaMemcpyAsync(s->dtinvh, s->host_stage, s->esz * ns, cudaMemcpyHostToDevice, s->stream));
+    if ((rc = window_begin(s))) return rc;
+    const long long plane = (long long)s->hdoms[0].nx * s->hdoms[0].ny;
+    const size_t esz = s->esz;
+    const size_t cbytes = (size_t)nsl * plane * esz;
+    const long long fs = s->hdoms[0].fs;
+    const int p = s->parity;
+    for (const WinOp& o : plan)
+    {
+        const int c = o.chunk, slot = c % ns;
+        DomDev& D = s->hdoms[slot];
+        const size_t off = (size_t)c * cbytes;
+        if (o.op == WOP_UPLOAD)
+        {
+            CK(cudaStreamWaitEvent(s->up, s->ev_free_c[slot], 0));
+            CK(cudaStreamWaitEvent(s->up, s->ev_free_d[slot], 0));
+            for (int q = 0; q < 7; ++q)
+            {
+                CK(cudaMemcpyAsync((char*)D.U[p] + (size_t)q * fs * esz, (const char*)state7[q] + off, cbytes,
+                                   cudaMemcpyHostToDevice, s->up));
+                CK(cudaMemcpyAsync((char*)D.R + (size_t)q * fs * esz, (const char*)reg7[q] + off, cbytes,
+                                   cudaMemcpyHostToDevice, s->up));
+            }
+            CK(cudaEventRecord(s->ev_up[c], s->up));
+        }
+        else if (o.op == WOP_STAGE)
+        {
+            CK(cudaStreamWaitEvent(s->stream, s->ev_up[std::min(c + 1, nch - 1)], 0));
+            const void* lo = c > 0 ? s->hdoms[(c - 1) % ns].U[p] : nullptr;
+            const void* hi = c < nch - 1 ? s->hdoms[(c + 1) % ns].U[p] : nullptr;
+            CK(launch_window_ghosts((int)esz, D.U[p], lo, hi, fs, plane, nsl, s->win_bc[0], s->win_bc[1], s->stream));
+            if ((rc = enqueue_stage_tiles(s, a, b, false, false, D.tile_begin, D.tile_begin + D.tiles_x * D.tiles_y * D.tiles_z)))
+                return rc;
+            CK(cudaEventRecord(s->ev_st[c], s->stream));
+            if (c > 0) CK(cudaEventRecord(s->ev_free_c[(c - 1) % ns], s->stream));
+            if (c == nch - 1) CK(cudaEventRecord(s->ev_free_c[slot], s->stream));
+        }
+        else
+        {
+            CK(cudaStreamWaitEvent(s->down, s->ev_st[c], 0));
+            for (int q = 0; q < 7; ++q)
+            {
+                CK(cudaMemcpyAsync((char*)state7[q] + off, (const char*)D.U[p ^ 1] + (size_t)q * fs * esz, cbytes,
+                                   cudaMemcpyDeviceToHost, s->down));
+                CK(cudaMemcpyAsync((char*)reg7[q] + off, (const char*)D.R + (size_t)q * fs * esz, cbytes,
+                                   cudaMemcpyDeviceToHost, s->down));
+            }
+            CK(cudaEventRecord(s->ev_free_d[slot], s->down));
+        }
+    }
+    return window_end(s);
+}
+
+int mpcf_window_max_sos(mpcf_solver* s, const void* const* state7, double* sos)
+{
+    Range nvtx("mpcf_window_max_sos");
+    if (!s) return fail(MPCF_ERR_ARG, "null solver");
+    if (!s->win_nch) return fail(MPCF_ERR_STATE, "mpcf_window_max_sos needs a windowed solver (mpcf_create_window)");
+    if (!state7) return fail(MPCF_ERR_ARG, "null host state");
+    for (int q = 0; q < 7; ++q) if (!state7[q]) return fail(MPCF_ERR_ARG, "host field %d is null", q);
+    const int nch = s->win_nch, ns = s->ndom, nsl = s->win_nslices;
+    DeviceGuard g(s->device);
+    int rc;
+    if ((rc = window_begin(s))) return rc;
+    const long long plane = (long long)s->hdoms[0].nx * s->hdoms[0].ny;
+    const size_t esz = s->esz;
+    const size_t cbytes = (size_t)nsl * plane * esz;
+    const long long fs = s->hdoms[0].fs;
+    const int p = s->parity;
+    CK(cudaMemsetAsync(s->sos_bits, 0, esz * ns, s->stream));
+    for (int c = 0; c < nch; ++c)
+    {
+        const int slot = c % ns;
+        DomDev& D = s->hdoms[slot];
+        CK(cudaStreamWaitEvent(s->up, s->ev_free_c[slot], 0));
+        for (int q = 0; q < 7; ++q)
+            CK(cudaMemcpyAsync((char*)D.U[p] + (size_t)q * fs * esz, (const char*)state7[q] + (size_t)c * cbytes, cbytes,
+                               cudaMemcpyHostToDevice, s->up));
+        CK(cudaEventRecord(s->ev_up[c], s->up));
+        CK(cudaStreamWaitEvent(s->stream, s->ev_up[c], 0));
+        SosArgs A;
+        A.doms = s->ddoms;
+        A.ndom = ns;
+        A.nchunks = D.sos_chunks;
+        A.chunk = s->sos_chunk;
+        A.chunk0 = D.sos_chunk_begin;
+        A.parity = p;
+        A.sos_bits = s->sos_bits;
+        CK(launch_sos(s->pol, A, s->stream));
+        CK(cudaEventRecord(s->ev_free_c[slot], s->stream));
+    }
+    std::vector<char> buf(esz * ns);
+    CK(cudaMemcpyAsync(buf.data(), s->sos_bits, buf.size(), cudaMemcpyDeviceToHost, s->stream));
+    CK(cudaMemsetAsync(s->sos_bits, 0, esz * ns, s->stream));
+    if ((rc = window_end(s))) return rc;
+    // the largest over the slots; a NaN anywhere (its bit pattern orders
+    // above every finite value in the device's maximum) stays NaN
+    double m = 0;
+    bool nan = false;
+    for (int d = 0; d < ns; ++d)
+    {
+        const double v = esz == 8 ? ((double*)buf.data())[d] : (double)((float*)buf.data())[d];
+        if (v != v) nan = true;
+        else if (v > m) m = v;
+    }
+    if (sos) *sos = nan ? std::numeric_limits<double>::quiet_NaN() : m;
+    return MPCF_OK;
+}
+
 int mpcf_synchronize(mpcf_solver* s)
 {
     if (!s) return fail(MPCF_ERR_ARG, "null solver");
@@ -1334,6 +1541,23 @@ int mpcf_set_bc(mpcf_solver* s, int dom, const int* bc6)
     int rc = check_dom(s, dom);
     if (rc) return rc;
     if (!bc6) return fail(MPCF_ERR_ARG, "null bc");
+    if (s->win_nch)
+    {
+        // a windowed solver: the domain's faces; x/y go to every slot, z to
+        // the ghost planes at the domain's own z faces
+        if (dom != 0) return fail(MPCF_ERR_ARG, "a windowed solver has one domain (index 0)");
+        for (int f = 0; f < 6; ++f)
+            if (bc6[f] != MPCF_BC_ABSORBING && bc6[f] != MPCF_BC_REFLECTING)
+                return fail(MPCF_ERR_ARG, "boundary condition %d on face %d: absorbing or reflecting", bc6[f], f);
+        DeviceGuard g(s->device);
+        for (int d = 0; d < s->ndom; ++d)
+            for (int f = 0; f < 4; ++f) s->hdoms[d].bc[f] = bc6[f];
+        s->win_bc[0] = bc6[4];
+        s->win_bc[1] = bc6[5];
+        CK(cudaMemcpyAsync(s->ddoms, s->hdoms.data(), sizeof(DomDev) * s->ndom, cudaMemcpyHostToDevice, s->stream));
+        CK(cudaStreamSynchronize(s->stream));
+        return MPCF_OK;
+    }
     for (int f = 0; f < 6; ++f)
     {
         if (bc6[f] != MPCF_BC_ABSORBING && bc6[f] != MPCF_BC_REFLECTING && bc6[f] != MPCF_BC_HALO)

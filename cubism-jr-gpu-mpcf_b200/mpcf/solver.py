@@ -462,6 +462,27 @@ class WindowSolver(Solver):
         return t.value
 
 
+    def stage_host(self, host_state, host_reg, a, b, dtinvh):
+        """One stage of a block whose state and register both live in host
+        memory (mpcf_window_stage), both overwritten."""
+        n = self.global_dims[0] * self.global_dims[1] * self.global_dims[2]
+        for arr in list(host_state) + list(host_reg):
+            if arr.dtype != self.dtype or not arr.flags["C_CONTIGUOUS"] or arr.size != n:
+                raise ValueError("host fields must be contiguous arrays of the solver's dtype and the domain's size")
+        check(lib().mpcf_window_stage(self._h, float(a), float(b), float(dtinvh), _ptr_array(host_state),
+                                      _ptr_array(host_reg)))
+
+    def max_sos_host(self, host_state):
+        """The largest sound speed of a host-resident state (mpcf_window_max_sos)."""
+        out = ctypes.c_double()
+        check(lib().mpcf_window_max_sos(self._h, _ptr_array(host_state), ctypes.byref(out)))
+        return out.value
+
+    def set_bc(self, bc6, dom=0):
+        """The block's six faces (absorbing or reflecting)."""
+        check(lib().mpcf_set_bc(self._h, 0, (ctypes.c_int * 6)(*[int(v) for v in bc6])))
+
+
 def window_plan(nchunks, nslots, nsteps):
     """The operations of a windowed run in enqueue order (mpcf_window_plan,
     no device work): an int array of rows (kind, step, stage, chunk), kind 0

@@ -93,7 +93,8 @@ bool GPUlab::Halo::untouched() const
 GPUlab::GPUlab(GridMPI& G, const uint_t nslices_, const int verbosity)
     : grid(G), halox(3 * sizeY * sizeZ), haloy(sizeX * 3 * sizeZ), haloz(sizeX * sizeY * 3),
       nslices(nslices_), m_verbosity(verbosity), m_solver(nullptr), m_bc_dirty(false), m_host_sync(true),
-      m_ghost_calls(0), m_check_halos(getenv("MPCF_CHECK_HALOS") && atoi(getenv("MPCF_CHECK_HALOS")) != 0)
+      m_ghost_calls(0), m_check_halos(getenv("MPCF_CHECK_HALOS") && atoi(getenv("MPCF_CHECK_HALOS")) != 0),
+      m_window(false)
 {
     // the reference's configuration checks and messages (GPUlab.cpp:37-47)
     if (nslices_ == 0 || sizeZ % nslices_ != 0)
@@ -112,7 +113,19 @@ GPUlab::GPUlab(GridMPI& G, const uint_t nslices_, const int verbosity)
 
     const int dims[3] = {(int)sizeX, (int)sizeY, (int)sizeZ};
     const int dev = getenv("MPCF_DEVICE") ? atoi(getenv("MPCF_DEVICE")) : 0;
-    GPU::check(mpcf_create(&m_solver, 1, dims, m_bc, precision_for_real(), dev), "GPUlab: mpcf_create");
+    // device resident when the block fits; otherwise (or on request)
+    // windowed through a few slots of nslices planes, as the reference streams
+    const bool want_window = getenv("MPCF_GPULAB_WINDOW") && atoi(getenv("MPCF_GPULAB_WINDOW")) != 0 && nslices_ < sizeZ;
+    int rc = want_window ? MPCF_ERR_NOMEM : mpcf_create(&m_solver, 1, dims, m_bc, precision_for_real(), dev);
+    if (rc == MPCF_ERR_NOMEM && nslices_ < sizeZ)
+    {
+        const int slots = getenv("MPCF_GPULAB_SLOTS") ? atoi(getenv("MPCF_GPULAB_SLOTS")) : 6;
+        rc = mpcf_create_window(&m_solver, (int)sizeX, (int)sizeY, (int)sizeZ, (int)nslices_, slots,
+                                precision_for_real(), m_bc, dev);
+        m_window = rc == MPCF_OK;
+        m_host_sync = true;
+    }
+    GPU::check(rc, "GPUlab: mpcf_create");
 #ifdef _WENO3_
     // the reference's compile-time WENO3 build (GPUonly.cuh:102,141)
     GPU::check(mpcf_set_weno_order(m_solver, 3), "GPUlab: WENO3");
@@ -129,7 +142,13 @@ GPUlab::GPUlab(GridMPI& G, const uint_t nslices_, const int verbosity)
     }
     upload();
     if (m_verbosity)
-        printf("[GPUlab: %ux%ux%u block device resident, precision %d]\n", sizeX, sizeY, sizeZ, precision_for_real());
+    {
+        if (m_window)
+            printf("[GPUlab: %ux%ux%u block streamed in chunks of %u slices, precision %d]\n", sizeX, sizeY, sizeZ,
+                   (unsigned)nslices_, precision_for_real());
+        else
+            printf("[GPUlab: %ux%ux%u block device resident, precision %d]\n", sizeX, sizeY, sizeZ, precision_for_real());
+    }
 }
 
 GPUlab::~GPUlab()
@@ -150,6 +169,7 @@ void GPUlab::record_bc_face(const int face, const int type)
 
 void GPUlab::upload()
 {
+    if (m_window) return;   // the host copy is the block; it streams per call
     const void* st[7];
     const void* rg[7];
     for (int q = 0; q < 7; ++q) { st[q] = grid.pdata()[q]; rg[q] = grid.ptmp()[q]; }
@@ -158,6 +178,7 @@ void GPUlab::upload()
 
 void GPUlab::download()
 {
+    if (m_window) return;
     void* st[7];
     void* rg[7];
     for (int q = 0; q < 7; ++q) { st[q] = grid.pdata()[q]; rg[q] = grid.ptmp()[q]; }
@@ -191,10 +212,18 @@ void GPUlab::load_ghosts(const double t)
 double GPUlab::max_sos(float& sos)
 {
     const double t0 = now_s();
+    double s = 0;
+    if (m_window)
+    {
+        const void* st[7];
+        for (int q = 0; q < 7; ++q) st[q] = grid.pdata()[q];
+        GPU::check(mpcf_window_max_sos(m_solver, st, &s), "GPUlab: max_sos");
+        sos = (float)s;
+        return now_s() - t0;
+    }
     // the reference reads the host state for the reduction (GPUlab.cpp:671);
     // with host synchronisation the host register is current too, so both go up
     if (m_host_sync) upload();
-    double s = 0;
     GPU::check(mpcf_max_sos(m_solver, &s), "GPUlab: max_sos");
     sos = (float)s;
     return now_s() - t0;
@@ -203,8 +232,18 @@ double GPUlab::max_sos(float& sos)
 double GPUlab::process_all(const Real a, const Real b, const Real dtinvh)
 {
     const double t0 = now_s();
-    if (m_host_sync) upload();
     const double dt = (double)dtinvh;
+    if (m_window)
+    {
+        // the reference's chunked process_all (GPUlab.cpp:703-793): every
+        // chunk's state and register through the device and back
+        void* st[7];
+        void* rg[7];
+        for (int q = 0; q < 7; ++q) { st[q] = grid.pdata()[q]; rg[q] = grid.ptmp()[q]; }
+        GPU::check(mpcf_window_stage(m_solver, (double)a, (double)b, dt, st, rg), "GPUlab: process_all");
+        return now_s() - t0;
+    }
+    if (m_host_sync) upload();
     GPU::check(mpcf_stage(m_solver, (double)a, (double)b, &dt), "GPUlab: process_all");
     if (m_host_sync) download();
     return now_s() - t0;

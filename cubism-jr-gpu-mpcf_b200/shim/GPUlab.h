@@ -8,7 +8,12 @@
 // process_all is one fused stage kernel (ghosts from the recorded boundary
 // conditions, WENO5/HLLC fluxes in x/y/z, divergence, register and state
 // update).  `nslices` is accepted and checked like the reference
-// (GPUlab.cpp:37-47) but there is no chunking.  With host synchronisation on
+// (GPUlab.cpp:37-47).  A block that fits on the device is not chunked.  A
+// block that does not (or any block with MPCF_GPULAB_WINDOW=1 and nslices <
+// sizeZ) runs windowed as the reference runs it: process_all and max_sos
+// stream grid.pdata()/ptmp() through MPCF_GPULAB_SLOTS (default 6) device
+// slots in chunks of nslices planes (mpcf_create_window, mpcf_window_stage,
+// mpcf_window_max_sos), the host copy always current.  With host synchronisation on
 // (the default) the observable contract of the reference holds: max_sos
 // and process_all read grid.pdata()/ptmp() and process_all leaves the new
 // state in grid.pdata() and the new register in grid.ptmp()
@@ -43,15 +48,16 @@ public:
     double max_sos(float& sos);
     double process_all(const Real a, const Real b, const Real dtinvh);
 
-    // info (GPUlab.h:260-264): one chunk covers the block
-    inline uint_t number_of_chunks() const { return 1; }
-    inline uint_t chunk_slices() const { return sizeZ; }
+    // info (GPUlab.h:260-264): one chunk covers a device-resident block
+    inline uint_t number_of_chunks() const { return m_window ? sizeZ / nslices : 1; }
+    inline uint_t chunk_slices() const { return m_window ? nslices : sizeZ; }
     inline uint_t chunk_start_iz() const { return 0; }
     inline uint_t chunk_id() const { return 1; }
 
     // B200 additions
     mpcf_solver* solver() const { return m_solver; }
-    void set_host_sync(const bool on) { m_host_sync = on; }
+    bool windowed() const { return m_window; }
+    void set_host_sync(const bool on) { m_host_sync = on || m_window; }
     bool host_sync() const { return m_host_sync; }
     void upload();      // grid.pdata()/ptmp() -> device
     void download();    // device -> grid.pdata()/ptmp()
@@ -93,4 +99,5 @@ private:
     bool m_host_sync;
     long m_ghost_calls;     // load_ghosts calls so far
     bool m_check_halos;     // check the halos after every _apply_bc, not only the first
+    bool m_window;          // the block streams through device slots in nslices chunks
 };

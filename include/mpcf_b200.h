@@ -192,6 +192,21 @@ int mpcf_create_window(mpcf_solver** out, int nx, int ny, int nz, int nslices, i
                        const int* bc6, int device);
 int mpcf_run_window(mpcf_solver* s, int nsteps, double cfl, double dt_max, void* const* host7, double* time_out);
 int mpcf_window_info(const mpcf_solver* s, int* info4);
+/* One stage, or the maximum sound speed, of a windowed block whose state and
+ * register both live in host memory: the reference's process_all and
+ * max_sos over nslices chunks (GPUlab.cpp:647-700,703-793), for the shim's
+ * GPUlab when the block does not fit on the device.
+ * mpcf_window_stage: state7 and reg7 (7 fields of nx*ny*nz each) are read
+ *   and overwritten chunk by chunk: rhs = a*R - dtinvh*L(U) into reg7,
+ *   U + b*rhs into state7, bit-identical to mpcf_stage on the whole block.
+ *   Each chunk's state and register go up, its ghost planes come from the
+ *   neighbouring slots (or the z boundary condition), the stage runs once
+ *   the chunk above is there, and both come back, on two copy streams.
+ * mpcf_window_max_sos: the largest sound speed of state7 (streamed through
+ *   the slots), NaN if any cell's is not real and finite.
+ * mpcf_set_bc on a windowed solver (dom 0) sets the block's six faces. */
+int mpcf_window_stage(mpcf_solver* s, double a, double b, double dtinvh, void* const* state7, void* const* reg7);
+int mpcf_window_max_sos(mpcf_solver* s, const void* const* state7, double* sos);
 int mpcf_window_plan(int nchunks, int nslots, int nsteps, int* ops4, int cap);
 int mpcf_synchronize(mpcf_solver* s);
 /* Stream-ordered building blocks of a step, for a driver that orders its

@@ -55,7 +55,19 @@ extern "C" int drv_dims(int* d)
  * place.  sos_cpp selects the reference's -SOSkernel cpp (CPU sound speed on
  * the host state) instead of cuda.  host_sync = 0 keeps the state on the
  * device between stages (then -SOSkernel must be cuda).  Returns the last dt. */
+extern "C" double drv_run_sliced(int nsteps, double cfl, int sos_cpp, const int* bc, float** U, float** R, int host_sync,
+                                 int nslices);
+
 extern "C" double drv_run(int nsteps, double cfl, int sos_cpp, const int* bc, float** U, float** R, int host_sync)
+{
+    return drv_run_sliced(nsteps, cfl, sos_cpp, bc, U, R, host_sync, (int)GridMPI::sizeZ);
+}
+
+/* The same with the lab built for chunks of nslices planes (the reference's
+ * GPUlab(grid, nslices)); with MPCF_GPULAB_WINDOW=1 in the environment the
+ * lab streams the block through device slots chunk by chunk. */
+extern "C" double drv_run_sliced(int nsteps, double cfl, int sos_cpp, const int* bc, float** U, float** R, int host_sync,
+                                 int nslices)
 {
     const size_t n = (size_t)GridMPI::sizeX * GridMPI::sizeY * GridMPI::sizeZ;
     GridMPI grid(1, 1, 1);
@@ -64,7 +76,7 @@ extern "C" double drv_run(int nsteps, double cfl, int sos_cpp, const int* bc, fl
         std::memcpy(grid.pdata()[q], U[q], sizeof(float) * n);
         std::memcpy(grid.ptmp()[q], R[q], sizeof(float) * n);
     }
-    DriverLab lab(grid, GridMPI::sizeZ, bc);
+    DriverLab lab(grid, (uint_t)nslices, bc);
     lab.set_host_sync(host_sync != 0);
     const char* argv[] = {"drv", "-verb", "0", "-SOSkernel", sos_cpp ? "cpp" : "cuda"};
     ArgumentParser parser(5, argv);

@@ -75,3 +75,32 @@ def test_reference_integrator_cpu_sos_reflecting(drv):
         O.stage(dims, bc, U, R, a, b, dt_o / h)
     assert dt == dt_o
     assert bitwise(Ud, U) and bitwise(Rd, R)
+
+
+@pytest.mark.parametrize("nslices,sos_cpp,bc", [(4, 0, (0,) * 6), (8, 1, (1, 0, 0, 1, 1, 0))])
+def test_reference_integrator_windowed_lab(drv, monkeypatch, nslices, sos_cpp, bc):
+    """The lab streamed in chunks of nslices planes (MPCF_GPULAB_WINDOW=1: the
+    path a block larger than device memory takes): the reference's
+    process_all and max_sos over its host state and register chunk by chunk,
+    through device slots.  Two steps equal the oracle bit for bit."""
+    monkeypatch.setenv("MPCF_GPULAB_WINDOW", "1")
+    monkeypatch.setenv("MPCF_GPULAB_SLOTS", "5")
+    drv.drv_run_sliced.restype = ctypes.c_double
+    drv.drv_run_sliced.argtypes = drv.drv_run.argtypes + [ctypes.c_int]
+    dims = drv.dims
+    U = cloud_state(dims, nb=2, seed=33)
+    R = [np.zeros_like(a) for a in U]
+    Ud = [a.copy() for a in U]
+    Rd = [a.copy() for a in R]
+    dt = drv.drv_run_sliced(2, 0.3, sos_cpp, O.bc_arr(bc), O.fptrs(Ud), O.fptrs(Rd), 1, nslices)
+    h = 1.0 / max(dims)
+    for _ in range(2):
+        if sos_cpp:
+            sos = O.oracle().oracle_max_sos_cpp_f32(U[0].size, O.fptrs(U))
+            dt_o = 0.3 * h / sos
+            for a, b in ((0.0, 0.25), (-17.0 / 32, 8.0 / 9), (-32.0 / 27, 0.75)):
+                O.stage(dims, bc, U, R, a, b, dt_o / h)
+        else:
+            dt_o, _ = O.step(dims, bc, U, R, cfl=0.3)
+    assert dt == dt_o
+    assert bitwise(Ud, U) and bitwise(Rd, R)

@@ -165,3 +165,30 @@ def test_window_run_larger_than_device_memory(mpcf):
         sl = slice((z0 - lo) * plane, (z1 - lo) * plane)
         for q in range(7):
             assert np.array_equal(U[q][sl], arrs[q][z0 * plane:z1 * plane]), (z0, q)
+
+
+@pytest.mark.parametrize("prec,nslices,nslots", [("fp32_ref", 4, 3), ("mixed", 8, 6), ("fp64", 6, 4)])
+def test_window_stage_and_sound_speed_equal_resident(mpcf, prec, nslices, nslots):
+    """One stage of a block whose state and register live in host memory
+    (mpcf_window_stage, the reference's chunked process_all) equals the
+    resident stage with the same dt/h bit for bit, register included; the
+    streamed sound speed equals the resident one."""
+    dims = (40, 24, 48)
+    bc = (ABS, REF, REF, ABS, REF, ABS)
+    dtype = mpcf.dtype_of(mpcf.PRECISIONS[prec])
+    U0 = cloud_state(dims, nb=2, seed=41, dtype=dtype)
+    R0 = [np.asarray(a, dtype=dtype) * dtype(1e-3) for a in cloud_state(dims, nb=1, seed=42, dtype=dtype)]
+    a, b, dtinvh = -17.0 / 32, 8.0 / 9, 0.0371
+    with mpcf.Solver([dims], bc=[bc], precision=prec) as s:
+        s.set_state(U0, R0)
+        sos = s.max_sos()[0]
+        s.stage(a, b, dtinvh)
+        U_res, R_res = s.get_state()
+    host = [np.array(x, dtype=dtype) for x in U0]
+    reg = [np.array(x, dtype=dtype) for x in R0]
+    with mpcf.WindowSolver(dims, nslices, max(nslots, 5), bc=bc, precision=prec) as w:
+        assert w.max_sos_host(host) == sos
+        w.stage_host(host, reg, a, b, dtinvh)
+        assert w.error_word() == 0
+    assert_bitwise(host, U_res, f"windowed stage {prec}")
+    assert_bitwise(reg, R_res, f"windowed stage register {prec}")
