@@ -1258,36 +1258,10 @@ int mpcf_run_window(mpcf_solver* s, int nsteps, double cfl, double dt_max, void*
     const size_t esz = s->esz;
     const size_t cbytes = (size_t)nsl * plane * esz;        // one field of one chunk
     const long long fs = s->hdoms[0].fs;
-    if (!s->up)
-    {
-        CK(cudaStreamCreateWithFlags(&s->up, cudaStreamNonBlocking));
-        CK(cudaStreamCreateWithFlags(&s->down, cudaStreamNonBlocking));
-        CK(cudaEventCreateWithFlags(&s->ev_start, cudaEventDisableTiming));
-    }
-    auto grow = [&](std::vector<cudaEvent_t>& v, const int n)
-    {
-        while ((int)v.size() < n)
-        {
-            cudaEvent_t e;
-            if (cudaEventCreateWithFlags(&e, cudaEventDisableTiming) != cudaSuccess) return false;
-            v.push_back(e);
-        }
-        return true;
-    };
-    if (!grow(s->ev_up, nch) || !grow(s->ev_st, nch) || !grow(s->ev_free_c, ns) || !grow(s->ev_free_d, ns))
-    { cudaGetLastError(); return fail(MPCF_ERR_CUDA, "cudaEventCreate failed"); }
-    // the slots' last use by earlier work on the solver's stream frees them
-    CK(cudaEventRecord(s->ev_start, s->stream));
-    CK(cudaStreamWaitEvent(s->up, s->ev_start, 0));
-    CK(cudaStreamWaitEvent(s->down, s->ev_start, 0));
-    for (int k = 0; k < ns; ++k)
-    {
-        CK(cudaEventRecord(s->ev_free_c[k], s->stream));
-        CK(cudaEventRecord(s->ev_free_d[k], s->down));
-    }
+    int rc;
+    if ((rc = window_begin(s))) return rc;
     CK(cudaMemsetAsync(s->sos_bits, 0, esz * ns, s->stream));
     const int p0 = s->parity;
-    int rc = MPCF_OK;
     for (const WinOp& o : plan)
     {
         const int c = o.chunk, slot = c % ns;
@@ -1355,12 +1329,12 @@ int mpcf_run_window(mpcf_solver* s, int nsteps, double cfl, double dt_max, void*
         }
     }
     s->parity = p0 ^ (nsteps & 1);
-    s->sos_fresh = false;
-    s->sums_valid = false;
-    CK(cudaStreamSynchronize(s->down));
-    CK(cudaStreamSynchronize(s->up));
-    if (time_out) CK(cudaMemcpyAsync(time_out, s->time, sizeof(double), cudaMemcpyDeviceToHost, s->stream));
-    CK(cudaStreamSynchronize(s->stream));
+    if ((rc = window_end(s))) return rc;
+    if (time_out)
+    {
+        CK(cudaMemcpyAsync(time_out, s->time, sizeof(double), cudaMemcpyDeviceToHost, s->stream));
+        CK(cudaStreamSynchronize(s->stream));
+    }
     return MPCF_OK;
 }
 
