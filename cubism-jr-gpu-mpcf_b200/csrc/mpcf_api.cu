@@ -1173,6 +1173,23 @@ int mpcf_window_plan(int nchunks, int nslots, int nsteps, int* ops4, int cap)
     return (int)plan.size();
 }
 
+int mpcf_window_stage_plan(int nchunks, int nslots, int* ops4, int cap)
+{
+    std::vector<WinOp> plan;
+    if (nchunks < 1 || nslots < 1) return fail(MPCF_ERR_ARG, "nchunks and nslots must be >= 1");
+    if (!window_stage_plan(nchunks, nslots, plan))
+        return fail(MPCF_ERR_ARG, "%d slots are too few for %d chunks", nslots, nchunks);
+    if (ops4)
+        for (int i = 0; i < (int)plan.size() && i < cap; ++i)
+        {
+            ops4[4 * i] = plan[i].op;
+            ops4[4 * i + 1] = plan[i].step;
+            ops4[4 * i + 2] = plan[i].stage;
+            ops4[4 * i + 3] = plan[i].chunk;
+        }
+    return (int)plan.size();
+}
+
 int mpcf_create_window(mpcf_solver** out, int nx, int ny, int nz, int nslices, int nslots, int precision,
                        const int* bc6, int device)
 {

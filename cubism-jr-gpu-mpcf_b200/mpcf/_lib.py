@@ -98,6 +98,7 @@ SIGNATURES = {
     "mpcf_run_window": (_I, [_P, _I, _D, _D, _PP, _PD]),
     "mpcf_window_info": (_I, [_P, _PI]),
     "mpcf_window_plan": (_I, [_I, _I, _I, _PI, _I]),
+    "mpcf_window_stage_plan": (_I, [_I, _I, _PI, _I]),
     "mpcf_window_stage": (_I, [_P, _D, _D, _D, _PP, _PP]),
     "mpcf_window_max_sos": (_I, [_P, _PP, _PD]),
     "mpcf_synchronize": (_I, [_P]),

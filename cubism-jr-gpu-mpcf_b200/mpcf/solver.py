@@ -483,6 +483,15 @@ class WindowSolver(Solver):
         check(lib().mpcf_set_bc(self._h, 0, (ctypes.c_int * 6)(*[int(v) for v in bc6])))
 
 
+def window_stage_plan(nchunks, nslots):
+    """The operations of one host-resident stage (mpcf_window_stage_plan),
+    rows (kind, step, stage, chunk): kind 0 upload, 3 stage, 4 download."""
+    n = check(lib().mpcf_window_stage_plan(int(nchunks), int(nslots), None, 0))
+    buf = (ctypes.c_int * (4 * max(n, 1)))()
+    check(lib().mpcf_window_stage_plan(int(nchunks), int(nslots), buf, n))
+    return np.frombuffer(buf, dtype=np.int32)[:4 * n].reshape(n, 4).copy()
+
+
 def window_plan(nchunks, nslots, nsteps):
     """The operations of a windowed run in enqueue order (mpcf_window_plan,
     no device work): an int array of rows (kind, step, stage, chunk), kind 0

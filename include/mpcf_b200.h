@@ -208,6 +208,10 @@ int mpcf_window_info(const mpcf_solver* s, int* info4);
 int mpcf_window_stage(mpcf_solver* s, double a, double b, double dtinvh, void* const* state7, void* const* reg7);
 int mpcf_window_max_sos(mpcf_solver* s, const void* const* state7, double* sos);
 int mpcf_window_plan(int nchunks, int nslots, int nsteps, int* ops4, int cap);
+/* The operations of one mpcf_window_stage in enqueue order (no device
+ * work), in mpcf_window_plan's format: kinds 0 upload (state and register),
+ * 3 stage, 4 download; step and stage 0. */
+int mpcf_window_stage_plan(int nchunks, int nslots, int* ops4, int cap);
 int mpcf_synchronize(mpcf_solver* s);
 /* Stream-ordered building blocks of a step, for a driver that orders its
  * own work with the solver's kernels: the reference's per-rank step with

@@ -10,7 +10,8 @@ upload), so those chunks must still sit in their slots; a slot takes its next
 chunk only after its chunk was downloaded and the stage 3 above it (which
 reads its top planes) is queued; dt comes after the sound speed of every
 chunk of the step's input; every chunk of every step is uploaded, staged
-three times and downloaded once.
+three times and downloaded once.  The plan of one host-resident stage
+(mpcf_window_stage, the shim's chunked process_all) is replayed the same way.
 """
 import pytest
 
@@ -97,3 +98,41 @@ def test_window_plan_overlaps_chunks(mpcf):
 def test_window_plan_rejects_too_few_slots(mpcf, nch, ns):
     with pytest.raises(mpcf.MpcfError, match="too few"):
         mpcf.window_plan(nch, ns, 1)
+
+
+def replay_stage(plan, nch, ns):
+    """The plan of one host-resident stage (mpcf_window_stage): a stage of
+    chunk c reads the uploaded chunks c-1 .. c+1; a slot is reused only after
+    its chunk was downloaded and the stage of the chunk above is queued."""
+    last = nch - 1
+    holds = [None] * ns
+    done = set()
+    for kind, n, k, c in plan:
+        key = (kind, c)
+        assert key not in done, ("repeated", key)
+        s = c % ns
+        if kind == UPLOAD:
+            prev = holds[s]
+            if prev is not None:
+                assert (DOWNLOAD, prev) in done, ("slot reused before its download", c, prev)
+                assert (STAGE, prev if prev == last else prev + 1) in done, ("slot reused before the stage above", c, prev)
+            holds[s] = c
+        elif kind == STAGE:
+            for j in range(max(0, c - 1), min(c + 1, last) + 1):
+                assert holds[j % ns] == j and (UPLOAD, j) in done, ("stage reads a chunk not in its slot", c, j)
+        elif kind == DOWNLOAD:
+            assert (STAGE, c) in done and holds[s] == c, ("download before its stage", c)
+        else:
+            raise AssertionError(("unexpected kind", kind))
+        done.add(key)
+    assert len(done) == 3 * nch
+
+
+@pytest.mark.parametrize("nch,ns", [(1, 1), (2, 2), (3, 3), (5, 3), (12, 3), (12, 6), (42, 6), (4, 8)])
+def test_window_stage_plan_is_complete_and_ordered(mpcf, nch, ns):
+    replay_stage(mpcf.window_stage_plan(nch, ns).tolist(), nch, ns)
+
+
+def test_window_stage_plan_rejects_too_few_slots(mpcf):
+    with pytest.raises(mpcf.MpcfError, match="too few"):
+        mpcf.window_stage_plan(6, 2)
