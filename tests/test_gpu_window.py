@@ -88,7 +88,7 @@ def test_window_rejects_what_it_cannot_run(mpcf):
 
 def test_window_run_512cube(mpcf):
     """The benchmark's 512^3 cloud in 16 chunks of 32 planes through 6 slots
-    (2.5 GB of slots on the device against 11.3 GB resident), three steps:
+    (5.0 GB of slots on the device against 11.3 GB resident), three steps:
     bit-identical to the resident run."""
     import torch
     cfg = mpcf.configs.config("c3_512")
