@@ -368,7 +368,7 @@ def main():
                     help="precision of the headline run (profiling of the other forms)")
     ap.add_argument("--workload", default=WORKLOAD)
     ap.add_argument("--e2e-chunks", type=int, default=8, help="z-chunks of the streamed e2e run")
-    ap.add_argument("--window-slots", type=int, default=6,
+    ap.add_argument("--window-slots", type=int, default=8,
                     help="device slots of the windowed e2e run (0: skip it)")
     args = ap.parse_args()
     if args.impl == "reference":

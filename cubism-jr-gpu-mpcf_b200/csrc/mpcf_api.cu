@@ -986,10 +986,19 @@ int mpcf_run_host(mpcf_solver* s, int nsteps, double cfl, double dt_max, void* c
 // Windowed runs: a domain held in host memory that may exceed device memory
 // (GPUlab's z-chunks of nslices planes streamed through the GPU,
 // GPUlab.cpp:202-372,703-793).  The solver's domains are slots of nslices
-// planes with 3 stored ghost planes on each z side; chunk c of a step passes
-// through slot c % nslots.
+// planes with 3 stored ghost planes on each z side.
 // ---------------------------------------------------------------------------
 namespace {
+
+// Slot of chunk c of step n: the chunks of successive steps take the slots
+// in turn, so the first chunks of a step reuse slots freed in the middle of
+// the step before (had every step restarted at slot 0, its first upload
+// would wait for the previous step's last chunks).  The sound-speed pass
+// (step -1) starts at slot 0.
+inline int window_slot(const int n, const int c, const int nch, const int ns)
+{
+    return n < 0 ? c % ns : (int)(((long long)n * nch + c) % ns);
+}
 
 // One operation of a windowed run in the order the host enqueues it.  step
 // -1: the sound-speed pass of the first step's input.
@@ -1063,7 +1072,7 @@ bool window_plan(const int nch, const int ns, const int nsteps, std::vector<WinO
         if (did) continue;
         if (up < total)
         {
-            const int slot = (int)((up % nch) % ns);
+            const int slot = (int)(up % ns);   // window_slot of (up / nch, up % nch)
             if (!busy[slot])
             {
                 busy[slot] = 1;
@@ -1281,7 +1290,7 @@ int mpcf_run_window(mpcf_solver* s, int nsteps, double cfl, double dt_max, void*
     const int p0 = s->parity;
     for (const WinOp& o : plan)
     {
-        const int c = o.chunk, slot = c % ns;
+        const int c = o.chunk, slot = window_slot(o.step, c, nch, ns);
         const int p = o.step < 0 ? p0 : (p0 ^ (o.step & 1));      // the step's input buffer
         DomDev& D = s->hdoms[slot];
         const size_t off = (size_t)c * cbytes;
@@ -1317,8 +1326,8 @@ int mpcf_run_window(mpcf_solver* s, int nsteps, double cfl, double dt_max, void*
             {
                 const int k = o.stage, b = p ^ (k & 1);
                 if (k == 0) CK(cudaStreamWaitEvent(s->stream, s->ev_up[std::min(c + 1, nch - 1)], 0));
-                const void* lo = c > 0 ? s->hdoms[(c - 1) % ns].U[b] : nullptr;
-                const void* hi = c < nch - 1 ? s->hdoms[(c + 1) % ns].U[b] : nullptr;
+                const void* lo = c > 0 ? s->hdoms[window_slot(o.step, c - 1, nch, ns)].U[b] : nullptr;
+                const void* hi = c < nch - 1 ? s->hdoms[window_slot(o.step, c + 1, nch, ns)].U[b] : nullptr;
                 CK(launch_window_ghosts((int)esz, D.U[b], lo, hi, fs, plane, nsl, s->win_bc[0], s->win_bc[1], s->stream));
                 s->parity = b;
                 rc = enqueue_stage_tiles(s, kLSRK3[k][0], kLSRK3[k][1], false, k == 2, D.tile_begin,
@@ -1331,7 +1340,7 @@ int mpcf_run_window(mpcf_solver* s, int nsteps, double cfl, double dt_max, void*
                     // the chunk below is no longer read (its top planes were
                     // this stage's lower ghost planes); the last chunk frees
                     // its own slot
-                    if (c > 0) CK(cudaEventRecord(s->ev_free_c[(c - 1) % ns], s->stream));
+                    if (c > 0) CK(cudaEventRecord(s->ev_free_c[window_slot(o.step, c - 1, nch, ns)], s->stream));
                     if (c == nch - 1) CK(cudaEventRecord(s->ev_free_c[slot], s->stream));
                 }
                 break;

@@ -171,7 +171,8 @@ int mpcf_run_host(mpcf_solver* s, int nsteps, double cfl, double dt_max, void* c
  *   set_tiling applies to the slots.
  * mpcf_run_window: nsteps LSRK3 steps of host7 (7 fields of nx*ny*nz, x
  *   fastest; page-locked memory lets copies overlap), overwritten with each
- *   step's result.  Chunk c goes through slot c % nslots: its upload, the
+ *   step's result.  The chunks of successive steps take the slots in turn
+ *   (chunk c of step n: slot (n*chunks + c) % nslots): each chunk's upload, the
  *   three stages as a wavefront over the chunks (a stage of chunk c runs once
  *   the stage before it covers chunk c+1; before each stage a kernel fills
  *   the slot's ghost planes from the neighbouring slots, or by the boundary

@@ -23,7 +23,9 @@ def replay(plan, nch, ns, nsteps):
     place; return the count of each kind."""
     last = nch - 1
     hi = lambda c: min(c + 1, last)
-    slot_of = lambda c: c % ns
+    # chunk c of step n: the steps take the slots in turn (the sound-speed
+    # pass, step -1, from slot 0)
+    slot_of = lambda n, c: c % ns if n < 0 else (n * nch + c) % ns
     holds = [None] * ns            # (step, chunk) now in the slot
     done = set()                   # (kind, step, stage, chunk) already enqueued
     sos_done = set()
@@ -33,7 +35,7 @@ def replay(plan, nch, ns, nsteps):
         key = (kind, n, k, c)
         assert key not in done, ("repeated", key)
         if kind == UPLOAD:
-            s = slot_of(c)
+            s = slot_of(n, c)
             prev = holds[s]
             if prev is not None:
                 pn, pc = prev
@@ -45,7 +47,7 @@ def replay(plan, nch, ns, nsteps):
                     assert (STAGE, pn, 2, above) in done, ("slot reused before the stage 3 above it", key, prev)
             holds[s] = (n, c)
         elif kind == SOS:
-            assert holds[slot_of(c)] == (-1, c), ("sound speed of a chunk not in its slot", key)
+            assert holds[slot_of(-1, c)] == (-1, c), ("sound speed of a chunk not in its slot", key)
             sos_done.add(c)
         elif kind == DT:
             if n == 0:
@@ -56,14 +58,14 @@ def replay(plan, nch, ns, nsteps):
         elif kind == STAGE:
             assert (DT, n, 0, 0) in done, ("stage before its dt", key)
             for j in range(max(0, c - 1), hi(c) + 1):
-                assert holds[slot_of(j)] == (n, j), ("stage reads a chunk not in its slot", key, j, holds[slot_of(j)])
+                assert holds[slot_of(n, j)] == (n, j), ("stage reads a chunk not in its slot", key, j, holds[slot_of(n, j)])
                 if k == 0:
                     assert (UPLOAD, n, 0, j) in done, ("stage 1 before the upload", key, j)
                 else:
                     assert (STAGE, n, k - 1, j) in done, ("stage before the previous stage", key, j)
         elif kind == DOWNLOAD:
             assert (STAGE, n, 2, c) in done, ("download before stage 3", key)
-            assert holds[slot_of(c)] == (n, c), ("download of a chunk not in its slot", key)
+            assert holds[slot_of(n, c)] == (n, c), ("download of a chunk not in its slot", key)
         done.add(key)
     return count
 
