@@ -1012,27 +1012,31 @@ enum { WOP_UPLOAD = 0, WOP_SOS = 1, WOP_DT = 2, WOP_STAGE = 3, WOP_DOWNLOAD = 4 
 // (which copies its top planes) is queued.  Each step's dt needs the sound
 // speed of all of its input: the first from a pass that streams every chunk
 // through the slots and reduces it, later ones from what stage 3 of the
-// step before accumulated.  Operations are taken greedily, downloads and the
-// later stages first; false if nothing can proceed (too few slots).
+// step before accumulated.  That pass runs from the last chunk down, so it
+// leaves chunks 0 .. ns-1 in their slots, where the first step finds them
+// without uploading them again.  Operations are taken greedily, downloads and
+// the later stages first; false if nothing can proceed (too few slots).
 bool window_plan(const int nch, const int ns, const int nsteps, std::vector<WinOp>& plan)
 {
     plan.clear();
     if (nsteps <= 0) return true;
     if (nch < 1 || ns < 1) return false;
     auto hi = [&](const int c) { return std::min(c + 1, nch - 1); };
-    // the sound-speed pass: chunk u into slot u % ns once chunk u - ns has
-    // been reduced
+    // the sound-speed pass, from the last chunk down: chunk c into slot
+    // c % ns once chunk c + ns has been reduced
     for (int u = 0, q = 0; q < nch;)
     {
-        if (u < nch && u - q < ns) plan.push_back({WOP_UPLOAD, -1, 0, u++});
-        else plan.push_back({WOP_SOS, -1, 0, q++});
+        if (u < nch && u - q < ns) plan.push_back({WOP_UPLOAD, -1, 0, nch - 1 - u++});
+        else plan.push_back({WOP_SOS, -1, 0, nch - 1 - q++});
     }
     plan.push_back({WOP_DT, 0, 0, 0});
     int dts = 1;                                   // steps whose dt is queued
     const long long total = (long long)nsteps * nch;
-    long long up = 0, dn = 0, st[3] = {0, 0, 0};   // next operation of each kind (step * nch + chunk)
+    const int kept = std::min(ns, nch);           // the first step's chunks the pass left in place
+    long long up = kept, dn = 0, st[3] = {0, 0, 0};   // next operation of each kind (step * nch + chunk)
     std::vector<long long> occ(ns, -1);
     std::vector<char> busy(ns, 0);
+    for (int k = 0; k < kept; ++k) { busy[k] = 1; occ[k] = k; }
     auto released = [&](const long long j)
     {
         const long long above = (j % nch == nch - 1) ? j : j + 1;

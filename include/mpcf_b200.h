@@ -178,7 +178,8 @@ int mpcf_run_host(mpcf_solver* s, int nsteps, double cfl, double dt_max, void* c
  *   the slot's ghost planes from the neighbouring slots, or by the boundary
  *   condition at the domain's z faces), and its download, on two copy
  *   streams and the solver's stream.  The first step's dt comes from a pass
- *   that streams every chunk through the slots and reduces its sound speed;
+ *   that streams every chunk through the slots, from the last down, and
+ *   reduces its sound speed (the first step reuses the chunks it leaves);
  *   later steps take what stage 3 accumulated.  Results are bit-identical
  *   to mpcf_run of the whole domain on one device.  time_out (optional): the
  *   time.

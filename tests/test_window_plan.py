@@ -1,7 +1,9 @@
 """The operation plan of windowed runs (mpcf_window_plan; CPU only, no device
 work): the order in which mpcf_run_window enqueues uploads, sound-speed
 reductions, dt, stages and downloads of z-chunks streamed through a few
-device slots (the reference's GPUlab chunks, GPUlab.cpp:202-372).
+device slots (the reference's GPUlab chunks, GPUlab.cpp:202-372).  The
+sound-speed pass runs from the last chunk down and leaves the first chunks
+in their slots for the first step.
 
 An independent replay checks every plan: which chunk each slot holds after
 every operation, and that each operation finds what it reads.  A stage of
@@ -52,6 +54,12 @@ def replay(plan, nch, ns, nsteps):
         elif kind == DT:
             if n == 0:
                 assert len(sos_done) == nch, ("dt before the sound speed of every chunk", key)
+                # the pass ran from the last chunk down and left chunks
+                # 0 .. ns-1 in place: they are the first step's input
+                for s_ in range(min(ns, nch)):
+                    assert holds[s_] == (-1, s_), ("the pass left the wrong chunk", s_, holds[s_])
+                    holds[s_] = (0, s_)
+                    done.add((UPLOAD, 0, 0, s_))
             else:
                 for j in range(nch):
                     assert (STAGE, n - 1, 2, j) in done, ("dt before the previous step's stage 3", key, j)
@@ -78,7 +86,8 @@ CASES = [(16, 8), (16, 5), (16, 16), (7, 5), (48, 6), (3, 3), (2, 2), (1, 1), (5
 def test_window_plan_is_complete_and_ordered(mpcf, nch, ns, nsteps):
     plan = mpcf.window_plan(nch, ns, nsteps).tolist()
     count = replay(plan, nch, ns, nsteps)
-    assert count[UPLOAD] == nch * (nsteps + 1)      # the sound-speed pass and every step
+    # the sound-speed pass and every step, less the chunks the pass left in place
+    assert count[UPLOAD] == nch * (nsteps + 1) - min(ns, nch)
     assert count[SOS] == nch
     assert count[DT] == nsteps
     assert count[STAGE] == 3 * nch * nsteps
