@@ -7,7 +7,8 @@ Every step must be bit-identical to the same steps of the whole domain
 resident on the device (mpcf_run): chunks of 3 planes (the stencil's reach)
 up to several tile layers, the fewest slots the wavefront needs and more,
 absorbing and reflecting z faces (ghost planes by the boundary condition),
-every precision form, and the 512^3 cloud of the benchmark."""
+every precision form, the reference's WENO3 build, and the 512^3 cloud of
+the benchmark."""
 import numpy as np
 import pytest
 
@@ -192,3 +193,25 @@ def test_window_stage_and_sound_speed_equal_resident(mpcf, prec, nslices, nslots
         assert w.error_word() == 0
     assert_bitwise(host, U_res, f"windowed stage {prec}")
     assert_bitwise(reg, R_res, f"windowed stage register {prec}")
+
+
+@pytest.mark.parametrize("prec", ["fp32_ref", "fp64"])
+def test_window_run_weno3_equals_resident(mpcf, prec):
+    """The reference's compile-time WENO3 reconstruction (set on the windowed
+    solver, every slot) streams like WENO5: two steps equal the resident run."""
+    dims = (40, 24, 48)
+    bc = (ABS, REF, ABS, ABS, REF, ABS)
+    dtype = mpcf.dtype_of(mpcf.PRECISIONS[prec])
+    U0 = cloud_state(dims, nb=2, seed=23, dtype=dtype)
+    with mpcf.Solver([dims], bc=[bc], precision=prec) as s:
+        s.set_weno_order(3)
+        s.set_state(U0)
+        t_res = s.run(2, cfl=0.3, graph=False)[0]
+        U_res = s.get_state(with_reg=False)
+    host = [np.array(a, dtype=dtype) for a in U0]
+    with mpcf.WindowSolver(dims, 6, 5, bc=bc, precision=prec) as w:
+        w.set_weno_order(3)
+        t = w.run(host, 2, cfl=0.3)
+        assert w.error_word() == 0
+    assert t == t_res
+    assert_bitwise(host, U_res, f"windowed WENO3 {prec}")
