@@ -42,7 +42,7 @@ METRIC = "cell-stage updates/s on 1 B200: mixed vs plain FP64 at stated L1 error
 UNIT = "cell-stage updates/s"
 BYTES_PER_CELL_STAGE = {"fp32_ref": 112, "fp32": 112, "mixed": 112, "fp64": 224, "fp64_fast": 224}
 # DRAM bytes per cell-stage of the mixed stage kernel measured by ncu
-# (dram__bytes_read.sum + dram__bytes_write.sum = 2.145 + 1.831 GB for one
+# (dram__bytes_read.sum + dram__bytes_write.sum = 2.135 + 1.831 GB for one
 # launch over the 512 x 512 x 128 lower quarter of the 512^3 cloud, 33.55 M
 # cells, 32 x 8 tiles over whole columns, persistent, bulk-copy staging: a
 # few-GB case of the bench's kernel and tiling).  The per-launch figure of the
