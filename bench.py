@@ -608,10 +608,42 @@ def window_measure(mpcf, cfg, K, W, cfl, dist, precision, tiling, host, nslots, 
         esz = 8 if precision in ("fp64", "fp64_fast") else 4
         slot_bytes = 3 * 7 * esz * dims[0] * dims[1] * (nslices + 6)
         v, _ = rp.throughput(dist, ncell, 3.0 * K, sec * 1e3, device="cuda" if dist is not None else None)
-        return {"value": v, "unit": UNIT, "ms_per_step": sec * 1e3 / K, "nslices": nslices, "slots": w.nslots,
-                "device_bytes": w.nslots * slot_bytes, "resident_bytes": 3 * 7 * esz * ncell,
-                "path": f"mpcf_run_window: {w.nchunks} chunks of {nslices} planes through {w.nslots} device slots, "
-                        f"host wall clock over one call of {K} steps"}
+        out = {"value": v, "unit": UNIT, "ms_per_step": sec * 1e3 / K, "nslices": nslices, "slots": w.nslots,
+               "device_bytes": w.nslots * slot_bytes, "resident_bytes": 3 * 7 * esz * ncell,
+               "path": f"mpcf_run_window: {w.nchunks} chunks of {nslices} planes through {w.nslots} device slots, "
+                       f"host wall clock over one call of {K} steps"}
+        # the reference's per-stage form (the shim's GPUlab for a block that
+        # does not fit): every stage streams the state and the register
+        # through the slots and back, every step streams the state once more
+        # for its sound speed (mpcf_window_max_sos, mpcf_window_stage)
+        reg = [torch.zeros(ncell, dtype=torch.float64 if esz == 8 else torch.float32, pin_memory=True)
+               for _ in range(7)]
+        regs = [r.numpy() for r in reg]
+        h = 1.0 / max(dims)
+
+        def per_stage(k):
+            for _ in range(k):
+                dt = cfl * h / w.max_sos_host(host)
+                for a, b in mpcf.LSRK3:
+                    w.stage_host(host, regs, a, b, dt / h)
+
+        ks = 2
+        per_stage(1)
+        if dist is not None:
+            dist.barrier()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        per_stage(ks)
+        torch.cuda.synchronize()
+        sec = time.perf_counter() - t0
+        v, _ = rp.throughput(dist, ncell, 3.0 * ks, sec * 1e3, device="cuda" if dist is not None else None)
+        out["per_stage"] = {"value": v, "unit": UNIT, "ms_per_step": sec * 1e3 / ks,
+                            "h2d_bytes_per_step": (1 + 3 * 2) * 7 * esz * ncell,
+                            "d2h_bytes_per_step": 3 * 2 * 7 * esz * ncell,
+                            "path": f"mpcf_window_max_sos + 3 x mpcf_window_stage per step (state and register in "
+                                    f"host memory, the reference's per-stage streaming), {ks} steps"}
+        del reg, regs
+        return out
 
 
 def e2e_measure(mpcf, cfg, K, W, cfl, dist, precision="mixed", tiling=None, nchunks=8, serial_form=True,
