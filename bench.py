@@ -709,8 +709,8 @@ def e2e_measure(mpcf, cfg, K, W, cfl, dist, precision="mixed", tiling=None, nchu
         if window_slots:
             try:
                 out["window"] = window_measure(mpcf, cfg, K, W, cfl, dist, precision, tiling, host, window_slots)
-            except mpcf.MpcfError as e:
-                out["window"] = {"error": str(e)}
+            except Exception as e:          # a side leg: the line stands without it
+                out["window"] = {"error": f"{type(e).__name__}: {e}"}
 
     def serial(k):
         for _ in range(k):
